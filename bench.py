@@ -1,0 +1,439 @@
+"""Benchmark of the B200 statevector engine on the random-circuit workload at n = 32.
+
+One step = one run of the seeded random layer circuit (n qubits, depth 20:
+per layer one of H/S/T/SQRT_X/RZ on every qubit, then CZ on a random perfect
+matching; n + n/2 gates per layer) on the device state.  The register is 32
+qubits: 64 GiB in complex128 (plain path) or 32 GiB in complex64 (fused
+precision form), far larger than L2, so no flush is needed between steps.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+Prints one JSON line.  For N > 1 (torchrun, one rank per GPU) every rank runs
+an independent replica with its own seed (weak scaling; the path has no
+data exchange between replicas) and the time is the max over ranks.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+METRIC = "gates/s & %HBM peak, FP32-fused vs FP64, n=32 (1−F≤1e-6); trajectories/s"
+FALLBACK_HBM_GBS = 6650.0
+
+
+def _dist_env():
+    return int(os.environ.get("RANK", "0")), int(os.environ.get("WORLD_SIZE", "1")), int(os.environ.get("LOCAL_RANK", "0"))
+
+
+RANK, WORLD, LOCAL_RANK = _dist_env()
+if WORLD > 1 and "CUDA_VISIBLE_DEVICES" not in os.environ:
+    # one GPU per rank: the engine uses device 0 of its own runtime
+    os.environ["CUDA_VISIBLE_DEVICES"] = str(LOCAL_RANK)
+
+sys.path.insert(0, ROOT)
+
+
+def measured_peaks():
+    for p in (os.path.join(ROOT, "MEASURED_PEAKS.json"), "/root/repo/MEASURED_PEAKS.json"):
+        if os.path.exists(p):
+            with open(p) as f:
+                d = json.load(f)
+            return float(d["hbm_gbs"]), "measured"
+    return FALLBACK_HBM_GBS, "fallback"
+
+
+def profiled_traffic(kernel: str):
+    """DRAM bytes per launch of `kernel` from a committed ncu summary, if any."""
+    path = os.path.join(ROOT, "profiles", f"{kernel}.md")
+    if not os.path.exists(path):
+        return None
+    for line in open(path):
+        if line.startswith("traffic_bytes_per_launch:"):
+            try:
+                return float(line.split(":", 1)[1].strip().split()[0])
+            except ValueError:
+                return None
+    return None
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled during the timed region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self):
+        self.proc = None
+        self.lines = []
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except OSError:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def __exit__(self, *a):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+
+    def summary(self, device_index: int = 0):
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            parts = [p.strip() for p in ln.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                idx = int(parts[0])
+            except ValueError:
+                continue
+            vis = os.environ.get("CUDA_VISIBLE_DEVICES")
+            want = int(vis.split(",")[0]) if vis and vis.split(",")[0].isdigit() else device_index
+            if idx != want:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                mx = float(parts[2])
+            except ValueError:
+                pass
+            for name, flag in zip(names, parts[5:9]):
+                if flag.lower() == "active":
+                    reasons.add(name)
+        if not sm:
+            return None
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": mx, "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def dist_init():
+    if WORLD <= 1:
+        return None
+    import datetime
+
+    import torch.distributed as dist
+
+    dist.init_process_group("gloo", timeout=datetime.timedelta(seconds=600))
+    return dist
+
+
+def max_over_ranks(dist, v: float) -> float:
+    if dist is None:
+        return v
+    import torch
+
+    t = torch.tensor([v], dtype=torch.float64)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def barrier(dist):
+    if dist is not None:
+        dist.barrier()
+
+
+def pick_n(nb, want: int, precision_bytes: int, states: int) -> int:
+    free = nb.device_info()["free_bytes"]
+    n = want
+    while n > 20 and states * (precision_bytes << n) + (6 << 30) > free:
+        n -= 1
+    return n
+
+
+def host_mem_available() -> int:
+    try:
+        for line in open("/proc/meminfo"):
+            if line.startswith("MemAvailable:"):
+                return int(line.split()[1]) * 1024
+    except OSError:
+        pass
+    return 0
+
+
+def cpu_baseline(n_want: int, depth: int, seed: int, budget_s: float = 15.0):
+    """The oracle (C++ restatement of the reference's StateVector, all host
+    threads) on a bounded sample of the same workload: the first G gates of
+    the same circuit from |+>^n, timed; G grows until the sample takes about
+    budget_s seconds."""
+    from oracle import oracle as O
+
+    avail = host_mem_available()
+    n = n_want
+    while n > 20 and (16 << n) * 1.3 > avail:
+        n -= 1
+    text = O.random_circuit_text(n, depth, seed)
+    circ = O.Circuit(text)
+    s = O.StateVector.plus_state(n)
+    done, elapsed, g = 0, 0.0, 1
+    total_gates = circ.num_gates
+    while elapsed < budget_s and done < total_gates:
+        g = min(g, total_gates - done)
+        # each call restarts at the circuit's first gate: the sample is the first g gates
+        dt = s.run_gates_timed(circ, g)
+        elapsed += dt
+        done += g
+        per = dt / g
+        g = max(1, int(min(budget_s - elapsed, budget_s / 3) / max(per, 1e-9)))
+    return {
+        "value": done / elapsed,
+        "unit": "gates/s",
+        "cores": O.lib().oracle_num_threads(),
+        "kind": "port",
+        "sample": f"oracle StateVector<C64> at n={n}: {done} gates of the random layer circuit "
+                  f"(depth {depth}, seed {seed}) from |+>^n in {elapsed:.1f} s"
+                  + ("" if n == n_want else f" (n reduced from {n_want} to fit host memory)"),
+        "n": n,
+    }
+
+
+def run_reference(args):
+    """--impl reference: the reference's CPU path (the oracle port) on host cores."""
+    if RANK != 0:
+        return 0
+    from oracle import oracle as O
+
+    O.lib()
+    vals = []
+    sample = None
+    for i in range(args.warmup + args.steps):
+        r = cpu_baseline(args.n, args.depth, 1, budget_s=args.cpu_budget)
+        if i >= args.warmup:
+            vals.append(r["value"])
+        sample = r
+    v = statistics.median(vals)
+    line = {
+        "impl": "reference",
+        "metric": METRIC,
+        "value": v,
+        "unit": "gates/s",
+        "n_gpus": args.gpus,
+        "steps": args.steps,
+        "warmup": args.warmup,
+        "ms_per_step": 1e3 / v,
+        "higher_is_better": True,
+        "scaling": "weak",
+        "vs_baseline": None,
+        "dtype": "f64",
+        "data": "synthetic",
+        "config": {"workload": f"random layers n={sample['n']} depth {args.depth} seed 1 (complex128)",
+                   "n": sample["n"], "depth": args.depth},
+        "cpu_baseline": {"value": v, "unit": "gates/s", "cores": sample["cores"], "kind": "port",
+                         "sample": sample["sample"]},
+        "e2e": {"value": v, "unit": "gates/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def timed_runs(nb, state, circuit, steps: int, warmup: int, fused: bool, dist):
+    rng = nb.StdRng(12345)
+    for _ in range(warmup):
+        state.run_fused(circuit, rng) if fused else state.run(circuit, rng)
+    state.synchronize()
+    barrier(dist)
+    state.profile(True)
+    state.timer_start()
+    for _ in range(steps):
+        state.run_fused(circuit, rng) if fused else state.run(circuit, rng)
+    ms = state.timer_stop()
+    prof = state.profile_read()
+    state.profile(False)
+    return ms, prof
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=3)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--n", type=int, default=32)
+    ap.add_argument("--depth", type=int, default=20)
+    ap.add_argument("--path", default="auto", choices=["auto", "plain", "fused"])
+    ap.add_argument("--cpu-budget", type=float, default=15.0)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-e2e", action="store_true")
+    args = ap.parse_args()
+
+    if args.impl == "reference":
+        return run_reference(args)
+
+    import ncsim_b200 as nb
+
+    nb.lib()
+    dist = dist_init()
+    seed = 1 + RANK
+    peak, peak_kind = measured_peaks()
+
+    fused_ok = args.path in ("auto", "fused")
+    if fused_ok:
+        try:
+            probe = nb.GpuStateVector(8, nb.C64)
+            probe.run_fused(nb.Circuit.random_layers(8, 1, 1), nb.StdRng(0))
+            del probe
+        except nb.SimError:
+            if args.path == "fused":
+                raise
+            fused_ok = False
+
+    result = {}
+    n = args.n
+    if fused_ok:
+        n = pick_n(nb, args.n, 8, 1)
+        circuit = nb.Circuit.random_layers(n, args.depth, seed)
+        st = nb.GpuStateVector(n, nb.C64)
+        with ClockSampler() as clk:
+            ms, prof = timed_runs(nb, st, circuit, args.steps, args.warmup, True, dist)
+        headline = ("fused", st, ms, prof, clk)
+    else:
+        n = pick_n(nb, args.n, 16, 1)
+        circuit = nb.Circuit.random_layers(n, args.depth, seed)
+        st = nb.GpuStateVector(n, nb.C128)
+        with ClockSampler() as clk:
+            ms, prof = timed_runs(nb, st, circuit, args.steps, args.warmup, False, dist)
+        headline = ("plain", st, ms, prof, clk)
+
+    path, state, ms, prof, clk = headline
+    gates = circuit.num_gates
+    ms_max = max_over_ranks(dist, ms)
+    value = WORLD * args.steps * gates / (ms_max / 1e3)
+    launches = sum(v["launches"] for v in prof.values())
+    dom = max(prof.items(), key=lambda kv: kv[1]["ms"])
+    dom_name, dom_v = dom
+    achieved = dom_v["bytes"] / (dom_v["ms"] / 1e3) / 1e9
+    total_bytes = sum(v["bytes"] for v in prof.values())
+    overall = total_bytes / (ms / 1e3) / 1e9
+    traffic = profiled_traffic(dom_name)
+    roofline = {
+        "bound": "hbm",
+        "kernel": dom_name,
+        "achieved": round(achieved, 1),
+        "peak": peak,
+        "unit": "GB/s",
+        "frac": round(achieved / peak, 4),
+        "peak_kind": peak_kind,
+        "traffic": traffic,
+        "algorithmic_bytes_per_launch": dom_v["bytes"] / max(1, dom_v["launches"]),
+        "launches": dom_v["launches"],
+        "step_frac": round(overall / peak, 4),
+    }
+    result["kernels"] = {k: {"launches": v["launches"], "ms": round(v["ms"], 3),
+                             "GBps": round(v["bytes"] / max(v["ms"], 1e-9) / 1e6, 1)} for k, v in prof.items()}
+
+    # the FP64 comparison arm and the fidelity of the fused result
+    if path == "fused":
+        del state
+        ref = nb.GpuStateVector(n, nb.C128)
+        ms_p, prof_p = timed_runs(nb, ref, circuit, 1, 1, False, None)
+        result["plain_fp64"] = {"gates_per_s": gates / (ms_p / 1e3), "ms_per_circuit": ms_p}
+        fz = nb.GpuStateVector(n, nb.C64)
+        ref64 = nb.GpuStateVector(n, nb.C128)
+        del ref
+        rng_a, rng_b = nb.StdRng(7), nb.StdRng(7)
+        ref64.run(circuit, rng_a)
+        fz.run_fused(circuit, rng_b)
+        cmpd = ref64.compare(fz)
+        result["fidelity"] = {"infidelity": cmpd["infidelity"], "max_abs_diff": cmpd["max_abs_diff"],
+                              "norm_fused": cmpd["norm_b"]}
+        result["speedup_vs_fp64"] = value / WORLD / result["plain_fp64"]["gates_per_s"]
+        del fz, ref64
+    else:
+        del state
+
+    # end to end through the C ABI: host circuit text in, readouts out
+    e2e = None
+    if not args.no_e2e:
+        text = circuit.to_text()
+        prec = nb.C64 if path == "fused" else nb.C128
+        e2e_state = nb.GpuStateVector(n, prec)
+        pz = nb.Pauli.from_string(n, "Z0*Z1")
+        idx = list(range(0, 1 << n, (1 << n) // 64))[:64]
+
+        def one_step():
+            c = nb.Circuit.parse(text)  # host bytes in
+            lib = nb.lib()
+            nb._check(lib.ncsim_sv_set_basis(e2e_state._h, 0))
+            if path == "fused":
+                e2e_state.run_fused(c, nb.StdRng(3))
+            else:
+                e2e_state.run(c, nb.StdRng(3))
+            e = e2e_state.expectation(pz)  # results out
+            a = e2e_state.amplitudes_at(idx)
+            return e, a
+
+        one_step()
+        barrier(dist)
+        t0 = time.perf_counter()
+        e2e_steps = max(1, min(args.steps, 2))
+        for _ in range(e2e_steps):
+            one_step()
+        dt = max_over_ranks(dist, time.perf_counter() - t0)
+        e2e = {"value": WORLD * e2e_steps * gates / dt, "unit": "gates/s",
+               "h2d_bytes_per_step": len(text.encode()), "d2h_bytes_per_step": 16 + 16 * len(idx),
+               "note": "per step: parse the circuit text, reset |0>, run, <Z0 Z1>, 64 amplitudes; host wall clock"}
+        del e2e_state
+
+    cpu = None
+    if RANK == 0 and WORLD == 1 and not args.no_cpu_baseline:
+        cpu = cpu_baseline(n if path == "plain" else args.n, args.depth, seed, args.cpu_budget)
+
+    clocks = clk.summary() if clk else None
+    line = {
+        "metric": METRIC,
+        "value": value,
+        "unit": "gates/s",
+        "n_gpus": WORLD,
+        "steps": args.steps,
+        "warmup": args.warmup,
+        "ms_per_step": ms_max / args.steps,
+        "higher_is_better": True,
+        "scaling": "weak",
+        "vs_baseline": None,
+        "dtype": "f32" if path == "fused" else "f64",
+        "data": "synthetic",
+        "config": {
+            "workload": f"random layers n={n} depth {args.depth} ({gates} gates), seed 1+rank, "
+                        f"{'fused precision form, complex64' if path == 'fused' else 'plain one-kernel-per-gate path, complex128'}",
+            "n": n,
+            "depth": args.depth,
+            "gates_per_step": gates,
+            "path": path,
+            "l2": "state larger than L2 (no flush needed)",
+            "parallelism": f"replicas x{WORLD}",
+        },
+        "roofline": roofline,
+        "cpu_baseline": cpu,
+        "e2e": e2e,
+        "clocks": clocks,
+        "gpu_launches": launches,
+    }
+    line.update(result)
+    if RANK == 0:
+        print(json.dumps(line), flush=True)
+    if dist is not None:
+        dist.barrier()
+        dist.destroy_process_group()
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -1,0 +1,266 @@
+/*
+ * ncsim_cuda.h — C ABI of the B200 dense statevector engine (libncsim_cuda.so).
+ *
+ * The engine is a drop-in for ncsim's `StateVector<C64>` behind the
+ * `QuantumState<C64>` trait (reference: src/state/mod.rs:41-234,
+ * src/state/vector.rs:16-549).  A thin Rust crate (`ncsim-cuda`) binds these
+ * functions and implements `GpuStateVector: QuantumState<C64>`; the core crate
+ * keeps `#![forbid(unsafe_code)]` (src/lib.rs:36).
+ *
+ * Two layers are exported:
+ *   1. state operations with plain-old-data arguments (pointers, sizes, bit
+ *      masks, row-major complex128 arrays): what the Rust crate calls after it
+ *      lowers a `Gate` through the reference's own views
+ *      (`Gate::monomial/matrix`, src/gate.rs:519-747);
+ *   2. a C++ host mirror of the trait's provided methods (run, measure,
+ *      sample with a seeded StdRng, text circuits, workloads) for hosts that
+ *      have no Rust toolchain, and the two GPU-only forms (fused precision
+ *      form, batched trajectories).
+ *
+ * Conventions (src/state/vector.rs:14, src/pauli/ops.rs:5):
+ *   - qubit q is bit q of a basis index; a k-qubit gate matrix is row-major,
+ *     2^k x 2^k, over the local index whose bit j is qubits[j];
+ *   - complex numbers are interleaved (re, im) doubles;
+ *   - a Pauli is i^phase * X^x * Z^z with x, z bit masks over the register
+ *     (so Y_q has x = z = 1<<q and phase 1).
+ *
+ * Every function returns an ncsim_status; NCSIM_OK is 0.  On error,
+ * ncsim_last_error() returns a thread-local message.  No function aborts or
+ * throws across the ABI.  Handles may be used from several threads: each
+ * state serialises its own calls (the trait requires Send + Sync; read-only
+ * calls such as expectation are issued from rayon threads by
+ * src/state/mod.rs:93-101 and src/bridge.rs:456-464).
+ */
+#ifndef NCSIM_CUDA_H
+#define NCSIM_CUDA_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* Status codes mirror SimError (src/error.rs:7-42) plus device errors. */
+typedef int32_t ncsim_status;
+#define NCSIM_OK 0
+#define NCSIM_ERR_UNSUPPORTED 1         /* SimError::Unsupported */
+#define NCSIM_ERR_QUBIT_OUT_OF_RANGE 2  /* SimError::QubitOutOfRange */
+#define NCSIM_ERR_ARITY 3               /* SimError::Arity */
+#define NCSIM_ERR_DUPLICATE_QUBIT 4     /* SimError::DuplicateQubit */
+#define NCSIM_ERR_NOT_REPRESENTABLE 5   /* SimError::NotRepresentable */
+#define NCSIM_ERR_ZERO_STATE 6          /* SimError::ZeroState */
+#define NCSIM_ERR_PARSE 7               /* SimError::Parse */
+#define NCSIM_ERR_INVALID 8             /* SimError::Invalid */
+#define NCSIM_ERR_DEVICE 9              /* CUDA error (maps to SimError::Invalid on the Rust side) */
+#define NCSIM_ERR_OUT_OF_MEMORY 10      /* device allocation failed */
+
+/* Amplitude storage. */
+#define NCSIM_C128 0 /* complex<double>: the drop-in for StateVector<C64> */
+#define NCSIM_C64 1  /* complex<float>: storage of the fused precision form and the batched form */
+
+typedef struct ncsim_state ncsim_state;
+typedef struct ncsim_rng ncsim_rng;
+typedef struct ncsim_circuit ncsim_circuit;
+typedef struct ncsim_gate ncsim_gate;
+
+/* Thread-local message of the last failed call on this thread. */
+const char* ncsim_last_error(void);
+/* ABI version (major * 10000 + minor * 100 + patch). */
+int32_t ncsim_abi_version(void);
+/* Streaming multiprocessors, free and total device memory of the current device. */
+ncsim_status ncsim_device_info(int32_t* sm_count, uint64_t* free_bytes, uint64_t* total_bytes);
+
+/* ======================================================================
+ * 1. State operations (the QuantumState<C64> boundary)
+ * ====================================================================== */
+
+/* |0...0> on n qubits (StateVector::zero_state, vector.rs:25). n <= 33 for
+ * C128 and n <= 34 for C64 (device memory bound; the reference caps at 30,
+ * vector.rs:30).  Fails with NCSIM_ERR_OUT_OF_MEMORY when it does not fit. */
+ncsim_status ncsim_sv_create(uint32_t n, int32_t precision, ncsim_state** out);
+/* Frees the handle and its device memory (Drop). */
+ncsim_status ncsim_sv_destroy(ncsim_state* s);
+/* A device-to-device copy (Clone, vector.rs:15): needs a second state's memory. */
+ncsim_status ncsim_sv_clone(const ncsim_state* s, ncsim_state** out);
+/* Register size (QuantumState::num_qubits, mod.rs:46) and storage precision. */
+ncsim_status ncsim_sv_num_qubits(const ncsim_state* s, uint32_t* n);
+ncsim_status ncsim_sv_precision(const ncsim_state* s, int32_t* precision);
+/* |x> (StateVector::basis_state, vector.rs:29-34). */
+ncsim_status ncsim_sv_set_basis(ncsim_state* s, uint64_t index);
+/* |+>^n with amplitude sqrt2_pow(-n) (StateVector::plus_state, vector.rs:36-42). */
+ncsim_status ncsim_sv_set_plus(ncsim_state* s);
+/* From 2^n interleaved complex128 host amplitudes (StateVector::from_amplitudes, vector.rs:44-52). */
+ncsim_status ncsim_sv_set_amplitudes(ncsim_state* s, const double* amps, uint64_t len);
+/* All 2^n amplitudes to host memory as complex128 (to_vector, vector.rs:542-544). */
+ncsim_status ncsim_sv_get_amplitudes(const ncsim_state* s, double* amps, uint64_t len);
+/* One amplitude <x|psi> (QuantumState::amplitude, vector.rs:408-410). */
+ncsim_status ncsim_sv_get_amplitude(const ncsim_state* s, uint64_t index, double* re_im);
+/* count amplitudes at the given indices (amplitude called in a loop). */
+ncsim_status ncsim_sv_gather_amplitudes(const ncsim_state* s, const uint64_t* indices, uint64_t count, double* out);
+
+/* Dense 2^k x 2^k complex128 matrix on qubits (StateVector::apply_matrix,
+ * vector.rs:67-93).  k <= 6.  Exact-zero entries contribute nothing, as in
+ * the reference's row-sparse product. */
+ncsim_status ncsim_sv_apply_matrix(ncsim_state* s, const uint32_t* qubits, uint32_t k, const double* matrix);
+/* Monomial gate given by its basis images (StateVector::apply_monomial,
+ * vector.rs:96-139): U|x> = phase[x] |image[x]> over the local index x.
+ * image must be a permutation of 0..2^k; phase is complex128.  Diagonal
+ * tables (image[x] == x) touch only amplitudes whose phase is not exactly 1.
+ * k <= 10. */
+ncsim_status ncsim_sv_apply_monomial(ncsim_state* s, const uint32_t* qubits, uint32_t k, const uint64_t* image,
+                                     const double* phase);
+/* Diagonal(PhasePoly) evaluated from each basis index (gate.rs:557 with
+ * phasepoly.rs:670-678): amplitude x is multiplied by
+ *   scalar * exp(2 pi i f(x) / 2^bits),  f(x) = constant + sum_t coeff[t] * prod_{l in t} parity(l . x)
+ * over the local index x of `qubits`.  Term t owns parity masks
+ * parities[term_start[t] .. term_start[t+1]) (masks over the k local
+ * variables); term_start has nterms+1 entries.  1 <= bits <= 32, any k <= n.
+ * The scalar is the exact phasor sqrt2^s2 * exp(2 pi i sphase / 2^sbits).
+ * Amplitudes whose factor is exactly 1, and exact zeros, are not rewritten. */
+ncsim_status ncsim_sv_apply_phasepoly(ncsim_state* s, const uint32_t* qubits, uint32_t k, uint32_t bits,
+                                      uint64_t constant, uint32_t nterms, const uint32_t* term_start,
+                                      const uint64_t* parities, const uint64_t* coeffs, int32_t scalar_s2,
+                                      uint64_t scalar_phase, uint32_t scalar_bits);
+/* psi <- P psi for P = i^phase X^x Z^z over the register (vector.rs:143-164). */
+ncsim_status ncsim_sv_apply_pauli(ncsim_state* s, uint64_t x, uint64_t z, uint32_t phase);
+/* <psi|psi> as complex (imaginary part 0) (vector.rs:397-406), FP64 reduction. */
+ncsim_status ncsim_sv_norm_sq(const ncsim_state* s, double* re_im);
+/* <psi|P|psi> (vector.rs:412-429), FP64 reduction. */
+ncsim_status ncsim_sv_expectation(const ncsim_state* s, uint64_t x, uint64_t z, uint32_t phase, double* re_im);
+/* <psi|P|psi> and <psi|psi> in one pass (what QuantumState::measure reads, mod.rs:119-120). */
+ncsim_status ncsim_sv_measure_stats(const ncsim_state* s, uint64_t x, uint64_t z, uint32_t phase,
+                                    double* expectation_re_im, double* norm_sq);
+/* <a|b> (vector.rs:431-443). Registers must have equal size. */
+ncsim_status ncsim_sv_inner(const ncsim_state* a, const ncsim_state* b, double* re_im);
+/* psi <- (1 + (-1)^outcome P)/2 psi for Hermitian P; writes the branch weight
+ * <psi|psi> after projection (vector.rs:445-479), projection and norm fused
+ * in one pass. */
+ncsim_status ncsim_sv_project(ncsim_state* s, uint64_t x, uint64_t z, uint32_t phase, int32_t outcome,
+                              double* weight_re_im);
+/* psi <- c psi (vector.rs:481-488). */
+ncsim_status ncsim_sv_scale(ncsim_state* s, double re, double im);
+/* Born sampling in one pass (StateVector::sample, vector.rs:494-540): the
+ * caller draws the shots' uniforms u[k] in [0,1) (rng.gen::<f64>(), in shot
+ * order); shot k is the basis index whose cumulative weight interval holds
+ * u[k] * total.  Zero-weight indices are never returned.  Fails with
+ * NCSIM_ERR_ZERO_STATE when the state vanished. */
+ncsim_status ncsim_sv_sample(const ncsim_state* s, const double* uniforms, uint64_t shots, uint64_t* out);
+/* psi (x) phi with psi on the low qubits (StateVector::kron, vector.rs:168-188). */
+ncsim_status ncsim_sv_kron(const ncsim_state* a, const ncsim_state* b, ncsim_state** out);
+/* Waits for the state's queued device work. */
+ncsim_status ncsim_sv_synchronize(const ncsim_state* s);
+/* Device time on the state's stream: start records an event; stop records a
+ * second one, waits for it and writes the milliseconds between them. */
+ncsim_status ncsim_sv_timer_start(ncsim_state* s);
+ncsim_status ncsim_sv_timer_stop(ncsim_state* s, double* milliseconds);
+/* One FP64 pass over two registers of equal size and any precisions:
+ * <a|b>, <a|a>, <b|b> and max_i |a_i - b_i|, for infidelity
+ * 1 - |<a|b>|^2 / (<a|a><b|b>) and the largest amplitude error. */
+ncsim_status ncsim_sv_compare(const ncsim_state* a, const ncsim_state* b, double* inner_re_im, double* norm_a,
+                              double* norm_b, double* max_abs_diff);
+
+/* Launch profiler: while enabled, every kernel launched for the state is
+ * bracketed by CUDA events on the state's stream.  Reading waits for the
+ * stream and returns, per kernel class, the launch count, the summed device
+ * time and the summed algorithmic bytes (read + written amplitudes in the
+ * 32-byte sectors an operation changes).  Enabling clears earlier records. */
+typedef struct ncsim_kernel_stat {
+  char name[32];
+  uint64_t launches;
+  double milliseconds;
+  double bytes;
+} ncsim_kernel_stat;
+ncsim_status ncsim_sv_profile_enable(ncsim_state* s, int32_t enable);
+ncsim_status ncsim_sv_profile_read(ncsim_state* s, ncsim_kernel_stat* out, uint32_t cap, uint32_t* count);
+
+/* ======================================================================
+ * 2. Host mirror of the reference interface (C++), and the GPU-only forms
+ * ====================================================================== */
+
+/* rand 0.8 StdRng (ChaCha12) seeded as StdRng::seed_from_u64. */
+ncsim_status ncsim_rng_new(uint64_t seed, ncsim_rng** out);
+ncsim_status ncsim_rng_free(ncsim_rng* r);
+ncsim_status ncsim_rng_next_u64(ncsim_rng* r, uint64_t* out);
+ncsim_status ncsim_rng_next_u32(ncsim_rng* r, uint32_t* out);
+ncsim_status ncsim_rng_gen_f64(ncsim_rng* r, double* out);
+ncsim_status ncsim_rng_gen_range(ncsim_rng* r, uint64_t lo, uint64_t hi, uint64_t* out);
+
+/* Circuit::parse (src/circuit.rs:459-565), plus DIAG(...) / MONOMIAL(...)
+ * lines for the reference's Diagonal and Monomial gates. */
+ncsim_status ncsim_circuit_parse(const char* text, ncsim_circuit** out);
+ncsim_status ncsim_circuit_free(ncsim_circuit* c);
+ncsim_status ncsim_circuit_info(const ncsim_circuit* c, uint32_t* num_qubits, uint64_t* num_ops, uint64_t* num_gates,
+                                uint64_t* num_measurements);
+/* The circuit in text form (circuit.rs:693-728); *len receives the length
+ * without the terminating zero, written only when cap > len. */
+ncsim_status ncsim_circuit_to_text(const ncsim_circuit* c, char* buf, size_t cap, size_t* len);
+
+/* Seeded synthetic workloads (see DESIGN.md for their definitions).
+ * Random layer family: per layer one of {H, S, T, SQRT_X, RZ(theta)} on every
+ * qubit, then CZ on a random perfect matching (optionally followed by
+ * DEPOLARIZE2(noise_p)); Z measurements of qubits [m_lo, m_hi) at the end. */
+ncsim_status ncsim_workload_random_circuit(uint32_t n, uint32_t depth, uint64_t seed, double noise_p, uint32_t m_lo,
+                                           uint32_t m_hi, ncsim_circuit** out);
+/* The same family drawn from the caller's generator, which keeps its state
+ * (a noisy trajectory draws its circuit and then its noise and measurement
+ * outcomes from one StdRng). */
+ncsim_status ncsim_workload_random_circuit_rng(ncsim_rng* rng, uint32_t n, uint32_t depth, double noise_p,
+                                               uint32_t m_lo, uint32_t m_hi, ncsim_circuit** out);
+/* Permutation/diagonal family: H on min(16, n) qubits, then `gates` gates
+ * from {CX, CCX, CCZ, DIAG over the register, MONOMIAL on 8 qubits}. */
+ncsim_status ncsim_workload_reversible_circuit(uint32_t n, uint32_t gates, uint64_t seed, ncsim_circuit** out);
+
+/* A gate from one text token ("H", "RZ(0.5)", "PHASE(3,4)", "DIAG(...)",
+ * "MONOMIAL(...)") and its arity. */
+ncsim_status ncsim_gate_parse(const char* token, uint32_t arity_hint, ncsim_gate** out, uint32_t* arity);
+/* Gate::Unitary (gate.rs:427-428): a dense complex128 matrix on k qubits. */
+ncsim_status ncsim_gate_unitary(uint32_t k, const double* matrix, ncsim_gate** out);
+/* Gate::Pauli (gate.rs:417-418): i^phase X^x Z^z on k local qubits. */
+ncsim_status ncsim_gate_pauli(uint32_t k, uint64_t x, uint64_t z, uint32_t phase, ncsim_gate** out);
+ncsim_status ncsim_gate_free(ncsim_gate* g);
+
+/* Pauli::from_string(n, text) (pauli/mod.rs:349-414) as (x, z, phase). */
+ncsim_status ncsim_pauli_parse(const char* text, uint32_t n, uint64_t* x, uint64_t* z, uint32_t* phase);
+
+/* QuantumState::apply_gate through the gate's views (vector.rs:364-395). */
+ncsim_status ncsim_sv_apply_gate(ncsim_state* s, const ncsim_gate* g, const uint32_t* qubits, uint32_t k);
+/* QuantumState::measure (mod.rs:113-131): one pass for <P> and <psi|psi>, a
+ * draw only when the outcome is uncertain, then the fused projection. */
+ncsim_status ncsim_sv_measure(ncsim_state* s, uint64_t x, uint64_t z, uint32_t phase, ncsim_rng* rng,
+                              int32_t* outcome);
+/* QuantumState::run (mod.rs:168-183): the record (one byte per measurement,
+ * 1 = eigenvalue -1) is written to rec (cap bytes); *len receives its length. */
+ncsim_status ncsim_sv_run(ncsim_state* s, const ncsim_circuit* c, ncsim_rng* rng, uint8_t* rec, size_t cap,
+                          size_t* len);
+/* StateVector::sample with draws from rng (vector.rs:494-540). */
+ncsim_status ncsim_sv_sample_rng(const ncsim_state* s, ncsim_rng* rng, uint64_t shots, uint64_t* out);
+/* QuantumState::normalize (mod.rs:220-233) and probability (mod.rs:104-108). */
+ncsim_status ncsim_sv_normalize(ncsim_state* s);
+ncsim_status ncsim_sv_probability(const ncsim_state* s, uint64_t index, double* out);
+/* QuantumState::expectation_sum (mod.rs:93-101): sum_k c_k <P_k>, summed pairwise. */
+ncsim_status ncsim_sv_expectation_sum(const ncsim_state* s, uint64_t count, const uint64_t* x, const uint64_t* z,
+                                      const uint32_t* phase, const double* coeffs, double* re_im);
+
+/* ---- precision form: fused k<=5 unitaries on tensor cores (C64 states) ----
+ * Runs of gates are fused on the host (FP64) into unitaries of at most
+ * max_fuse qubits, grouped into passes over a qubit window held in shared
+ * memory, and applied as BF16x3 split-precision complex GEMMs (tcgen05, FP32
+ * accumulation) to FP32 amplitudes.  Measurements, resets and noise go
+ * through the plain kernels with FP64 reductions.  Same record semantics as
+ * ncsim_sv_run. */
+typedef struct ncsim_fused_stats {
+  uint64_t source_gates;     /* Op::Gate count of the circuit */
+  uint64_t fused_unitaries;  /* unitaries after fusion */
+  uint64_t passes;           /* HBM read+write passes over the state */
+  uint64_t remap_passes;     /* of which qubit-permutation passes */
+  uint64_t gemm_launches;    /* tensor-core kernel launches */
+} ncsim_fused_stats;
+ncsim_status ncsim_sv_run_fused(ncsim_state* s, const ncsim_circuit* c, ncsim_rng* rng, uint32_t max_fuse,
+                                uint8_t* rec, size_t cap, size_t* len, ncsim_fused_stats* stats);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* NCSIM_CUDA_H */

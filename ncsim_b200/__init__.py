@@ -1,0 +1,591 @@
+"""ncsim_b200 — a B200 dense statevector engine behind ncsim's ``QuantumState<C64>`` interface.
+
+Python binding (ctypes) of ``libncsim_cuda.so``.  The names follow the
+reference's trait and types (``src/state/mod.rs:41-234``,
+``src/state/vector.rs``, ``src/gate.rs``, ``src/circuit.rs``): a
+``GpuStateVector`` offers ``apply_gate``, ``run``, ``amplitude``,
+``expectation``, ``expectation_sum``, ``norm_sq``, ``inner``, ``project``,
+``scale``, ``measure``, ``sample``, ``to_vector``, ``normalize``,
+``probability`` and ``tensor``.
+
+There is no CPU fallback: every operation runs the CUDA kernels of the
+library, and importing this module fails loudly when the library is absent.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+from typing import Iterable, Sequence
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "libncsim_cuda.so")
+
+C128 = 0
+C64 = 1
+
+# status codes (include/ncsim_cuda.h), mirroring SimError (src/error.rs:7-42)
+STATUS_NAMES = {
+    1: "Unsupported",
+    2: "QubitOutOfRange",
+    3: "Arity",
+    4: "DuplicateQubit",
+    5: "NotRepresentable",
+    6: "ZeroState",
+    7: "Parse",
+    8: "Invalid",
+    9: "Device",
+    10: "OutOfMemory",
+}
+
+
+class SimError(RuntimeError):
+    """An error status of the engine; ``kind`` names the SimError variant."""
+
+    def __init__(self, status: int, message: str):
+        self.status = status
+        self.kind = STATUS_NAMES.get(status, f"status{status}")
+        super().__init__(f"{self.kind}: {message}")
+
+
+_lib = None
+
+_P = C.POINTER
+_u32, _u64, _i32, _dbl, _vp = C.c_uint32, C.c_uint64, C.c_int32, C.c_double, C.c_void_p
+
+_SIGNATURES = {
+    "ncsim_last_error": (C.c_char_p, []),
+    "ncsim_abi_version": (_i32, []),
+    "ncsim_device_info": (_i32, [_P(_i32), _P(_u64), _P(_u64)]),
+    "ncsim_sv_create": (_i32, [_u32, _i32, _P(_vp)]),
+    "ncsim_sv_destroy": (_i32, [_vp]),
+    "ncsim_sv_clone": (_i32, [_vp, _P(_vp)]),
+    "ncsim_sv_num_qubits": (_i32, [_vp, _P(_u32)]),
+    "ncsim_sv_precision": (_i32, [_vp, _P(_i32)]),
+    "ncsim_sv_set_basis": (_i32, [_vp, _u64]),
+    "ncsim_sv_set_plus": (_i32, [_vp]),
+    "ncsim_sv_set_amplitudes": (_i32, [_vp, _P(_dbl), _u64]),
+    "ncsim_sv_get_amplitudes": (_i32, [_vp, _P(_dbl), _u64]),
+    "ncsim_sv_get_amplitude": (_i32, [_vp, _u64, _P(_dbl)]),
+    "ncsim_sv_gather_amplitudes": (_i32, [_vp, _P(_u64), _u64, _P(_dbl)]),
+    "ncsim_sv_apply_matrix": (_i32, [_vp, _P(_u32), _u32, _P(_dbl)]),
+    "ncsim_sv_apply_monomial": (_i32, [_vp, _P(_u32), _u32, _P(_u64), _P(_dbl)]),
+    "ncsim_sv_apply_phasepoly": (
+        _i32,
+        [_vp, _P(_u32), _u32, _u32, _u64, _u32, _P(_u32), _P(_u64), _P(_u64), _i32, _u64, _u32],
+    ),
+    "ncsim_sv_apply_pauli": (_i32, [_vp, _u64, _u64, _u32]),
+    "ncsim_sv_norm_sq": (_i32, [_vp, _P(_dbl)]),
+    "ncsim_sv_expectation": (_i32, [_vp, _u64, _u64, _u32, _P(_dbl)]),
+    "ncsim_sv_measure_stats": (_i32, [_vp, _u64, _u64, _u32, _P(_dbl), _P(_dbl)]),
+    "ncsim_sv_inner": (_i32, [_vp, _vp, _P(_dbl)]),
+    "ncsim_sv_project": (_i32, [_vp, _u64, _u64, _u32, _i32, _P(_dbl)]),
+    "ncsim_sv_scale": (_i32, [_vp, _dbl, _dbl]),
+    "ncsim_sv_sample": (_i32, [_vp, _P(_dbl), _u64, _P(_u64)]),
+    "ncsim_sv_kron": (_i32, [_vp, _vp, _P(_vp)]),
+    "ncsim_sv_synchronize": (_i32, [_vp]),
+    "ncsim_rng_new": (_i32, [_u64, _P(_vp)]),
+    "ncsim_rng_free": (_i32, [_vp]),
+    "ncsim_rng_next_u64": (_i32, [_vp, _P(_u64)]),
+    "ncsim_rng_next_u32": (_i32, [_vp, _P(_u32)]),
+    "ncsim_rng_gen_f64": (_i32, [_vp, _P(_dbl)]),
+    "ncsim_rng_gen_range": (_i32, [_vp, _u64, _u64, _P(_u64)]),
+    "ncsim_circuit_parse": (_i32, [C.c_char_p, _P(_vp)]),
+    "ncsim_circuit_free": (_i32, [_vp]),
+    "ncsim_circuit_info": (_i32, [_vp, _P(_u32), _P(_u64), _P(_u64), _P(_u64)]),
+    "ncsim_circuit_to_text": (_i32, [_vp, C.c_char_p, C.c_size_t, _P(C.c_size_t)]),
+    "ncsim_workload_random_circuit": (_i32, [_u32, _u32, _u64, _dbl, _u32, _u32, _P(_vp)]),
+    "ncsim_workload_random_circuit_rng": (_i32, [_vp, _u32, _u32, _dbl, _u32, _u32, _P(_vp)]),
+    "ncsim_workload_reversible_circuit": (_i32, [_u32, _u32, _u64, _P(_vp)]),
+    "ncsim_gate_parse": (_i32, [C.c_char_p, _u32, _P(_vp), _P(_u32)]),
+    "ncsim_gate_unitary": (_i32, [_u32, _P(_dbl), _P(_vp)]),
+    "ncsim_gate_pauli": (_i32, [_u32, _u64, _u64, _u32, _P(_vp)]),
+    "ncsim_gate_free": (_i32, [_vp]),
+    "ncsim_pauli_parse": (_i32, [C.c_char_p, _u32, _P(_u64), _P(_u64), _P(_u32)]),
+    "ncsim_sv_apply_gate": (_i32, [_vp, _vp, _P(_u32), _u32]),
+    "ncsim_sv_measure": (_i32, [_vp, _u64, _u64, _u32, _vp, _P(_i32)]),
+    "ncsim_sv_run": (_i32, [_vp, _vp, _vp, _P(C.c_uint8), C.c_size_t, _P(C.c_size_t)]),
+    "ncsim_sv_sample_rng": (_i32, [_vp, _vp, _u64, _P(_u64)]),
+    "ncsim_sv_normalize": (_i32, [_vp]),
+    "ncsim_sv_probability": (_i32, [_vp, _u64, _P(_dbl)]),
+    "ncsim_sv_expectation_sum": (_i32, [_vp, _u64, _P(_u64), _P(_u64), _P(_u32), _P(_dbl), _P(_dbl)]),
+    "ncsim_sv_run_fused": (_i32, [_vp, _vp, _vp, _u32, _P(C.c_uint8), C.c_size_t, _P(C.c_size_t), _vp]),
+    "ncsim_sv_timer_start": (_i32, [_vp]),
+    "ncsim_sv_timer_stop": (_i32, [_vp, _P(_dbl)]),
+    "ncsim_sv_compare": (_i32, [_vp, _vp, _P(_dbl), _P(_dbl), _P(_dbl), _P(_dbl)]),
+    "ncsim_sv_profile_enable": (_i32, [_vp, _i32]),
+    "ncsim_sv_profile_read": (_i32, [_vp, _vp, _u32, _P(_u32)]),
+}
+
+
+class KernelStat(C.Structure):
+    _fields_ = [("name", C.c_char * 32), ("launches", _u64), ("milliseconds", _dbl), ("bytes", _dbl)]
+
+
+def lib():
+    """The loaded C library (raises if it has not been built)."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise ImportError(
+                f"{LIB_PATH} is missing: build it with `python -m ncsim_b200.build` "
+                "(there is no CPU fallback)"
+            )
+        L = C.CDLL(LIB_PATH)
+        for name, (res, args) in _SIGNATURES.items():
+            f = getattr(L, name)
+            f.restype = res
+            f.argtypes = args
+        _lib = L
+    return _lib
+
+
+def _check(status: int) -> None:
+    if status != 0:
+        raise SimError(status, lib().ncsim_last_error().decode(errors="replace"))
+
+
+def _dp(a: np.ndarray):
+    return a.ctypes.data_as(_P(_dbl))
+
+
+def _u32s(v: Sequence[int]):
+    return (_u32 * max(1, len(v)))(*v)
+
+
+# ---------------------------------------------------------------------------
+# Paulis: (x, z, phase) with P = i^phase X^x Z^z (src/pauli/ops.rs:5)
+# ---------------------------------------------------------------------------
+class Pauli:
+    """A Pauli operator on ``n`` qubits in ncsim's stored form."""
+
+    __slots__ = ("n", "x", "z", "phase")
+
+    def __init__(self, n: int, x: int = 0, z: int = 0, phase: int = 0):
+        self.n, self.x, self.z, self.phase = n, x, z, phase & 3
+
+    @classmethod
+    def from_string(cls, n: int, text: str) -> "Pauli":
+        """``Pauli::from_string`` (src/pauli/mod.rs:349-351)."""
+        x, z, ph = _u64(), _u64(), _u32()
+        _check(lib().ncsim_pauli_parse(text.encode(), n, C.byref(x), C.byref(z), C.byref(ph)))
+        return cls(n, x.value, z.value, ph.value)
+
+    @classmethod
+    def z_on(cls, n: int, q: int) -> "Pauli":
+        return cls(n, 0, 1 << q, 0)
+
+    def is_hermitian(self) -> bool:
+        return ((self.phase & 1) == 1) == (bin(self.x & self.z).count("1") & 1 == 1)
+
+    def __repr__(self) -> str:
+        return f"Pauli(n={self.n}, x={self.x:#x}, z={self.z:#x}, phase={self.phase})"
+
+
+# ---------------------------------------------------------------------------
+class StdRng:
+    """rand 0.8 ``StdRng`` seeded with ``seed_from_u64`` (C++ in the library)."""
+
+    def __init__(self, seed: int):
+        h = _vp()
+        _check(lib().ncsim_rng_new(seed, C.byref(h)))
+        self._h = h
+
+    def __del__(self):
+        h = getattr(self, "_h", None)
+        if h and _lib is not None:
+            _lib.ncsim_rng_free(h)
+
+    def next_u64(self) -> int:
+        v = _u64()
+        _check(lib().ncsim_rng_next_u64(self._h, C.byref(v)))
+        return v.value
+
+    def next_u32(self) -> int:
+        v = _u32()
+        _check(lib().ncsim_rng_next_u32(self._h, C.byref(v)))
+        return v.value
+
+    def gen_f64(self) -> float:
+        v = _dbl()
+        _check(lib().ncsim_rng_gen_f64(self._h, C.byref(v)))
+        return v.value
+
+    def gen_range(self, lo: int, hi: int) -> int:
+        v = _u64()
+        _check(lib().ncsim_rng_gen_range(self._h, lo, hi, C.byref(v)))
+        return v.value
+
+
+class Gate:
+    """A gate (``src/gate.rs:356-431``): a text token, a dense unitary or a Pauli."""
+
+    def __init__(self, handle, arity: int, label: str):
+        self._h, self.arity, self.label = handle, arity, label
+
+    @classmethod
+    def parse(cls, token: str, arity: int = 0) -> "Gate":
+        """A gate from its circuit-text token: ``H``, ``RZ(0.5)``, ``CCZ``, ``DIAG(...)``.
+
+        ``arity`` is the qubit count of DIAG/MONOMIAL tokens (other gates know theirs).
+        """
+        h, k = _vp(), _u32()
+        _check(lib().ncsim_gate_parse(token.encode(), arity, C.byref(h), C.byref(k)))
+        return cls(h, k.value, token)
+
+    @classmethod
+    def unitary(cls, m: np.ndarray) -> "Gate":
+        """``Gate::Unitary``: a dense 2^k x 2^k matrix, row-major, little-endian."""
+        m = np.ascontiguousarray(np.asarray(m, dtype=np.complex128))
+        k = int(round(np.log2(m.shape[0])))
+        h = _vp()
+        _check(lib().ncsim_gate_unitary(k, _dp(m.view(np.float64)), C.byref(h)))
+        return cls(h, k, f"UNITARY[{k}]")
+
+    @classmethod
+    def pauli(cls, p: Pauli) -> "Gate":
+        """``Gate::Pauli`` on ``p.n`` local qubits."""
+        h = _vp()
+        _check(lib().ncsim_gate_pauli(p.n, p.x, p.z, p.phase, C.byref(h)))
+        return cls(h, p.n, "PAULI")
+
+    def __del__(self):
+        h = getattr(self, "_h", None)
+        if h and _lib is not None:
+            _lib.ncsim_gate_free(h)
+
+    def __repr__(self) -> str:
+        return f"Gate({self.label})"
+
+
+class Circuit:
+    """``Circuit`` (src/circuit.rs:151): parsed from ncsim's text format."""
+
+    def __init__(self, handle):
+        self._h = handle
+
+    @classmethod
+    def parse(cls, text: str) -> "Circuit":
+        h = _vp()
+        _check(lib().ncsim_circuit_parse(text.encode(), C.byref(h)))
+        return cls(h)
+
+    @classmethod
+    def random_layers(cls, n: int, depth: int, seed: int, noise_p: float = 0.0, m_lo: int = 0, m_hi: int = 0):
+        """The seeded random layer family (H/S/T/SQRT_X/RZ on every qubit, CZ matching)."""
+        h = _vp()
+        _check(lib().ncsim_workload_random_circuit(n, depth, seed, noise_p, m_lo, m_hi, C.byref(h)))
+        return cls(h)
+
+    @classmethod
+    def random_layers_from(cls, rng: "StdRng", n: int, depth: int, noise_p: float = 0.0, m_lo: int = 0, m_hi: int = 0):
+        """The random layer family drawn from ``rng``, which keeps its state."""
+        h = _vp()
+        _check(lib().ncsim_workload_random_circuit_rng(rng._h, n, depth, noise_p, m_lo, m_hi, C.byref(h)))
+        return cls(h)
+
+    @classmethod
+    def reversible(cls, n: int, gates: int, seed: int) -> "Circuit":
+        """The seeded permutation/diagonal family (CX, CCX, CCZ, DIAG, MONOMIAL)."""
+        h = _vp()
+        _check(lib().ncsim_workload_reversible_circuit(n, gates, seed, C.byref(h)))
+        return cls(h)
+
+    def __del__(self):
+        h = getattr(self, "_h", None)
+        if h and _lib is not None:
+            _lib.ncsim_circuit_free(h)
+
+    def _info(self):
+        nq, no, ng, nm = _u32(), _u64(), _u64(), _u64()
+        _check(lib().ncsim_circuit_info(self._h, C.byref(nq), C.byref(no), C.byref(ng), C.byref(nm)))
+        return nq.value, no.value, ng.value, nm.value
+
+    @property
+    def num_qubits(self) -> int:
+        return self._info()[0]
+
+    @property
+    def num_gates(self) -> int:
+        return self._info()[2]
+
+    @property
+    def num_measurements(self) -> int:
+        return self._info()[3]
+
+    def to_text(self) -> str:
+        n = C.c_size_t()
+        _check(lib().ncsim_circuit_to_text(self._h, None, 0, C.byref(n)))
+        buf = C.create_string_buffer(n.value + 1)
+        _check(lib().ncsim_circuit_to_text(self._h, buf, n.value + 1, C.byref(n)))
+        return buf.value.decode()
+
+
+class FusedStats(C.Structure):
+    _fields_ = [
+        ("source_gates", _u64),
+        ("fused_unitaries", _u64),
+        ("passes", _u64),
+        ("remap_passes", _u64),
+        ("gemm_launches", _u64),
+    ]
+
+
+def _complex(buf) -> complex:
+    return complex(buf[0], buf[1])
+
+
+class GpuStateVector:
+    """A dense state vector in B200 memory: the drop-in for ``StateVector<C64>``.
+
+    ``precision`` is ``C128`` (complex128, the drop-in) or ``C64`` (complex64,
+    the storage of the fused precision form).
+    """
+
+    BACKEND = "GpuStateVector"
+
+    def __init__(self, n: int, precision: int = C128, _handle=None):
+        if _handle is None:
+            h = _vp()
+            _check(lib().ncsim_sv_create(n, precision, C.byref(h)))
+            _handle = h
+        self._h = _handle
+        self.n = n
+        self.precision = precision
+
+    # ---- constructors (vector.rs:25-52) ----
+    @classmethod
+    def zero_state(cls, n: int, precision: int = C128) -> "GpuStateVector":
+        return cls(n, precision)
+
+    @classmethod
+    def basis_state(cls, n: int, index: int, precision: int = C128) -> "GpuStateVector":
+        s = cls(n, precision)
+        _check(lib().ncsim_sv_set_basis(s._h, index))
+        return s
+
+    @classmethod
+    def plus_state(cls, n: int, precision: int = C128) -> "GpuStateVector":
+        s = cls(n, precision)
+        _check(lib().ncsim_sv_set_plus(s._h))
+        return s
+
+    @classmethod
+    def from_amplitudes(cls, amps: np.ndarray, precision: int = C128) -> "GpuStateVector":
+        amps = np.asarray(amps, dtype=np.complex128)
+        n = int(amps.size).bit_length() - 1
+        if (1 << n) != amps.size:
+            raise SimError(8, f"{amps.size} amplitudes for {n} qubits")
+        s = cls(n, precision)
+        s.set_amplitudes(amps)
+        return s
+
+    def __del__(self):
+        h = getattr(self, "_h", None)
+        if h and _lib is not None:
+            _lib.ncsim_sv_destroy(h)
+            self._h = None
+
+    def clone(self) -> "GpuStateVector":
+        h = _vp()
+        _check(lib().ncsim_sv_clone(self._h, C.byref(h)))
+        return GpuStateVector(self.n, self.precision, h)
+
+    def num_qubits(self) -> int:
+        return self.n
+
+    def set_amplitudes(self, amps: np.ndarray) -> None:
+        b = np.ascontiguousarray(np.asarray(amps, dtype=np.complex128)).view(np.float64)
+        _check(lib().ncsim_sv_set_amplitudes(self._h, _dp(b), 1 << self.n))
+
+    def to_vector(self) -> np.ndarray:
+        """All amplitudes as complex128 (``to_vector``, vector.rs:542)."""
+        b = np.empty(2 << self.n, dtype=np.float64)
+        _check(lib().ncsim_sv_get_amplitudes(self._h, _dp(b), 1 << self.n))
+        return b.view(np.complex128)
+
+    def amplitude(self, index: int) -> complex:
+        o = (_dbl * 2)()
+        _check(lib().ncsim_sv_get_amplitude(self._h, index, o))
+        return _complex(o)
+
+    def amplitudes_at(self, indices: Iterable[int]) -> np.ndarray:
+        idx = np.ascontiguousarray(np.asarray(list(indices), dtype=np.uint64))
+        out = np.empty(2 * idx.size, dtype=np.float64)
+        _check(lib().ncsim_sv_gather_amplitudes(self._h, idx.ctypes.data_as(_P(_u64)), idx.size, _dp(out)))
+        return out.view(np.complex128)
+
+    # ---- gates ----
+    def apply_gate(self, gate: Gate, qubits: Sequence[int]) -> None:
+        """``apply_gate`` through the gate's views (vector.rs:364-395)."""
+        _check(lib().ncsim_sv_apply_gate(self._h, gate._h, _u32s(qubits), len(qubits)))
+
+    def apply_matrix(self, m: np.ndarray, qubits: Sequence[int]) -> None:
+        m = np.ascontiguousarray(np.asarray(m, dtype=np.complex128))
+        _check(lib().ncsim_sv_apply_matrix(self._h, _u32s(qubits), len(qubits), _dp(m.view(np.float64))))
+
+    def apply_monomial(self, qubits: Sequence[int], image: Sequence[int], phase: np.ndarray) -> None:
+        img = np.ascontiguousarray(np.asarray(image, dtype=np.uint64))
+        ph = np.ascontiguousarray(np.asarray(phase, dtype=np.complex128))
+        _check(
+            lib().ncsim_sv_apply_monomial(
+                self._h, _u32s(qubits), len(qubits), img.ctypes.data_as(_P(_u64)), _dp(ph.view(np.float64))
+            )
+        )
+
+    def apply_phasepoly(self, qubits, bits, constant, terms, scalar=(0, 0, 0)) -> None:
+        """Diagonal(PhasePoly) from the bit index; ``terms`` = [(coeff, [parity masks])]."""
+        starts, pars, coeffs = [0], [], []
+        for c, ps in terms:
+            pars.extend(ps)
+            starts.append(len(pars))
+            coeffs.append(c)
+        st = (_u32 * len(starts))(*starts)
+        pa = (_u64 * max(1, len(pars)))(*pars)
+        co = (_u64 * max(1, len(coeffs)))(*coeffs)
+        _check(
+            lib().ncsim_sv_apply_phasepoly(
+                self._h, _u32s(qubits), len(qubits), bits, constant, len(coeffs), st, pa, co, *scalar
+            )
+        )
+
+    def apply_pauli(self, p: Pauli) -> None:
+        _check(lib().ncsim_sv_apply_pauli(self._h, p.x, p.z, p.phase))
+
+    # ---- readouts ----
+    def norm_sq(self) -> complex:
+        o = (_dbl * 2)()
+        _check(lib().ncsim_sv_norm_sq(self._h, o))
+        return _complex(o)
+
+    def expectation(self, p: Pauli) -> complex:
+        if p.n != self.n:
+            raise SimError(8, "expectation: operator on the wrong register")
+        o = (_dbl * 2)()
+        _check(lib().ncsim_sv_expectation(self._h, p.x, p.z, p.phase, o))
+        return _complex(o)
+
+    def measure_stats(self, p: Pauli):
+        e = (_dbl * 2)()
+        nn = _dbl()
+        _check(lib().ncsim_sv_measure_stats(self._h, p.x, p.z, p.phase, e, C.byref(nn)))
+        return _complex(e), nn.value
+
+    def expectation_sum(self, terms: Sequence[tuple[complex, Pauli]]) -> complex:
+        k = len(terms)
+        xs = (_u64 * max(1, k))(*[p.x for _, p in terms])
+        zs = (_u64 * max(1, k))(*[p.z for _, p in terms])
+        ph = (_u32 * max(1, k))(*[p.phase for _, p in terms])
+        cs = np.array([[complex(c).real, complex(c).imag] for c, _ in terms] or [[0.0, 0.0]], dtype=np.float64)
+        o = (_dbl * 2)()
+        _check(lib().ncsim_sv_expectation_sum(self._h, k, xs, zs, ph, _dp(cs), o))
+        return _complex(o)
+
+    def inner(self, other: "GpuStateVector") -> complex:
+        o = (_dbl * 2)()
+        _check(lib().ncsim_sv_inner(self._h, other._h, o))
+        return _complex(o)
+
+    def project(self, p: Pauli, outcome: bool) -> complex:
+        o = (_dbl * 2)()
+        _check(lib().ncsim_sv_project(self._h, p.x, p.z, p.phase, int(bool(outcome)), o))
+        return _complex(o)
+
+    def scale(self, c: complex) -> None:
+        c = complex(c)
+        _check(lib().ncsim_sv_scale(self._h, c.real, c.imag))
+
+    def normalize(self) -> None:
+        _check(lib().ncsim_sv_normalize(self._h))
+
+    def probability(self, index: int) -> float:
+        o = _dbl()
+        _check(lib().ncsim_sv_probability(self._h, index, C.byref(o)))
+        return o.value
+
+    def measure(self, p: Pauli, rng: StdRng) -> bool:
+        o = _i32()
+        _check(lib().ncsim_sv_measure(self._h, p.x, p.z, p.phase, rng._h, C.byref(o)))
+        return bool(o.value)
+
+    def run(self, circuit: Circuit, rng: StdRng) -> list[bool]:
+        m = circuit.num_measurements
+        rec = (C.c_uint8 * max(1, m))()
+        ln = C.c_size_t()
+        _check(lib().ncsim_sv_run(self._h, circuit._h, rng._h, rec, m, C.byref(ln)))
+        return [bool(rec[i]) for i in range(ln.value)]
+
+    def run_fused(self, circuit: Circuit, rng: StdRng, max_fuse: int = 5):
+        m = circuit.num_measurements
+        rec = (C.c_uint8 * max(1, m))()
+        ln = C.c_size_t()
+        st = FusedStats()
+        _check(lib().ncsim_sv_run_fused(self._h, circuit._h, rng._h, max_fuse, rec, m, C.byref(ln), C.byref(st)))
+        return [bool(rec[i]) for i in range(ln.value)], st
+
+    def sample(self, rng: StdRng, shots: int) -> np.ndarray:
+        out = np.empty(shots, dtype=np.uint64)
+        _check(lib().ncsim_sv_sample_rng(self._h, rng._h, shots, out.ctypes.data_as(_P(_u64))))
+        return out
+
+    def sample_uniforms(self, u: np.ndarray) -> np.ndarray:
+        u = np.ascontiguousarray(u, dtype=np.float64)
+        out = np.empty(u.size, dtype=np.uint64)
+        _check(lib().ncsim_sv_sample(self._h, _dp(u), u.size, out.ctypes.data_as(_P(_u64))))
+        return out
+
+    def tensor(self, other: "GpuStateVector") -> "GpuStateVector":
+        h = _vp()
+        _check(lib().ncsim_sv_kron(self._h, other._h, C.byref(h)))
+        return GpuStateVector(self.n + other.n, self.precision, h)
+
+    kron = tensor
+
+    def synchronize(self) -> None:
+        _check(lib().ncsim_sv_synchronize(self._h))
+
+    def timer_start(self) -> None:
+        """Records a start event on the state's stream."""
+        _check(lib().ncsim_sv_timer_start(self._h))
+
+    def timer_stop(self) -> float:
+        """Device milliseconds since timer_start (waits for the stream)."""
+        ms = _dbl()
+        _check(lib().ncsim_sv_timer_stop(self._h, C.byref(ms)))
+        return ms.value
+
+    def compare(self, other: "GpuStateVector") -> dict:
+        """<a|b>, norms, infidelity and max amplitude difference, in one FP64 pass."""
+        inner = (_dbl * 2)()
+        na, nb_, mx = _dbl(), _dbl(), _dbl()
+        _check(lib().ncsim_sv_compare(self._h, other._h, inner, C.byref(na), C.byref(nb_), C.byref(mx)))
+        ip = _complex(inner)
+        return {
+            "inner": ip,
+            "norm_a": na.value,
+            "norm_b": nb_.value,
+            "infidelity": 1.0 - abs(ip) ** 2 / (na.value * nb_.value),
+            "max_abs_diff": mx.value,
+        }
+
+    # ---- launch profiler (CUDA events on the state's stream) ----
+    def profile(self, enable: bool = True) -> None:
+        """Start (clearing earlier records) or stop per-launch event timing."""
+        _check(lib().ncsim_sv_profile_enable(self._h, int(enable)))
+
+    def profile_read(self) -> dict:
+        """{kernel class: {"launches", "ms", "bytes"}} since profiling was enabled."""
+        arr = (KernelStat * 32)()
+        cnt = _u32()
+        _check(lib().ncsim_sv_profile_read(self._h, C.cast(arr, _vp), 32, C.byref(cnt)))
+        return {
+            arr[i].name.decode(): {"launches": arr[i].launches, "ms": arr[i].milliseconds, "bytes": arr[i].bytes}
+            for i in range(min(cnt.value, 32))
+        }
+
+
+def device_info() -> dict:
+    sm, fr, tot = _i32(), _u64(), _u64()
+    _check(lib().ncsim_device_info(C.byref(sm), C.byref(fr), C.byref(tot)))
+    return {"sm_count": sm.value, "free_bytes": fr.value, "total_bytes": tot.value}

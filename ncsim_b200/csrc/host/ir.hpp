@@ -1,0 +1,129 @@
+// Host-side circuit IR of the engine: the reference's gates, Paulis, phase
+// polynomials, noise channels and circuits (src/gate.rs, src/pauli/mod.rs,
+// src/phasepoly.rs, src/circuit.rs), each gate lowered once, at parse time,
+// to the kernel that applies it ("lowered op").
+#pragma once
+
+#include <cstdint>
+#include <string>
+#include <vector>
+
+#include "../engine.cuh"
+#include "../host_math.hpp"
+#include "rng.hpp"
+
+namespace ncsim {
+
+// i^phase X^x Z^z on n <= 64 qubits (src/pauli/mod.rs:81-87)
+struct PauliOp {
+  uint32_t n = 0;
+  uint64_t x = 0, z = 0;
+  uint32_t phase = 0;
+  bool hermitian() const { return ((phase & 1) == 1) == bool(__builtin_popcountll(x & z) & 1); }
+};
+// Pauli::from_string / Pauli::parse (src/pauli/mod.rs:344-414); n < 0 infers the size
+PauliOp parse_pauli(const std::string& text, int64_t n);
+
+// f(x) = constant + sum_t c_t prod_{l in t} [l . x] mod 2^bits over nvars
+// local variables (src/phasepoly.rs:536-545); terms kept as given
+struct PhasePolyIR {
+  uint32_t nvars = 0;
+  uint32_t bits = 1;
+  uint64_t constant = 0;
+  std::vector<std::vector<uint64_t>> parities;
+  std::vector<uint64_t> coeffs;
+  uint64_t eval(uint64_t x) const;
+};
+
+// U|x> = scalar zeta^{f(x)} |M x + shift> (src/gate.rs:24-37)
+struct MonomialIR {
+  uint32_t k = 0;
+  std::vector<uint64_t> rows;
+  uint64_t shift = 0;
+  PhasePolyIR phase;
+  Phase scalar;
+  bool affine_identity() const;
+};
+
+enum class GateKind : int {
+  I, X, Y, Z, H, S, Sdg, SqrtX, SqrtXdg, SqrtY, SqrtYdg, T, Tdg, Cx, Cy, Cz, Swap, Cs, Csdg, Ccz, Ccx,
+  Phase, CPhase, Rx, Ry, Rz, Diagonal, Monomial, Pauli, Unitary
+};
+
+struct GateIR {
+  GateKind kind = GateKind::I;
+  int64_t pk = 0;
+  uint32_t pbits = 1;
+  double theta = 0.0;
+  PhasePolyIR poly;
+  MonomialIR mono;
+  PauliOp pauli;
+  uint32_t uk = 0;
+  std::vector<CplxD> umat;
+  uint32_t arity() const;
+  std::string text() const;  // the circuit-text token
+};
+
+// What one kernel launch needs to apply a gate on given qubits.
+enum class LoweredKind : int { Nothing, Dense, Monomial, PhasePoly, Pauli };
+struct LoweredOp {
+  LoweredKind kind = LoweredKind::Nothing;
+  std::vector<uint32_t> qubits;
+  std::vector<CplxD> matrix;   // Dense (row-major) or the monomial phases
+  std::vector<uint32_t> image; // Monomial
+  PolyTerms poly;              // PhasePoly
+  uint64_t x = 0, z = 0;       // Pauli
+  uint32_t phase = 0;
+};
+
+// The gate's views in the reference's order (vector.rs:364-395): Pauli,
+// monomial, matrix.  Throws Error on arity or qubit problems.
+LoweredOp lower_gate(const GateIR& g, const std::vector<uint32_t>& qubits, uint32_t n);
+// Gate::matrix (gate.rs:670-747) for gates with a dense view
+std::vector<CplxD> gate_matrix(const GateIR& g);
+
+enum class NoiseKind : int { XError, YError, ZError, PauliChannel1, Depolarize1, Depolarize2 };
+struct NoiseIR {
+  NoiseKind kind = NoiseKind::XError;
+  double p[3] = {0, 0, 0};
+  uint32_t arity() const { return kind == NoiseKind::Depolarize2 ? 2 : 1; }
+  std::string text() const;
+  bool valid() const;
+  // Noise::sample (circuit.rs:136-146): always one draw; -1 for no error,
+  // otherwise (x bits) | (z bits) << 8
+  int sample(ncsim_rng& rng) const;
+};
+
+enum class OpKind : int { Gate, Measure, Reset, Noise, Detector, Observable, Tick };
+struct OpIR {
+  OpKind kind = OpKind::Tick;
+  GateIR gate;
+  std::vector<uint32_t> qubits;
+  LoweredOp lowered;
+  PauliOp pauli;
+  NoiseIR noise;
+  std::vector<uint64_t> lookback;
+  uint64_t index = 0;
+};
+
+}  // namespace ncsim
+
+struct ncsim_circuit {
+  uint32_t n = 0;
+  std::vector<ncsim::OpIR> ops;
+  uint64_t num_gates() const;
+  uint64_t num_measurements() const;
+  std::string text() const;
+};
+
+struct ncsim_gate {
+  ncsim::GateIR g;
+};
+
+namespace ncsim {
+ncsim_circuit parse_circuit(const std::string& text);
+GateIR parse_gate_token(const std::string& tok, uint32_t nq_hint);
+std::string random_layer_text(uint32_t n, uint32_t depth, ncsim_rng& rng, double noise_p, uint32_t m_lo, uint32_t m_hi);
+std::string reversible_text(uint32_t n, uint32_t gates, ncsim_rng& rng);
+std::string fmt_f64(double v);
+}  // namespace ncsim

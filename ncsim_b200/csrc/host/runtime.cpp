@@ -1,0 +1,360 @@
+// The trait's provided methods on the device state (src/state/mod.rs:93-234)
+// and the C ABI of the host layer: RNG, circuits, gates, run/measure/sample.
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+
+#include "ir.hpp"
+
+using namespace ncsim;
+
+namespace ncsim {
+
+PolyTerms build_poly_terms(const PhasePolyIR& p, const std::vector<uint32_t>& qubits, const Phase& scalar);
+
+void apply_lowered(ncsim_state* s, const LoweredOp& op) {
+  switch (op.kind) {
+    case LoweredKind::Nothing: return;
+    case LoweredKind::Dense: launch_dense(s, op.qubits, op.matrix); return;
+    case LoweredKind::Monomial: launch_perm_table(s, op.qubits, op.image, op.matrix); return;
+    case LoweredKind::PhasePoly: launch_phasepoly(s, op.poly); return;
+    case LoweredKind::Pauli: launch_pauli(s, op.x, op.z, op.phase); return;
+  }
+}
+
+// QuantumState::measure (mod.rs:113-131); expectation and norm in one pass
+bool measure_op(ncsim_state* s, const PauliOp& p, ncsim_rng& rng) {
+  if (!p.hermitian()) throw Error(NCSIM_ERR_INVALID, "measured operator is not Hermitian");
+  if (p.n != s->n) throw Error(NCSIM_ERR_INVALID, "expectation: operator on the wrong register");
+  double e[2], nn;
+  state_measure_stats(s, p.x, p.z, p.phase, e, &nn);
+  double p_plus = (1.0 + e[0] / nn) / 2.0;
+  if (!std::isnan(p_plus)) p_plus = std::min(1.0, std::max(0.0, p_plus));
+  bool outcome;
+  if (p_plus > 1.0 - 1e-12) outcome = false;
+  else if (p_plus < 1e-12) outcome = true;
+  else outcome = rng.f64() >= p_plus;
+  state_project(s, p.x, p.z, p.phase, outcome);
+  return outcome;
+}
+
+// QuantumState::apply_op (mod.rs:134-165); returns -1, 0 or 1
+int apply_op(ncsim_state* s, const OpIR& op, ncsim_rng& rng) {
+  switch (op.kind) {
+    case OpKind::Gate: apply_lowered(s, op.lowered); return -1;
+    case OpKind::Measure: return measure_op(s, op.pauli, rng) ? 1 : 0;
+    case OpKind::Reset: {
+      PauliOp z;
+      z.n = s->n;
+      z.z = uint64_t(1) << op.qubits[0];
+      if (measure_op(s, z, rng)) launch_pauli(s, uint64_t(1) << op.qubits[0], 0, 0);
+      return -1;
+    }
+    case OpKind::Noise: {
+      int e = op.noise.sample(rng);
+      if (e >= 0) {
+        // raw X^x Z^z bits with phase 0 (mod.rs:148-162)
+        uint64_t x = 0, z = 0;
+        for (size_t j = 0; j < op.qubits.size(); ++j) {
+          x |= uint64_t((e >> j) & 1) << op.qubits[j];
+          z |= uint64_t((e >> (8 + j)) & 1) << op.qubits[j];
+        }
+        launch_pauli(s, x, z, 0);
+      }
+      return -1;
+    }
+    default: return -1;
+  }
+}
+
+}  // namespace ncsim
+
+namespace {
+void need(const void* p, const char* what) {
+  if (!p) throw Error(NCSIM_ERR_INVALID, std::string(what) + " is null");
+}
+}  // namespace
+
+extern "C" {
+
+// ---- rng ----
+ncsim_status ncsim_rng_new(uint64_t seed, ncsim_rng** out) {
+  return guarded([&] {
+    need(out, "out");
+    *out = new ncsim_rng(seed);
+  });
+}
+ncsim_status ncsim_rng_free(ncsim_rng* r) {
+  return guarded([&] { delete r; });
+}
+ncsim_status ncsim_rng_next_u64(ncsim_rng* r, uint64_t* out) {
+  return guarded([&] {
+    need(r, "rng");
+    need(out, "out");
+    *out = r->u64();
+  });
+}
+ncsim_status ncsim_rng_next_u32(ncsim_rng* r, uint32_t* out) {
+  return guarded([&] {
+    need(r, "rng");
+    need(out, "out");
+    *out = r->u32();
+  });
+}
+ncsim_status ncsim_rng_gen_f64(ncsim_rng* r, double* out) {
+  return guarded([&] {
+    need(r, "rng");
+    need(out, "out");
+    *out = r->f64();
+  });
+}
+ncsim_status ncsim_rng_gen_range(ncsim_rng* r, uint64_t lo, uint64_t hi, uint64_t* out) {
+  return guarded([&] {
+    need(r, "rng");
+    need(out, "out");
+    if (hi <= lo) throw Error(NCSIM_ERR_INVALID, "gen_range: empty range");
+    *out = r->range64(lo, hi);
+  });
+}
+
+// ---- circuits ----
+ncsim_status ncsim_circuit_parse(const char* text, ncsim_circuit** out) {
+  return guarded([&] {
+    need(text, "text");
+    need(out, "out");
+    *out = nullptr;
+    *out = new ncsim_circuit(parse_circuit(text));
+  });
+}
+ncsim_status ncsim_circuit_free(ncsim_circuit* c) {
+  return guarded([&] { delete c; });
+}
+ncsim_status ncsim_circuit_info(const ncsim_circuit* c, uint32_t* nq, uint64_t* nops, uint64_t* ng, uint64_t* nm) {
+  return guarded([&] {
+    need(c, "circuit");
+    if (nq) *nq = c->n;
+    if (nops) *nops = c->ops.size();
+    if (ng) *ng = c->num_gates();
+    if (nm) *nm = c->num_measurements();
+  });
+}
+ncsim_status ncsim_circuit_to_text(const ncsim_circuit* c, char* buf, size_t cap, size_t* len) {
+  return guarded([&] {
+    need(c, "circuit");
+    std::string t = c->text();
+    if (len) *len = t.size();
+    if (buf && cap > t.size()) std::memcpy(buf, t.c_str(), t.size() + 1);
+  });
+}
+ncsim_status ncsim_workload_random_circuit(uint32_t n, uint32_t depth, uint64_t seed, double noise_p, uint32_t m_lo,
+                                           uint32_t m_hi, ncsim_circuit** out) {
+  return guarded([&] {
+    need(out, "out");
+    *out = nullptr;
+    if (n < 1 || n > 64) throw Error(NCSIM_ERR_INVALID, "workload register must have 1..64 qubits");
+    ncsim_rng rng(seed);
+    *out = new ncsim_circuit(parse_circuit(random_layer_text(n, depth, rng, noise_p, m_lo, m_hi)));
+  });
+}
+ncsim_status ncsim_workload_random_circuit_rng(ncsim_rng* rng, uint32_t n, uint32_t depth, double noise_p, uint32_t m_lo,
+                                               uint32_t m_hi, ncsim_circuit** out) {
+  return guarded([&] {
+    need(rng, "rng");
+    need(out, "out");
+    *out = nullptr;
+    if (n < 1 || n > 64) throw Error(NCSIM_ERR_INVALID, "workload register must have 1..64 qubits");
+    *out = new ncsim_circuit(parse_circuit(random_layer_text(n, depth, *rng, noise_p, m_lo, m_hi)));
+  });
+}
+ncsim_status ncsim_workload_reversible_circuit(uint32_t n, uint32_t gates, uint64_t seed, ncsim_circuit** out) {
+  return guarded([&] {
+    need(out, "out");
+    *out = nullptr;
+    if (n < 8 || n > 64) throw Error(NCSIM_ERR_INVALID, "reversible workload needs 8..64 qubits");
+    ncsim_rng rng(seed);
+    *out = new ncsim_circuit(parse_circuit(reversible_text(n, gates, rng)));
+  });
+}
+
+// ---- gates ----
+ncsim_status ncsim_gate_parse(const char* token, uint32_t arity_hint, ncsim_gate** out, uint32_t* arity) {
+  return guarded([&] {
+    need(token, "token");
+    need(out, "out");
+    *out = nullptr;
+    auto* g = new ncsim_gate();
+    try {
+      g->g = parse_gate_token(token, arity_hint);
+    } catch (...) {
+      delete g;
+      throw;
+    }
+    if (arity) *arity = g->g.arity();
+    *out = g;
+  });
+}
+ncsim_status ncsim_gate_unitary(uint32_t k, const double* m, ncsim_gate** out) {
+  return guarded([&] {
+    need(m, "matrix");
+    need(out, "out");
+    if (k < 1 || k > 5) throw Error(NCSIM_ERR_UNSUPPORTED, "dense gates on 1..5 qubits");
+    auto* g = new ncsim_gate();
+    g->g.kind = GateKind::Unitary;
+    g->g.uk = k;
+    const size_t d = size_t(1) << k;
+    for (size_t i = 0; i < d * d; ++i) g->g.umat.push_back({m[2 * i], m[2 * i + 1]});
+    *out = g;
+  });
+}
+ncsim_status ncsim_gate_pauli(uint32_t k, uint64_t x, uint64_t z, uint32_t phase, ncsim_gate** out) {
+  return guarded([&] {
+    need(out, "out");
+    if (k > 64) throw Error(NCSIM_ERR_INVALID, "Pauli on more than 64 qubits");
+    const uint64_t mask = k >= 64 ? ~uint64_t(0) : ((uint64_t(1) << k) - 1);
+    auto* g = new ncsim_gate();
+    g->g.kind = GateKind::Pauli;
+    g->g.pauli.n = k;
+    g->g.pauli.x = x & mask;
+    g->g.pauli.z = z & mask;
+    g->g.pauli.phase = phase & 3;
+    *out = g;
+  });
+}
+ncsim_status ncsim_gate_free(ncsim_gate* g) {
+  return guarded([&] { delete g; });
+}
+ncsim_status ncsim_pauli_parse(const char* text, uint32_t n, uint64_t* x, uint64_t* z, uint32_t* phase) {
+  return guarded([&] {
+    need(text, "text");
+    PauliOp p = parse_pauli(text, int64_t(n));
+    if (x) *x = p.x;
+    if (z) *z = p.z;
+    if (phase) *phase = p.phase;
+  });
+}
+
+// ---- trait methods on the device state ----
+ncsim_status ncsim_sv_apply_gate(ncsim_state* s, const ncsim_gate* g, const uint32_t* qubits, uint32_t k) {
+  return guarded([&] {
+    need(s, "state");
+    need(g, "gate");
+    if (k) need(qubits, "qubits");
+    LoweredOp op = lower_gate(g->g, std::vector<uint32_t>(qubits, qubits + k), s->n);
+    std::lock_guard<std::recursive_mutex> lk(s->mu);
+    apply_lowered(s, op);
+  });
+}
+
+ncsim_status ncsim_sv_measure(ncsim_state* s, uint64_t x, uint64_t z, uint32_t phase, ncsim_rng* rng, int32_t* outcome) {
+  return guarded([&] {
+    need(s, "state");
+    need(rng, "rng");
+    need(outcome, "out");
+    PauliOp p;
+    p.n = s->n;
+    p.x = x;
+    p.z = z;
+    p.phase = phase & 3;
+    if ((x | z) >> s->n && s->n < 64) throw Error(NCSIM_ERR_INVALID, "Pauli acts outside the register");
+    std::lock_guard<std::recursive_mutex> lk(s->mu);
+    *outcome = measure_op(s, p, *rng) ? 1 : 0;
+  });
+}
+
+ncsim_status ncsim_sv_run(ncsim_state* s, const ncsim_circuit* c, ncsim_rng* rng, uint8_t* rec, size_t cap, size_t* len) {
+  return guarded([&] {
+    need(s, "state");
+    need(c, "circuit");
+    need(rng, "rng");
+    if (c->n != s->n)
+      throw Error(NCSIM_ERR_INVALID, "circuit on " + std::to_string(c->n) + " qubits, state on " + std::to_string(s->n));
+    if (c->num_measurements() > cap) throw Error(NCSIM_ERR_INVALID, "record buffer too small");
+    if (c->num_measurements()) need(rec, "record");
+    std::lock_guard<std::recursive_mutex> lk(s->mu);
+    size_t m = 0;
+    for (auto& op : c->ops) {
+      int r = apply_op(s, op, *rng);
+      if (r >= 0) rec[m++] = uint8_t(r);
+    }
+    NCSIM_CUDA(cudaStreamSynchronize(s->stream));
+    if (len) *len = m;
+  });
+}
+
+ncsim_status ncsim_sv_sample_rng(const ncsim_state* s, ncsim_rng* rng, uint64_t shots, uint64_t* out) {
+  return guarded([&] {
+    need(s, "state");
+    need(rng, "rng");
+    std::vector<double> u(shots);
+    for (auto& v : u) v = rng->f64();  // drawn first, in shot order (vector.rs:505)
+    std::lock_guard<std::recursive_mutex> lk(s->mu);
+    state_sample(s, u.data(), shots, out);
+  });
+}
+
+ncsim_status ncsim_sv_normalize(ncsim_state* s) {
+  return guarded([&] {
+    need(s, "state");
+    std::lock_guard<std::recursive_mutex> lk(s->mu);
+    const double nn = state_norm_sq(s).re;
+    if (!(nn > 0.0)) throw Error(NCSIM_ERR_ZERO_STATE, "state vanished: normalize");
+    const double l = -std::log2(nn);
+    double c;
+    if (std::fabs(l - std::round(l)) < 1e-9) c = sqrt2_power(int64_t(std::round(l)));
+    else c = 1.0 / std::sqrt(nn);
+    launch_scale(s, {c, 0.0});
+  });
+}
+
+ncsim_status ncsim_sv_probability(const ncsim_state* s, uint64_t index, double* out) {
+  return guarded([&] {
+    need(s, "state");
+    need(out, "out");
+    std::lock_guard<std::recursive_mutex> lk(s->mu);
+    double a[2];
+    uint64_t i = s->n >= 64 ? index : (index & ((uint64_t(1) << s->n) - 1));
+    state_gather(s, &i, 1, a);
+    *out = (a[0] * a[0] + a[1] * a[1]) / state_norm_sq(s).re;
+  });
+}
+
+ncsim_status ncsim_sv_expectation_sum(const ncsim_state* s, uint64_t count, const uint64_t* x, const uint64_t* z,
+                                      const uint32_t* phase, const double* coeffs, double* re_im) {
+  return guarded([&] {
+    need(s, "state");
+    need(re_im, "out");
+    if (count) {
+      need(x, "x");
+      need(z, "z");
+      need(phase, "phase");
+      need(coeffs, "coeffs");
+    }
+    std::lock_guard<std::recursive_mutex> lk(s->mu);
+    std::vector<CplxD> t(count);
+    for (uint64_t k = 0; k < count; ++k) {
+      CplxD e = state_expectation(s, x[k], z[k], phase[k] & 3);
+      const double cr = coeffs[2 * k], ci = coeffs[2 * k + 1];
+      t[k] = {cr * e.re - ci * e.im, cr * e.im + ci * e.re};
+    }
+    // Amplitude::sum (scalar.rs:80-94): pairwise, leaves of at most 8
+    struct Rec {
+      static CplxD sum(const CplxD* v, size_t n) {
+        if (n <= 8) {
+          CplxD a{0, 0};
+          for (size_t i = 0; i < n; ++i) a = {a.re + v[i].re, a.im + v[i].im};
+          return a;
+        }
+        CplxD l = sum(v, n / 2), r = sum(v + n / 2, n - n / 2);
+        return {l.re + r.re, l.im + r.im};
+      }
+    };
+    CplxD r = Rec::sum(t.data(), t.size());
+    re_im[0] = r.re;
+    re_im[1] = r.im;
+  });
+}
+
+ncsim_status ncsim_sv_run_fused(ncsim_state* s, const ncsim_circuit* c, ncsim_rng* rng, uint32_t max_fuse, uint8_t* rec,
+                                size_t cap, size_t* len, ncsim_fused_stats* stats);
+
+}  // extern "C"
