@@ -219,6 +219,11 @@ ncsim_status ncsim_gate_unitary(uint32_t k, const double* matrix, ncsim_gate** o
 /* Gate::Pauli (gate.rs:417-418): i^phase X^x Z^z on k local qubits. */
 ncsim_status ncsim_gate_pauli(uint32_t k, uint64_t x, uint64_t z, uint32_t phase, ncsim_gate** out);
 ncsim_status ncsim_gate_free(ncsim_gate* g);
+/* The dense 2^k x 2^k complex128 matrix that the engine's lowering of the
+ * gate applies on qubits 0..k-1 (host only, k <= 8): the dense view, the
+ * permutation table, the phase polynomial or the Pauli, as launched.  For
+ * checking the lowering against Gate::matrix (gate.rs:670-747). */
+ncsim_status ncsim_gate_lowered_matrix(const ncsim_gate* g, double* out, size_t cap_doubles, uint32_t* k);
 
 /* Pauli::from_string(n, text) (pauli/mod.rs:349-414) as (x, z, phase). */
 ncsim_status ncsim_pauli_parse(const char* text, uint32_t n, uint64_t* x, uint64_t* z, uint32_t* phase);

@@ -102,6 +102,7 @@ _SIGNATURES = {
     "ncsim_gate_unitary": (_i32, [_u32, _P(_dbl), _P(_vp)]),
     "ncsim_gate_pauli": (_i32, [_u32, _u64, _u64, _u32, _P(_vp)]),
     "ncsim_gate_free": (_i32, [_vp]),
+    "ncsim_gate_lowered_matrix": (_i32, [_vp, _P(_dbl), C.c_size_t, _P(_u32)]),
     "ncsim_pauli_parse": (_i32, [C.c_char_p, _u32, _P(_u64), _P(_u64), _P(_u32)]),
     "ncsim_sv_apply_gate": (_i32, [_vp, _vp, _P(_u32), _u32]),
     "ncsim_sv_measure": (_i32, [_vp, _u64, _u64, _u32, _vp, _P(_i32)]),
@@ -254,6 +255,14 @@ class Gate:
         h = getattr(self, "_h", None)
         if h and _lib is not None:
             _lib.ncsim_gate_free(h)
+
+    def lowered_matrix(self) -> np.ndarray:
+        """The dense matrix the engine's lowering applies (host only)."""
+        d = 1 << self.arity
+        buf = np.zeros(2 * d * d, dtype=np.float64)
+        k = _u32()
+        _check(lib().ncsim_gate_lowered_matrix(self._h, _dp(buf), buf.size, C.byref(k)))
+        return buf.view(np.complex128).reshape(d, d)
 
     def __repr__(self) -> str:
         return f"Gate({self.label})"

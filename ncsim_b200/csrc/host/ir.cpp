@@ -421,11 +421,18 @@ LoweredOp lower_gate(const GateIR& g, const std::vector<uint32_t>& qubits, uint3
     op.phase = g.pauli.phase & 3;
     return op;
   }
+  if (g.kind == GateKind::Ccx) {
+    // Its dense view (gate.rs:697-705) is a 0/1 permutation matrix, applied
+    // exactly as a permutation table: the target flips when both controls
+    // are set (not an affine map, so not a MonomialGate).
+    op.kind = LoweredKind::Monomial;
+    op.image.resize(8);
+    op.matrix.assign(8, CplxD{1.0, 0.0});
+    for (uint32_t x = 0; x < 8; ++x) op.image[x] = (x & 3) == 3 ? (x ^ 4) : x;
+    return op;
+  }
   MonomialIR mo;
-  if (g.kind == GateKind::Ccx) {  // its dense view is a 0/1 permutation: a monomial in effect
-    mo = diag_mono(3, 1, {});
-    mo.rows = {1, 2, 7};
-  } else if (!monomial_view(g, mo)) {
+  if (!monomial_view(g, mo)) {
     op.kind = LoweredKind::Dense;
     op.matrix = gate_matrix(g);
     if (qubits.size() > 5) throw Error(NCSIM_ERR_UNSUPPORTED, "dense gates on more than 5 qubits");

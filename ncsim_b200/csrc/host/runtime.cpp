@@ -223,6 +223,55 @@ ncsim_status ncsim_gate_pauli(uint32_t k, uint64_t x, uint64_t z, uint32_t phase
 ncsim_status ncsim_gate_free(ncsim_gate* g) {
   return guarded([&] { delete g; });
 }
+ncsim_status ncsim_gate_lowered_matrix(const ncsim_gate* g, double* out, size_t cap, uint32_t* kout) {
+  return guarded([&] {
+    need(g, "gate");
+    need(out, "out");
+    const uint32_t k = g->g.arity();
+    if (k < 1 || k > 8) throw Error(NCSIM_ERR_UNSUPPORTED, "lowered matrices of 1..8 qubits");
+    const size_t d = size_t(1) << k;
+    if (cap < 2 * d * d) throw Error(NCSIM_ERR_INVALID, "output buffer too small");
+    std::vector<uint32_t> qs(k);
+    for (uint32_t j = 0; j < k; ++j) qs[j] = j;
+    LoweredOp op = lower_gate(g->g, qs, k);
+    std::vector<CplxD> m(d * d, CplxD{0, 0});
+    switch (op.kind) {
+      case LoweredKind::Dense: m = op.matrix; break;
+      case LoweredKind::Monomial:
+        for (size_t x = 0; x < d; ++x) m[size_t(op.image[x]) * d + x] = op.matrix[x];
+        break;
+      case LoweredKind::PhasePoly:
+        for (uint64_t x = 0; x < d; ++x) {
+          uint64_t f = op.poly.constant;
+          for (size_t t = 0; t + 1 < op.poly.term_start.size(); ++t) {
+            bool all = true;
+            for (uint32_t l = op.poly.term_start[t]; l < op.poly.term_start[t + 1]; ++l)
+              all &= bool(__builtin_popcountll(op.poly.parities[l] & x) & 1);
+            if (all) f += op.poly.coeffs[t];
+          }
+          f &= (uint64_t(1) << op.poly.bits) - 1;
+          Cd r = root_value(int64_t(f), op.poly.bits);
+          CplxD c = op.poly.root_table.empty()
+                        ? CplxD{op.poly.scalar.re * r.re - op.poly.scalar.im * r.im, op.poly.scalar.re * r.im + op.poly.scalar.im * r.re}
+                        : op.poly.root_table[f];
+          m[x * d + x] = c;
+        }
+        break;
+      case LoweredKind::Pauli:
+        for (uint64_t x = 0; x < d; ++x) {
+          int kk = int(op.phase + 2 * __builtin_popcountll(op.z & x)) & 3;
+          static const CplxD ip[4] = {{1, 0}, {0, 1}, {-1, 0}, {0, -1}};
+          m[(x ^ op.x) * d + x] = ip[kk];
+        }
+        break;
+      case LoweredKind::Nothing:
+        for (size_t x = 0; x < d; ++x) m[x * d + x] = {1, 0};
+        break;
+    }
+    for (size_t i = 0; i < d * d; ++i) out[2 * i] = m[i].re, out[2 * i + 1] = m[i].im;
+    if (kout) *kout = k;
+  });
+}
 ncsim_status ncsim_pauli_parse(const char* text, uint32_t n, uint64_t* x, uint64_t* z, uint32_t* phase) {
   return guarded([&] {
     need(text, "text");

@@ -211,6 +211,53 @@ struct DiagParams {
   uint8_t unit[1 << KMAX];
 };
 
+// One phase for every enumerated amplitude: the gate's only phased pattern
+// has all its gate bits fixed (S, T, Z, PHASE, CZ, CS, CPHASE, CCZ).  Two
+// amplitudes in flight per thread.
+template <class R>
+struct DiagConstParams {
+  int nfix;
+  uint8_t fixpos[MAX_DIAG_K];
+  uint64_t fixmask;
+  V<R> c;
+};
+
+template <class R>
+__global__ void __launch_bounds__(THREADS) k_diag_const(V<R>* __restrict__ a, uint64_t count, const __grid_constant__ DiagConstParams<R> P) {
+  const uint64_t stride = uint64_t(gridDim.x) * blockDim.x;
+  const V<R> c = P.c;
+  uint64_t p = uint64_t(blockIdx.x) * blockDim.x + threadIdx.x;
+  for (; p + stride < count; p += 2 * stride) {
+    const uint64_t i = insert_zeros(p, P.fixpos, P.nfix) | P.fixmask;
+    const uint64_t j = insert_zeros(p + stride, P.fixpos, P.nfix) | P.fixmask;
+    V<R> u = a[i], v = a[j];
+    if (!is_zero(u)) a[i] = cmul(c, u);
+    if (!is_zero(v)) a[j] = cmul(c, v);
+  }
+  if (p < count) {
+    const uint64_t i = insert_zeros(p, P.fixpos, P.nfix) | P.fixmask;
+    V<R> u = a[i];
+    if (!is_zero(u)) a[i] = cmul(c, u);
+  }
+}
+
+// Two phases selected by one index bit (RZ and any diagonal 1-qubit matrix).
+template <class R>
+__global__ void __launch_bounds__(THREADS) k_diag_1q(V<R>* __restrict__ a, uint64_t len, int q, V<R> c0, V<R> c1) {
+  const uint64_t stride = uint64_t(gridDim.x) * blockDim.x;
+  uint64_t i = uint64_t(blockIdx.x) * blockDim.x + threadIdx.x;
+  for (; i + stride < len; i += 2 * stride) {
+    const uint64_t j = i + stride;
+    V<R> u = a[i], v = a[j];
+    if (!is_zero(u)) a[i] = cmul(((i >> q) & 1) ? c1 : c0, u);
+    if (!is_zero(v)) a[j] = cmul(((j >> q) & 1) ? c1 : c0, v);
+  }
+  if (i < len) {
+    V<R> u = a[i];
+    if (!is_zero(u)) a[i] = cmul(((i >> q) & 1) ? c1 : c0, u);
+  }
+}
+
 template <class R, int KMAX>
 __global__ void __launch_bounds__(THREADS) k_diag(V<R>* __restrict__ a, uint64_t count, const __grid_constant__ DiagParams<R, KMAX> P) {
   __shared__ V<R> d[1 << KMAX];
@@ -836,6 +883,35 @@ void launch_diag_table(ncsim_state* s, const std::vector<uint32_t>& qubits, cons
   for (int x = 0; x < gd; ++x)
     if (!is_one(diag[x])) fixed &= uint32_t(x), any = true;
   if (!any) return;  // identity: no amplitude changes
+  int nphased = 0;
+  for (int x = 0; x < gd; ++x) nphased += !is_one(diag[x]);
+  if (nphased == 1 && fixed == uint32_t(gd - 1)) {
+    // one phased pattern with every gate bit fixed: a constant phase on it
+    NCSIM_DISPATCH(s, {
+      DiagConstParams<R> P{};
+      std::vector<int> fp(qubits.begin(), qubits.end());
+      std::sort(fp.begin(), fp.end());
+      P.nfix = k;
+      uint64_t fm = 0;
+      for (int i = 0; i < k; ++i) P.fixpos[i] = uint8_t(fp[i]), fm |= uint64_t(1) << fp[i];
+      P.fixmask = fm;
+      P.c = cv<R>(diag[gd - 1]);
+      uint64_t count = s->len >> k;
+      ProfScope ps(s, K_DIAG, touched_bytes(s, fm));
+      k_diag_const<R><<<grid_for(count, THREADS, 2), THREADS, 0, s->stream>>>(amp_of<R>(s), count, P);
+    });
+    NCSIM_LAUNCHED("diag_const");
+    return;
+  }
+  if (k == 1) {  // both patterns phased
+    NCSIM_DISPATCH(s, {
+      ProfScope ps(s, K_DIAG, full_bytes(s));
+      k_diag_1q<R><<<grid_for(s->len, THREADS, 2), THREADS, 0, s->stream>>>(amp_of<R>(s), s->len, int(qubits[0]),
+                                                                             cv<R>(diag[0]), cv<R>(diag[1]));
+    });
+    NCSIM_LAUNCHED("diag_1q");
+    return;
+  }
   auto body = [&](auto tagR, auto tagK) {
     using R = decltype(tagR);
     constexpr int KM = decltype(tagK)::value;

@@ -115,3 +115,41 @@ def test_state_argument_errors_need_no_device(nb):
     assert nb.lib().ncsim_sv_create(10, 7, ctypes.byref(h)) == 8
     assert nb.lib().ncsim_sv_norm_sq(None, (ctypes.c_double * 2)()) == 8
     assert "null" in nb.lib().ncsim_last_error().decode()
+
+
+LOWERED = ["I", "X", "Y", "Z", "H", "S", "S_DAG", "SQRT_X", "SQRT_X_DAG", "SQRT_Y", "SQRT_Y_DAG", "T", "T_DAG",
+           "CX", "CY", "CZ", "SWAP", "CS", "CS_DAG", "CCZ", "CCX", "PHASE(3,4)", "PHASE(-5,9)", "CPHASE(1,3)",
+           "CPHASE(7,2)", "RX(0.3)", "RY(-1.1)", "RZ(2.2)"]
+
+
+@pytest.mark.parametrize("name", LOWERED)
+def test_lowering_of_named_gates_matches_gate_matrix(nb, oracle, name):
+    """The kernel descriptors built on the host equal the oracle's Gate::matrix (gate.rs:670-747)."""
+    import numpy as np
+
+    g = nb.Gate.parse(name)
+    k = g.arity
+    want = oracle.gate_matrix(f"QUBITS {k}\n{name} " + " ".join(map(str, range(k))) + "\n")
+    assert np.abs(g.lowered_matrix() - want).max() < 1e-15
+
+
+def test_lowering_of_random_diagonals_and_monomials(nb, oracle):
+    import numpy as np
+
+    text = oracle.reversible_circuit_text(8, 40, 21)
+    for line in text.splitlines()[1:]:
+        toks = line.split()
+        if not toks[0].startswith(("DIAG", "MONOMIAL")):
+            continue
+        k = len(toks) - 1
+        local = f"QUBITS {k}\n{toks[0]} " + " ".join(map(str, range(k))) + "\n"
+        g = nb.Gate.parse(toks[0], k)
+        want = np.eye(1 << k, dtype=complex)
+        s = oracle.StateVector(k)
+        for col in range(1 << k):
+            e = np.zeros(1 << k, dtype=complex)
+            e[col] = 1
+            s.set_amplitudes(e)
+            s.apply_gate_text(local.split("\n", 1)[1])
+            want[:, col] = s.to_vector()
+        assert np.abs(g.lowered_matrix() - want).max() < 1e-15, toks[0][:40]

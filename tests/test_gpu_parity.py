@@ -305,7 +305,8 @@ def test_kron_clone_and_basis_states(nb, oracle):
 def test_argument_errors_on_device(nb):
     s = nb.GpuStateVector(6)
     h = nb.Gate.parse("H")
-    for qs, kind in (([6], "QubitOutOfRange"), ([1, 1], "Arity"), ([], "Arity")):
+    # check_qubits runs before the arity check (vector.rs:365-372)
+    for qs, kind in (([6], "QubitOutOfRange"), ([1, 1], "DuplicateQubit"), ([1, 2], "Arity"), ([], "Arity")):
         with pytest.raises(nb.SimError) as e:
             s.apply_gate(h, qs)
         assert e.value.kind == kind
