@@ -174,6 +174,23 @@ typedef struct ncsim_kernel_stat {
 ncsim_status ncsim_sv_profile_enable(ncsim_state* s, int32_t enable);
 ncsim_status ncsim_sv_profile_read(ncsim_state* s, ncsim_kernel_stat* out, uint32_t cap, uint32_t* count);
 
+/* <psi|P|psi> and <psi|psi> of 2^n amplitudes that the caller already holds
+ * in its own device memory (interleaved complex128 or complex64, per
+ * `precision`), computed on the caller's stream (`stream` is a cudaStream_t;
+ * NULL is the default stream), with no device or host allocation.
+ * This entry point has no counterpart in the reference: it serves callers
+ * that cannot let a library call cudaMalloc, because their amplitudes live in
+ * memory they manage themselves (a framework's pool, a fixed device budget)
+ * where an allocation or free could synchronize the device, fragment the pool
+ * or exceed the budget.  The reduction scratch is a file-scope device array of
+ * 1024 block partials (32 KB); registers of up to 34 qubits are accepted and
+ * larger ones are rejected with NCSIM_ERR_INVALID.  The first call on a
+ * device resolves the array's device address (set-up), so make it before any
+ * stream capture.  All calls share the array: calls that overlap on the GPU
+ * race and must be serialized by the caller. */
+ncsim_status ncsim_measure_stats_noalloc(const void* amps, uint32_t n, int32_t precision, uint64_t x, uint64_t z,
+                                         uint32_t phase, void* stream, double* expectation_re_im, double* norm_sq);
+
 /* ======================================================================
  * 2. Host mirror of the reference interface (C++), and the GPU-only forms
  * ====================================================================== */

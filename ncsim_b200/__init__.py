@@ -117,6 +117,7 @@ _SIGNATURES = {
     "ncsim_sv_compare": (_i32, [_vp, _vp, _P(_dbl), _P(_dbl), _P(_dbl), _P(_dbl)]),
     "ncsim_sv_profile_enable": (_i32, [_vp, _i32]),
     "ncsim_sv_profile_read": (_i32, [_vp, _vp, _u32, _P(_u32)]),
+    "ncsim_measure_stats_noalloc": (_i32, [_vp, _u32, _i32, _u64, _u64, _u32, _vp, _P(_dbl), _P(_dbl)]),
 }
 
 

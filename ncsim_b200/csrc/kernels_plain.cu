@@ -1225,3 +1225,114 @@ void fetch_partials(const ncsim_state* s, int nb, int slots, double* out) {
 }
 
 }  // namespace ncsim
+
+// ===========================================================================
+// <P> and <psi|psi> over caller-owned device amplitudes, allocating nothing.
+//
+// Some callers cannot let a library call cudaMalloc: they keep the amplitudes
+// in device memory they already own (a framework's memory pool, a buffer
+// carved from a fixed device budget), and a device allocation or free there
+// could synchronize the device, fragment the pool or break the budget they
+// reserved.  This entry point reads their buffer in place and keeps its
+// reduction scratch in the file-scope array below instead.
+//
+// The array: NOALLOC_BLOCKS per-block partials (PARTIAL_SLOTS doubles each)
+// plus 8 result doubles, 32 KB + 64 B, held by every GPU that loads the
+// library until the process exits.  Host code must not pass the array's name
+// to a kernel (on the host it is only a stand-in, not a device address): the
+// device address comes from cudaGetSymbolAddress, fetched once per device,
+// with that device current, by the first call made on it.  That first call
+// therefore does the set-up and should come before any stream capture.
+//
+// Every call shares the array and it keeps the last call's contents.  Each
+// call writes every partial slot it later reads (one per launched block) and
+// then the result slots, so nothing has to start at zero; calls that overlap
+// on the GPU (two streams, two host threads) race on the array and must be
+// serialized by the caller.
+// ===========================================================================
+namespace ncsim {
+namespace {
+
+constexpr int NOALLOC_BLOCKS = 1024;
+constexpr int NOALLOC_RESULT = NOALLOC_BLOCKS * PARTIAL_SLOTS;
+constexpr int NOALLOC_MAX_QUBITS = 34;
+
+static __device__ __align__(256) double g_noalloc_scratch[NOALLOC_RESULT + 8];
+
+// slot j of the result = the sum over blocks of slot j, in block order
+__global__ void k_noalloc_finish(double* scratch, int nblocks, int slots) {
+  const int j = threadIdx.x;
+  if (j >= slots) return;
+  double s = 0.0;
+  for (int b = 0; b < nblocks; ++b) s += scratch[b * PARTIAL_SLOTS + j];
+  scratch[NOALLOC_RESULT + j] = s;
+}
+
+constexpr int NOALLOC_MAX_DEVICES = 64;
+std::mutex g_noalloc_mu;
+double* g_noalloc_ptr[NOALLOC_MAX_DEVICES] = {};
+
+// the array's device address on the current device (set-up on first use)
+double* noalloc_scratch(int dev) {
+  if (dev < 0 || dev >= NOALLOC_MAX_DEVICES) throw Error(NCSIM_ERR_DEVICE, "device index out of range");
+  std::lock_guard<std::mutex> lk(g_noalloc_mu);
+  if (!g_noalloc_ptr[dev]) {
+    void* p = nullptr;
+    cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+    if (e != cudaSuccess || !p) {
+      cudaGetLastError();
+      throw Error(NCSIM_ERR_DEVICE, std::string("cudaGetSymbolAddress of the static scratch: ") + cudaGetErrorString(e));
+    }
+    g_noalloc_ptr[dev] = static_cast<double*>(p);
+  }
+  return g_noalloc_ptr[dev];
+}
+
+}  // namespace
+
+}  // namespace ncsim
+
+extern "C" ncsim_status ncsim_measure_stats_noalloc(const void* amps, uint32_t n, int32_t precision, uint64_t x,
+                                                    uint64_t z, uint32_t phase, void* stream, double* expectation_re_im,
+                                                    double* norm_sq) {
+  using namespace ncsim;
+  return guarded([&] {
+    if (!amps) throw Error(NCSIM_ERR_INVALID, "amplitudes are null");
+    if (!expectation_re_im || !norm_sq) throw Error(NCSIM_ERR_INVALID, "outputs are null");
+    if (precision != NCSIM_C128 && precision != NCSIM_C64) throw Error(NCSIM_ERR_INVALID, "precision must be C128 or C64");
+    if (n > uint32_t(NOALLOC_MAX_QUBITS))
+      throw Error(NCSIM_ERR_INVALID, "register of " + std::to_string(n) + " qubits exceeds the " +
+                                         std::to_string(NOALLOC_MAX_QUBITS) + "-qubit maximum of the no-allocation entry point");
+    const uint64_t len = uint64_t(1) << n;
+    if ((x | z) & ~(len - 1)) throw Error(NCSIM_ERR_INVALID, "Pauli acts outside the register");
+    int dev = 0;
+    NCSIM_CUDA(cudaGetDevice(&dev));
+    double* scratch = noalloc_scratch(dev);
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    const int ph = int(phase & 3);
+    int g;
+    auto launch = [&](auto tag) {
+      using R = decltype(tag);
+      const V<R>* a = static_cast<const V<R>*>(amps);
+      if (x == 0) {
+        g = std::min(reduce_grid(len), NOALLOC_BLOCKS);
+        k_expect_diag<R, true><<<g, REDUCE_THREADS, 0, st>>>(a, len, z, ph, scratch);
+      } else {
+        const int h = 63 - __builtin_clzll(x);
+        g = std::min(reduce_grid(len >> 1), NOALLOC_BLOCKS);
+        k_expect_pair<R, true><<<g, REDUCE_THREADS, 0, st>>>(a, len >> 1, h, x, z, ph, scratch);
+      }
+    };
+    if (precision == NCSIM_C128) launch(double());
+    else launch(float());
+    NCSIM_LAUNCHED("measure_stats_noalloc");
+    k_noalloc_finish<<<1, 32, 0, st>>>(scratch, g, 3);
+    NCSIM_LAUNCHED("measure_stats_noalloc finish");
+    double res[3];
+    NCSIM_CUDA(cudaMemcpyAsync(res, scratch + NOALLOC_RESULT, sizeof(res), cudaMemcpyDeviceToHost, st));
+    NCSIM_CUDA(cudaStreamSynchronize(st));
+    expectation_re_im[0] = res[0];
+    expectation_re_im[1] = res[1];
+    *norm_sq = res[2];
+  });
+}
