@@ -280,6 +280,11 @@ typedef struct ncsim_fused_stats {
 } ncsim_fused_stats;
 ncsim_status ncsim_sv_run_fused(ncsim_state* s, const ncsim_circuit* c, ncsim_rng* rng, uint32_t max_fuse,
                                 uint8_t* rec, size_t cap, size_t* len, ncsim_fused_stats* stats);
+/* Host-only check of the fusion planner: applies the fused form's plan of a
+ * gates-only circuit (n <= 22) to complex128 host amplitudes in FP64, in the
+ * pass, tile and op order the device uses. */
+ncsim_status ncsim_fused_emulate(const ncsim_circuit* c, uint32_t max_fuse, double* amps, uint64_t len,
+                                 ncsim_fused_stats* stats);
 
 #ifdef __cplusplus
 }

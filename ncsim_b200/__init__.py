@@ -112,6 +112,7 @@ _SIGNATURES = {
     "ncsim_sv_probability": (_i32, [_vp, _u64, _P(_dbl)]),
     "ncsim_sv_expectation_sum": (_i32, [_vp, _u64, _P(_u64), _P(_u64), _P(_u32), _P(_dbl), _P(_dbl)]),
     "ncsim_sv_run_fused": (_i32, [_vp, _vp, _vp, _u32, _P(C.c_uint8), C.c_size_t, _P(C.c_size_t), _vp]),
+    "ncsim_fused_emulate": (_i32, [_vp, _u32, _P(_dbl), _u64, _vp]),
     "ncsim_sv_timer_start": (_i32, [_vp]),
     "ncsim_sv_timer_stop": (_i32, [_vp, _P(_dbl)]),
     "ncsim_sv_compare": (_i32, [_vp, _vp, _P(_dbl), _P(_dbl), _P(_dbl), _P(_dbl)]),
@@ -323,6 +324,13 @@ class Circuit:
     @property
     def num_measurements(self) -> int:
         return self._info()[3]
+
+    def fused_emulate(self, amps: np.ndarray, max_fuse: int = 5):
+        """The fused form's plan applied on the host in FP64 (planner check)."""
+        b = np.ascontiguousarray(np.asarray(amps, dtype=np.complex128)).copy().view(np.float64)
+        st = FusedStats()
+        _check(lib().ncsim_fused_emulate(self._h, max_fuse, _dp(b), b.size // 2, C.byref(st)))
+        return b.view(np.complex128), st
 
     def to_text(self) -> str:
         n = C.c_size_t()

@@ -18,12 +18,14 @@ SOURCES = [
     "csrc/capi_state.cu",
     "csrc/kernels_plain.cu",
     "csrc/fused.cu",
+    "csrc/fused_plan.cpp",
     "csrc/host/ir.cpp",
     "csrc/host/runtime.cpp",
 ]
 HEADERS = [
     "csrc/engine.cuh",
     "csrc/host_math.hpp",
+    "csrc/fused_plan.hpp",
     "csrc/host/ir.hpp",
     "csrc/host/rng.hpp",
     "../include/ncsim_cuda.h",

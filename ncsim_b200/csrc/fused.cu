@@ -1,10 +1,574 @@
-// Precision form: fused k<=5 unitaries applied as BF16x3 tensor-core GEMMs.
+// Precision form, device side: one kernel launch per pass.
+//
+// A persistent CTA per SM streams tiles of 2^12 complex64 amplitudes (32 KB)
+// through shared memory with the bulk-copy engine (cp.async.bulk, runs of
+// >= 128 contiguous bytes, double-buffered: tile i+1 loads and tile i-1
+// stores while tile i computes).  Four warps run the pass's program on each
+// tile:
+//   unitary op: the tile as 32 rows (the unitary's 5 qubits) x 128 columns;
+//     each thread owns a column, splits its 32 amplitudes into bf16 hi/lo and
+//     writes them K-major, 128-byte swizzled (A = X^T, 128 x 64 per half);
+//     one thread issues 12 tcgen05.mma (M=128, N=64, K=16, bf16 in, f32
+//     accumulate in TMEM): D = Xhi.Rhi + Xlo.Rhi + Xhi.Rlo with R the real
+//     form [[Ur, -Ui], [Ui, Ur]] of the fused unitary (bf16 hi/lo images made
+//     on the host); each thread reads its D row back (tcgen05.ld) and writes
+//     the 32 new amplitudes into the tile;
+//   diagonal op: every amplitude times the product of the active terms.
+// The fifth warp issues the bulk copies.  Every wait on an mbarrier is
+// bounded in time: on timeout the CTA records an error code, stops, waits for
+// its own copies and frees its TMEM.
+#include <cuda_bf16.h>
+
 #include "engine.cuh"
+#include "fused_plan.hpp"
+
+#include <algorithm>
+#include <memory>
+
+namespace ncsim {
+namespace fused {
+
+namespace {
+
+constexpr int THREADS = 160;  // warps 0-3: tensor-core program; warp 4: bulk copies
+constexpr int TILE = 1 << TILE_BITS;
+constexpr uint32_t TILE_BYTES = uint32_t(TILE) * 8u;
+constexpr int OPERAND_BYTES = 16384;
+constexpr int A_BYTES = 16384;
+constexpr int SM_ROPS = 0;
+constexpr int SM_AHI = SM_ROPS + MAX_UNITARIES * OPERAND_BYTES;
+constexpr int SM_ALO = SM_AHI + A_BYTES;
+constexpr int SM_TILE0 = SM_ALO + A_BYTES;
+constexpr int SM_TOTAL = SM_TILE0 + 2 * int(TILE_BYTES);
+constexpr int SM_DYNAMIC = SM_TOTAL + 1024;  // slack to align the base to 1024 bytes
+constexpr uint32_t TMEM_COLS = 64;
+constexpr long long WAIT_CYCLES = 4000000000ll;  // about 2 s at 1.9 GHz
+
+struct OpDesc {
+  uint8_t kind;  // 0 unitary, 1 terms
+  uint8_t u;     // unitary index (operand slot)
+  uint16_t t0, t1;
+};
+
+struct TermDesc {
+  uint64_t cmask;  // bits outside the window (constant over a tile)
+  uint32_t tmask;  // tile-local bits
+  float cr, ci;
+};
+
+struct PassParams {
+  float2* amp;
+  const uint4* rops;  // nu x 16 KB operand images
+  int* err;
+  uint64_t ntiles;
+  int wl;                      // window bits 0..wl-1 are index bits 0..wl-1
+  uint8_t win[TILE_BITS];      // window qubits, ascending (tile-local bit j = win[j])
+  int nops, nu;
+  uint8_t pos[MAX_UNITARIES][GROUP_QUBITS];  // tile-local positions of each unitary's qubits
+  OpDesc ops[MAX_OPS];
+  TermDesc terms[MAX_TERMS];
+};
+
+// ---- PTX wrappers ----
+__device__ __forceinline__ uint32_t smem_u32(const void* p) { return uint32_t(__cvta_generic_to_shared(p)); }
+
+__device__ __forceinline__ void mbar_init(uint32_t bar, uint32_t count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(bar), "r"(count) : "memory");
+}
+__device__ __forceinline__ void mbar_arrive(uint32_t bar) {
+  asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(bar) : "memory");
+}
+__device__ __forceinline__ void mbar_expect_tx(uint32_t bar, uint32_t bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar), "r"(bytes) : "memory");
+}
+__device__ __forceinline__ bool mbar_try(uint32_t bar, uint32_t parity) {
+  uint32_t ok;
+  asm volatile(
+      "{\n\t.reg .pred p;\n\t"
+      "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+      "selp.u32 %0, 1, 0, p;\n\t}"
+      : "=r"(ok)
+      : "r"(bar), "r"(parity)
+      : "memory");
+  return ok != 0;
+}
+// bounded wait: false when the phase did not complete within WAIT_CYCLES
+__device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t parity) {
+  const long long t0 = clock64();
+  while (!mbar_try(bar, parity)) {
+    if (clock64() - t0 > WAIT_CYCLES) return false;
+  }
+  return true;
+}
+
+__device__ __forceinline__ void bulk_load(uint32_t dst, const void* src, uint32_t bytes, uint32_t bar) {
+  asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(dst),
+               "l"(src), "r"(bytes), "r"(bar)
+               : "memory");
+}
+__device__ __forceinline__ void bulk_store(void* dst, uint32_t src, uint32_t bytes) {
+  asm volatile("cp.async.bulk.global.shared::cta.bulk_group [%0], [%1], %2;" ::"l"(dst), "r"(src), "r"(bytes) : "memory");
+}
+__device__ __forceinline__ void bulk_commit() { asm volatile("cp.async.bulk.commit_group;" ::: "memory"); }
+__device__ __forceinline__ void bulk_wait_read_all() { asm volatile("cp.async.bulk.wait_group.read 0;" ::: "memory"); }
+__device__ __forceinline__ void bulk_wait_all() { asm volatile("cp.async.bulk.wait_group 0;" ::: "memory"); }
+__device__ __forceinline__ void fence_async_smem() { asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); }
+__device__ __forceinline__ void bar_compute() { asm volatile("bar.sync 1, 128;" ::: "memory"); }
+
+__device__ __forceinline__ void tc_fence_before() { asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory"); }
+__device__ __forceinline__ void tc_fence_after() { asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory"); }
+
+// K-major, 128-byte swizzle, 8-row atoms 1024 bytes apart (sm100 descriptor version 1)
+__device__ __forceinline__ uint64_t sw128_desc(uint32_t saddr) {
+  uint64_t d = uint64_t((saddr >> 4) & 0x3FFFu);
+  d |= uint64_t(1) << 16;            // leading byte offset (16 B; unused by swizzled K-major)
+  d |= uint64_t(1024 >> 4) << 32;    // stride byte offset between 8-row atoms
+  d |= uint64_t(1) << 46;            // descriptor version for sm100
+  d |= uint64_t(2) << 61;            // SWIZZLE_128B
+  return d;
+}
+
+__device__ __forceinline__ void mma_bf16(uint32_t tmem_d, uint64_t a, uint64_t b, uint32_t idesc, uint32_t acc) {
+  asm volatile(
+      "{\n\t.reg .pred p;\n\t"
+      "setp.ne.b32 p, %4, 0;\n\t"
+      "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, {%5, %6, %7, %8}, p;\n\t}"
+      ::"r"(tmem_d), "l"(a), "l"(b), "r"(idesc), "r"(acc), "r"(0), "r"(0), "r"(0), "r"(0));
+}
+__device__ __forceinline__ void mma_commit(uint32_t bar) {
+  asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(bar) : "memory");
+}
+
+#define NCSIM_TMEM_LD32(taddr, r)                                                                                    \
+  asm volatile(                                                                                                      \
+      "tcgen05.ld.sync.aligned.32x32b.x32.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15,%16,%17,%18,%19," \
+      "%20,%21,%22,%23,%24,%25,%26,%27,%28,%29,%30,%31}, [%32];"                                                     \
+      : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]), "=r"(r[8]),  \
+        "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15]), "=r"(r[16]),       \
+        "=r"(r[17]), "=r"(r[18]), "=r"(r[19]), "=r"(r[20]), "=r"(r[21]), "=r"(r[22]), "=r"(r[23]), "=r"(r[24]),      \
+        "=r"(r[25]), "=r"(r[26]), "=r"(r[27]), "=r"(r[28]), "=r"(r[29]), "=r"(r[30]), "=r"(r[31])                    \
+      : "r"(taddr))
+
+__device__ __forceinline__ uint32_t pack_bf16(float a, float b) {
+  __nv_bfloat162 v = __floats2bfloat162_rn(a, b);
+  return *reinterpret_cast<uint32_t*>(&v);
+}
+__device__ __forceinline__ float bf16_round(float a) { return __bfloat162float(__float2bfloat16_rn(a)); }
+
+// index of tile-local element e of a tile whose base index is `base`
+__device__ __forceinline__ uint64_t global_index(uint64_t base, uint32_t e, const PassParams& P) {
+  uint64_t g = base | (e & ((1u << P.wl) - 1));
+  for (int j = P.wl; j < TILE_BITS; ++j) g |= uint64_t((e >> j) & 1u) << P.win[j];
+  return g;
+}
+// the tile's base: the tile number deposited into the bits outside the window
+__device__ __forceinline__ uint64_t tile_base(uint64_t t, const PassParams& P) {
+  uint64_t v = t;
+  for (int j = 0; j < TILE_BITS; ++j) {
+    const int b = P.win[j];
+    v = ((v >> b) << (b + 1)) | (v & ((uint64_t(1) << b) - 1));
+  }
+  return v;
+}
+
+__global__ void __launch_bounds__(THREADS, 1) k_fused_pass(const __grid_constant__ PassParams P) {
+  extern __shared__ uint8_t smem_raw[];
+  uint8_t* smem = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
+  __shared__ __align__(8) uint64_t bars[5];  // full[2], done[2], mma
+  __shared__ uint32_t tmem_base_sh;
+  __shared__ volatile int abort_sh;
+  __shared__ uint16_t rowoff[MAX_UNITARIES][32];
+  __shared__ uint8_t nongate[MAX_UNITARIES][TILE_BITS - GROUP_QUBITS];
+
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  const uint32_t bar_full0 = smem_u32(&bars[0]), bar_done0 = smem_u32(&bars[2]), bar_mma = smem_u32(&bars[4]);
+  auto bar_full = [&](int b) { return bar_full0 + 8u * uint32_t(b); };
+  auto bar_done = [&](int b) { return bar_done0 + 8u * uint32_t(b); };
+  auto fail = [&](int code) {
+    abort_sh = 1;
+    atomicCAS(P.err, 0, code);
+  };
+
+  if (tid == 0) {
+    mbar_init(bar_full(0), 1);
+    mbar_init(bar_full(1), 1);
+    mbar_init(bar_done(0), 128);
+    mbar_init(bar_done(1), 128);
+    mbar_init(bar_mma, 1);
+    abort_sh = 0;
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  if (warp == 0) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(&tmem_base_sh)),
+                 "r"(TMEM_COLS));
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
+  }
+  // operand images and per-unitary index tables
+  {
+    uint4* dst = reinterpret_cast<uint4*>(smem + SM_ROPS);
+    const int n16 = P.nu * (OPERAND_BYTES / 16);
+    for (int i = tid; i < n16; i += THREADS) dst[i] = P.rops[i];
+    for (int i = tid; i < P.nu * 32; i += THREADS) {
+      const int u = i >> 5, r = i & 31;
+      uint32_t o = 0;
+      for (int j = 0; j < GROUP_QUBITS; ++j) o |= uint32_t((r >> j) & 1) << P.pos[u][j];
+      rowoff[u][r] = uint16_t(o);
+    }
+    for (int u = tid; u < P.nu; u += THREADS) {
+      uint32_t gm = 0;
+      for (int j = 0; j < GROUP_QUBITS; ++j) gm |= 1u << P.pos[u][j];
+      int m = 0;
+      for (int b = 0; b < TILE_BITS; ++b)
+        if (!((gm >> b) & 1)) nongate[u][m++] = uint8_t(b);
+    }
+  }
+  fence_async_smem();
+  tc_fence_before();
+  __syncthreads();
+  tc_fence_after();
+  const uint32_t tmem = tmem_base_sh;
+  const uint64_t my_tiles = P.ntiles > blockIdx.x ? (P.ntiles - 1 - blockIdx.x) / gridDim.x + 1 : 0;
+  float2* tiles = reinterpret_cast<float2*>(smem + SM_TILE0);
+
+  if (warp == 4) {
+    // ---------------- bulk-copy producer ----------------
+    const uint32_t run_elems = 1u << P.wl, run_bytes = run_elems * 8u, nruns = uint32_t(TILE) >> P.wl;
+    auto copy_tile = [&](uint64_t it, int b, bool load) {
+      const uint64_t t = uint64_t(blockIdx.x) + it * gridDim.x;
+      const uint64_t base = tile_base(t, P);
+      float2* buf = tiles + size_t(b) * TILE;
+      for (uint32_t r = lane; r < nruns; r += 32) {
+        const uint32_t e = r << P.wl;
+        float2* g = P.amp + global_index(base, e, P);
+        if (load) bulk_load(smem_u32(buf + e), g, run_bytes, bar_full(b));
+        else bulk_store(g, smem_u32(buf + e), run_bytes);
+      }
+    };
+    uint64_t it = 0;
+    for (; it < my_tiles; ++it) {
+      const int b = int(it & 1);
+      if (it >= 2) {
+        bool ok = true;
+        if (lane == 0) ok = mbar_wait(bar_done(b), uint32_t(((it - 2) >> 1) & 1));
+        ok = __shfl_sync(0xffffffffu, ok, 0);
+        if (!ok || abort_sh) {
+          if (lane == 0 && !ok) fail(3);
+          break;
+        }
+        copy_tile(it - 2, b, false);
+        bulk_commit();
+        bulk_wait_read_all();
+        __syncwarp();
+      }
+      if (lane == 0) mbar_expect_tx(bar_full(b), TILE_BYTES);
+      __syncwarp();
+      copy_tile(it, b, true);
+    }
+    if (!abort_sh) {
+      // the last (up to two) tiles
+      for (uint64_t j = my_tiles >= 2 ? my_tiles - 2 : 0; j < my_tiles; ++j) {
+        const int b = int(j & 1);
+        bool ok = true;
+        if (lane == 0) ok = mbar_wait(bar_done(b), uint32_t((j >> 1) & 1));
+        ok = __shfl_sync(0xffffffffu, ok, 0);
+        if (!ok) {
+          if (lane == 0) fail(3);
+          break;
+        }
+        copy_tile(j, b, false);
+        bulk_commit();
+      }
+    } else if (it > 0) {
+      // an abort: let the loads already issued land before the CTA exits
+      for (uint64_t j = it >= 2 ? it - 2 : 0; j < it; ++j)
+        if (lane == 0) mbar_wait(bar_full(int(j & 1)), uint32_t((j >> 1) & 1));
+    }
+    bulk_wait_all();
+  } else {
+    // ---------------- tensor-core program ----------------
+    const uint32_t idesc = (1u << 4) | (1u << 7) | (1u << 10) | ((64u >> 3) << 17) | ((128u >> 4) << 24);
+    const uint32_t a_hi = smem_u32(smem + SM_AHI), a_lo = smem_u32(smem + SM_ALO);
+    const uint32_t taddr = tmem + (uint32_t(warp * 32) << 16);
+    uint32_t mma_phase = 0;
+    for (uint64_t it = 0; it < my_tiles; ++it) {
+      const int b = int(it & 1);
+      if (!mbar_wait(bar_full(b), uint32_t((it >> 1) & 1))) fail(1);
+      bar_compute();
+      if (abort_sh) break;
+      const uint64_t t = uint64_t(blockIdx.x) + it * gridDim.x;
+      const uint64_t base = tile_base(t, P);
+      float2* T = tiles + size_t(b) * TILE;
+      for (int oi = 0; oi < P.nops; ++oi) {
+        const OpDesc op = P.ops[oi];
+        if (op.kind == 1) {
+          float2 v[32];
+#pragma unroll
+          for (int i = 0; i < 32; ++i) v[i] = T[tid + 128 * i];
+          for (int k = op.t0; k < op.t1; ++k) {
+            const TermDesc tm = P.terms[k];
+            if ((base & tm.cmask) != tm.cmask) continue;
+#pragma unroll
+            for (int i = 0; i < 32; ++i) {
+              const uint32_t e = uint32_t(tid + 128 * i);
+              if ((e & tm.tmask) == tm.tmask) {
+                const float x = v[i].x, y = v[i].y;
+                v[i].x = tm.cr * x - tm.ci * y;
+                v[i].y = tm.cr * y + tm.ci * x;
+              }
+            }
+          }
+#pragma unroll
+          for (int i = 0; i < 32; ++i) T[tid + 128 * i] = v[i];
+          bar_compute();
+          continue;
+        }
+        // ---- unitary op ----
+        const int u = op.u;
+        uint32_t cb = 0;
+#pragma unroll
+        for (int j = 0; j < TILE_BITS - GROUP_QUBITS; ++j) cb |= uint32_t((tid >> j) & 1) << nongate[u][j];
+        float2 x[32];
+#pragma unroll
+        for (int r = 0; r < 32; ++r) x[r] = T[cb | rowoff[u][r]];
+        const uint32_t row7 = uint32_t(tid) & 7u;
+        uint8_t* ahi = smem + SM_AHI + (tid >> 3) * 1024 + row7 * 128;
+        uint8_t* alo = smem + SM_ALO + (tid >> 3) * 1024 + row7 * 128;
+#pragma unroll
+        for (int j = 0; j < 4; ++j) {
+          uint32_t hr[4], lr[4], hm[4], lm[4];
+#pragma unroll
+          for (int i = 0; i < 4; ++i) {
+            const float2 p0 = x[8 * j + 2 * i], p1 = x[8 * j + 2 * i + 1];
+            const float h0 = bf16_round(p0.x), h1 = bf16_round(p1.x);
+            const float g0 = bf16_round(p0.y), g1 = bf16_round(p1.y);
+            hr[i] = pack_bf16(h0, h1);
+            lr[i] = pack_bf16(p0.x - h0, p1.x - h1);
+            hm[i] = pack_bf16(g0, g1);
+            lm[i] = pack_bf16(p0.y - g0, p1.y - g1);
+          }
+          *reinterpret_cast<uint4*>(ahi + ((uint32_t(j) ^ row7) << 4)) = make_uint4(hr[0], hr[1], hr[2], hr[3]);
+          *reinterpret_cast<uint4*>(alo + ((uint32_t(j) ^ row7) << 4)) = make_uint4(lr[0], lr[1], lr[2], lr[3]);
+          *reinterpret_cast<uint4*>(ahi + ((uint32_t(j + 4) ^ row7) << 4)) = make_uint4(hm[0], hm[1], hm[2], hm[3]);
+          *reinterpret_cast<uint4*>(alo + ((uint32_t(j + 4) ^ row7) << 4)) = make_uint4(lm[0], lm[1], lm[2], lm[3]);
+        }
+        fence_async_smem();
+        bar_compute();
+        if (tid == 0) {
+          tc_fence_after();
+          const uint32_t b_hi = smem_u32(smem + SM_ROPS + u * OPERAND_BYTES);
+          const uint32_t b_lo = b_hi + OPERAND_BYTES / 2;
+          const uint64_t dah = sw128_desc(a_hi), dal = sw128_desc(a_lo), dbh = sw128_desc(b_hi), dbl = sw128_desc(b_lo);
+#pragma unroll
+          for (int s = 0; s < 4; ++s) mma_bf16(tmem, dah + 2 * s, dbh + 2 * s, idesc, s > 0);
+#pragma unroll
+          for (int s = 0; s < 4; ++s) mma_bf16(tmem, dal + 2 * s, dbh + 2 * s, idesc, 1);
+#pragma unroll
+          for (int s = 0; s < 4; ++s) mma_bf16(tmem, dah + 2 * s, dbl + 2 * s, idesc, 1);
+          mma_commit(bar_mma);
+        }
+        if (!mbar_wait(bar_mma, mma_phase)) fail(2);
+        mma_phase ^= 1u;
+        tc_fence_after();
+        uint32_t re[32], im[32];
+        NCSIM_TMEM_LD32(taddr, re);
+        NCSIM_TMEM_LD32(taddr + 32u, im);
+        asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+#pragma unroll
+        for (int r = 0; r < 32; ++r) T[cb | rowoff[u][r]] = make_float2(__uint_as_float(re[r]), __uint_as_float(im[r]));
+        tc_fence_before();
+        bar_compute();
+        if (abort_sh) break;
+      }
+      fence_async_smem();
+      mbar_arrive(bar_done(b));
+      if (abort_sh) break;
+    }
+  }
+  tc_fence_before();
+  __syncthreads();
+  if (warp == 0) {
+    tc_fence_after();
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(TMEM_COLS));
+  }
+}
+
+// ---------------------------------------------------------------------------
+// device copy of a plan: every pass's operand images in one buffer
+struct DevicePlan {
+  Plan plan;
+  std::vector<PassParams> params;  // per pass, in segment order (amp/err filled per run)
+  uint8_t* rops = nullptr;
+  int device = -1;
+  ~DevicePlan() {
+    if (rops) cudaFree(rops);
+  }
+};
+
+std::unique_ptr<DevicePlan> build_device_plan(const ncsim_circuit& c, uint32_t max_fuse) {
+  auto dp = std::make_unique<DevicePlan>();
+  dp->plan = make_plan(c, max_fuse);
+  std::vector<uint8_t> images;
+  std::vector<size_t> offsets;
+  for (const Segment& s : dp->plan.segments) {
+    if (!s.fused) continue;
+    for (const Pass& ps : s.passes) {
+      PassParams P{};
+      P.ntiles = (uint64_t(1) << c.n) >> TILE_BITS;
+      uint64_t wmask = 0;
+      for (int j = 0; j < TILE_BITS; ++j) P.win[j] = uint8_t(ps.window[j]), wmask |= uint64_t(1) << ps.window[j];
+      int wl = 0;
+      while (wl < TILE_BITS && ps.window[wl] == uint32_t(wl)) ++wl;
+      if (wl < LOW_BITS) throw Error(NCSIM_ERR_INVALID, "fused pass window lacks the low index bits");
+      P.wl = wl;
+      int nu = 0, nt = 0, no = 0;
+      for (const FusedOp& op : ps.ops) {
+        OpDesc d{};
+        if (op.kind == 0) {
+          if (nu >= MAX_UNITARIES) throw Error(NCSIM_ERR_INVALID, "fused pass has too many unitaries");
+          d.kind = 0;
+          d.u = uint8_t(nu);
+          for (int j = 0; j < GROUP_QUBITS; ++j) {
+            auto it = std::find(ps.window.begin(), ps.window.end(), op.qubits[j]);
+            if (it == ps.window.end()) throw Error(NCSIM_ERR_INVALID, "fused unitary outside its window");
+            P.pos[nu][j] = uint8_t(it - ps.window.begin());
+          }
+          const size_t at = images.size();
+          images.resize(at + OPERAND_BYTES);
+          build_operand_image(op.u, images.data() + at);
+          offsets.push_back(at);
+          ++nu;
+        } else {
+          d.kind = 1;
+          d.t0 = uint16_t(nt);
+          for (const Term& t : op.terms) {
+            if (nt >= MAX_TERMS) throw Error(NCSIM_ERR_INVALID, "fused pass has too many terms");
+            TermDesc td{};
+            uint32_t tm = 0;
+            for (int j = 0; j < TILE_BITS; ++j)
+              if ((t.mask >> ps.window[j]) & 1) tm |= 1u << j;
+            td.tmask = tm;
+            td.cmask = t.mask & ~wmask;
+            td.cr = float(t.c.re);
+            td.ci = float(t.c.im);
+            P.terms[nt++] = td;
+          }
+          d.t1 = uint16_t(nt);
+        }
+        if (no >= MAX_OPS) throw Error(NCSIM_ERR_INVALID, "fused pass has too many ops");
+        P.ops[no++] = d;
+      }
+      P.nops = no;
+      P.nu = nu;
+      // the pass's first operand: an offset for now, a device pointer below
+      P.rops = reinterpret_cast<const uint4*>(uintptr_t(nu ? offsets[offsets.size() - nu] : 0));
+      dp->params.push_back(P);
+    }
+  }
+  if (!images.empty()) {
+    NCSIM_CUDA(cudaMalloc(&dp->rops, images.size()));
+    NCSIM_CUDA(cudaMemcpy(dp->rops, images.data(), images.size(), cudaMemcpyHostToDevice));
+  }
+  for (auto& P : dp->params) P.rops = reinterpret_cast<const uint4*>(dp->rops + uintptr_t(P.rops));
+  NCSIM_CUDA(cudaGetDevice(&dp->device));
+  return dp;
+}
+
+}  // namespace
+
+}  // namespace fused
+
+int apply_op(ncsim_state* s, const OpIR& op, ncsim_rng& rng);
+
+}  // namespace ncsim
 
 using namespace ncsim;
 
+namespace {
+std::mutex g_fused_mu;
+
+// the circuit's device plan for this device and fusion width (built once)
+std::shared_ptr<fused::DevicePlan> device_plan_for(const ncsim_circuit* c, uint32_t max_fuse) {
+  std::lock_guard<std::mutex> lk(g_fused_mu);
+  int dev = 0;
+  NCSIM_CUDA(cudaGetDevice(&dev));
+  if (c->fused_plan && c->fused_plan_fuse == max_fuse && c->fused_plan_device == dev)
+    return std::static_pointer_cast<fused::DevicePlan>(c->fused_plan);
+  std::shared_ptr<fused::DevicePlan> dp(fused::build_device_plan(*c, max_fuse).release());
+  c->fused_plan = dp;
+  c->fused_plan_fuse = max_fuse;
+  c->fused_plan_device = dev;
+  return dp;
+}
+}  // namespace
+
 extern "C" ncsim_status ncsim_sv_run_fused(ncsim_state* s, const ncsim_circuit* c, ncsim_rng* rng, uint32_t max_fuse,
                                            uint8_t* rec, size_t cap, size_t* len, ncsim_fused_stats* stats) {
-  (void)s, (void)c, (void)rng, (void)max_fuse, (void)rec, (void)cap, (void)len, (void)stats;
-  return guarded([&] { throw Error(NCSIM_ERR_UNSUPPORTED, "the fused precision form is not built yet"); });
+  return guarded([&] {
+    if (!s || !c || !rng) throw Error(NCSIM_ERR_INVALID, "null argument");
+    if (s->precision != NCSIM_C64) throw Error(NCSIM_ERR_INVALID, "the fused form runs on complex64 states");
+    if (c->n != s->n) throw Error(NCSIM_ERR_INVALID, "circuit on a different register");
+    if (c->num_measurements() > cap) throw Error(NCSIM_ERR_INVALID, "record buffer too small");
+    if (c->num_measurements()) {
+      if (!rec) throw Error(NCSIM_ERR_INVALID, "record is null");
+    }
+    std::lock_guard<std::recursive_mutex> lk(s->mu);
+    std::shared_ptr<fused::DevicePlan> dp = device_plan_for(c, max_fuse ? max_fuse : 5);
+    int* d_err = nullptr;
+    NCSIM_CUDA(cudaMallocAsync(&d_err, sizeof(int), s->stream));
+    NCSIM_CUDA(cudaMemsetAsync(d_err, 0, sizeof(int), s->stream));
+    NCSIM_CUDA(cudaFuncSetAttribute(fused::k_fused_pass, cudaFuncAttributeMaxDynamicSharedMemorySize, fused::SM_DYNAMIC));
+    const unsigned grid = unsigned(std::min<uint64_t>(uint64_t(sm_count()), s->len >> fused::TILE_BITS));
+    size_t m = 0, pi = 0;
+    uint64_t gemm = 0;
+    for (const fused::Segment& seg : dp->plan.segments) {
+      if (!seg.fused) {
+        int r = apply_op(s, c->ops[seg.op], *rng);
+        if (r >= 0) rec[m++] = uint8_t(r);
+        continue;
+      }
+      for (size_t k = 0; k < seg.passes.size(); ++k, ++pi) {
+        fused::PassParams P = dp->params[pi];
+        P.amp = reinterpret_cast<float2*>(s->amp);
+        P.err = d_err;
+        gemm += uint64_t(P.nu);
+        ProfScope ps(s, K_FUSED_GEMM, 2.0 * double(s->bytes()));
+        fused::k_fused_pass<<<grid, fused::THREADS, fused::SM_DYNAMIC, s->stream>>>(P);
+        NCSIM_LAUNCHED("fused pass");
+      }
+    }
+    int h_err = 0;
+    NCSIM_CUDA(cudaMemcpyAsync(&h_err, d_err, sizeof(int), cudaMemcpyDeviceToHost, s->stream));
+    NCSIM_CUDA(cudaFreeAsync(d_err, s->stream));
+    NCSIM_CUDA(cudaStreamSynchronize(s->stream));
+    if (h_err) throw Error(NCSIM_ERR_DEVICE, "fused pass stopped: a bounded wait timed out (code " + std::to_string(h_err) + ")");
+    if (len) *len = m;
+    if (stats) {
+      stats->source_gates = dp->plan.source_gates;
+      stats->fused_unitaries = dp->plan.unitaries;
+      stats->passes = dp->plan.passes;
+      stats->remap_passes = 0;
+      stats->gemm_launches = gemm;
+    }
+  });
+}
+
+extern "C" ncsim_status ncsim_fused_emulate(const ncsim_circuit* c, uint32_t max_fuse, double* amps, uint64_t len,
+                                            ncsim_fused_stats* stats) {
+  return guarded([&] {
+    if (!c || !amps) throw Error(NCSIM_ERR_INVALID, "null argument");
+    if (c->n > 22) throw Error(NCSIM_ERR_UNSUPPORTED, "emulation is for registers of at most 22 qubits");
+    if (len != (uint64_t(1) << c->n)) throw Error(NCSIM_ERR_INVALID, "amplitude buffer length differs from 2^n");
+    fused::Plan p = fused::make_plan(*c, max_fuse ? max_fuse : 5);
+    std::vector<CplxD> a(len);
+    for (uint64_t i = 0; i < len; ++i) a[i] = {amps[2 * i], amps[2 * i + 1]};
+    fused::emulate(p, *c, a);
+    for (uint64_t i = 0; i < len; ++i) amps[2 * i] = a[i].re, amps[2 * i + 1] = a[i].im;
+    if (stats) {
+      stats->source_gates = p.source_gates;
+      stats->fused_unitaries = p.unitaries;
+      stats->passes = p.passes;
+      stats->remap_passes = 0;
+      stats->gemm_launches = p.passes;
+    }
+  });
 }

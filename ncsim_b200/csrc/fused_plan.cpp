@@ -1,0 +1,508 @@
+// Precision form, host side: planning, fusion, operand images, emulation.
+#include "fused_plan.hpp"
+
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <map>
+
+namespace ncsim {
+namespace fused {
+
+namespace {
+
+enum class GClass { Skip, Diag, Dense, Plain };
+
+struct GInfo {
+  GClass cls = GClass::Skip;
+  std::vector<uint32_t> q;
+  std::vector<CplxD> m;  // Dense: 2^k x 2^k row-major
+  std::vector<CplxD> d;  // Diag: 2^k entries
+  uint64_t mask = 0;
+};
+
+inline CplxD mul(CplxD a, CplxD b) { return {a.re * b.re - a.im * b.im, a.re * b.im + a.im * b.re}; }
+inline CplxD inv(CplxD a) {
+  const double s = a.re * a.re + a.im * a.im;
+  return {a.re / s, -a.im / s};
+}
+inline bool exactly_one(CplxD c) { return c.re == 1.0 && c.im == 0.0; }
+
+GInfo classify(const OpIR& op) {
+  GInfo g;
+  if (op.kind == OpKind::Tick || op.kind == OpKind::Detector || op.kind == OpKind::Observable) return g;
+  if (op.kind != OpKind::Gate) {
+    g.cls = GClass::Plain;
+    return g;
+  }
+  const LoweredOp& lo = op.lowered;
+  g.q = lo.qubits;
+  for (uint32_t q : g.q) g.mask |= uint64_t(1) << q;
+  const size_t k = g.q.size(), d = size_t(1) << k;
+  switch (lo.kind) {
+    case LoweredKind::Nothing: g.cls = GClass::Skip; return g;
+    case LoweredKind::PhasePoly:
+    case LoweredKind::Pauli: g.cls = GClass::Plain; return g;
+    case LoweredKind::Dense: {
+      bool diag = true;
+      for (size_t r = 0; r < d && diag; ++r)
+        for (size_t c = 0; c < d; ++c)
+          if (r != c && (lo.matrix[r * d + c].re != 0.0 || lo.matrix[r * d + c].im != 0.0)) {
+            diag = false;
+            break;
+          }
+      if (diag && k <= 3) {
+        g.cls = GClass::Diag;
+        for (size_t x = 0; x < d; ++x) g.d.push_back(lo.matrix[x * d + x]);
+      } else if (k <= size_t(GROUP_QUBITS)) {
+        g.cls = GClass::Dense;
+        g.m = lo.matrix;
+      } else {
+        g.cls = GClass::Plain;
+      }
+      return g;
+    }
+    case LoweredKind::Monomial: {
+      bool ident = true;
+      for (size_t x = 0; x < d; ++x) ident &= lo.image[x] == x;
+      if (ident && k <= 3) {
+        g.cls = GClass::Diag;
+        g.d = lo.matrix;
+      } else if (k <= size_t(GROUP_QUBITS)) {
+        g.cls = GClass::Dense;
+        g.m.assign(d * d, CplxD{0, 0});
+        for (size_t x = 0; x < d; ++x) g.m[size_t(lo.image[x]) * d + x] = lo.matrix[x];
+      } else {
+        g.cls = GClass::Plain;
+      }
+      return g;
+    }
+  }
+  g.cls = GClass::Plain;
+  return g;
+}
+
+// diag(d) over local bits -> product of (mask, c) terms: c_S = prod_{T in S} d[T]^{(-1)^{|S|-|T|}}
+void diag_terms(const GInfo& g, std::vector<Term>& out) {
+  const size_t k = g.q.size(), dsz = size_t(1) << k;
+  for (size_t s = 0; s < dsz; ++s) {
+    CplxD c{1.0, 0.0};
+    for (size_t t = s;; t = (t - 1) & s) {
+      const int sign = (__builtin_popcountll(s) - __builtin_popcountll(t)) & 1;
+      c = mul(c, sign ? inv(g.d[t]) : g.d[t]);
+      if (t == 0) break;
+    }
+    if (exactly_one(c)) continue;
+    uint64_t m = 0;
+    for (size_t j = 0; j < k; ++j)
+      if ((s >> j) & 1) m |= uint64_t(1) << g.q[j];
+    out.push_back({m, c});
+  }
+}
+
+// An open fused group: a unitary over the local qubits q (bit j = q[j]).
+struct Group {
+  std::vector<uint32_t> q;
+  std::vector<CplxD> u;  // 2^|q| square
+  uint64_t mask = 0;
+  bool open = false;
+
+  void start() {
+    q.clear();
+    u.assign(1, CplxD{1.0, 0.0});
+    mask = 0;
+    open = true;
+  }
+  void add_qubit(uint32_t qb) {
+    const size_t d = size_t(1) << q.size();
+    std::vector<CplxD> nu(4 * d * d, CplxD{0, 0});
+    // U (x) I on the new highest local bit
+    for (size_t h = 0; h < 2; ++h)
+      for (size_t r = 0; r < d; ++r)
+        for (size_t c = 0; c < d; ++c) nu[(h * d + r) * (2 * d) + (h * d + c)] = u[r * d + c];
+    u.swap(nu);
+    q.push_back(qb);
+    mask |= uint64_t(1) << qb;
+  }
+  int local_of(uint32_t qb) const {
+    for (size_t j = 0; j < q.size(); ++j)
+      if (q[j] == qb) return int(j);
+    return -1;
+  }
+  // U <- G U for a dense gate G on (a subset of) the group's qubits
+  void apply_dense(const std::vector<uint32_t>& gq, const std::vector<CplxD>& gm) {
+    for (uint32_t qb : gq)
+      if (local_of(qb) < 0) add_qubit(qb);
+    const size_t d = size_t(1) << q.size(), k = gq.size(), gd = size_t(1) << k;
+    std::vector<int> pos(k);
+    uint64_t gmask = 0;
+    for (size_t j = 0; j < k; ++j) pos[j] = local_of(gq[j]), gmask |= uint64_t(1) << pos[j];
+    std::vector<CplxD> nu(d * d, CplxD{0, 0});
+    for (size_t row = 0; row < d; ++row) {
+      size_t a = 0;
+      for (size_t j = 0; j < k; ++j) a |= ((row >> pos[j]) & 1) << j;
+      const size_t rest = row & ~gmask;
+      for (size_t b = 0; b < gd; ++b) {
+        const CplxD gv = gm[a * gd + b];
+        if (gv.re == 0.0 && gv.im == 0.0) continue;
+        size_t src = rest;
+        for (size_t j = 0; j < k; ++j) src |= ((b >> j) & 1) << pos[j];
+        for (size_t c = 0; c < d; ++c) {
+          const CplxD t = mul(gv, u[src * d + c]);
+          nu[row * d + c].re += t.re;
+          nu[row * d + c].im += t.im;
+        }
+      }
+    }
+    u.swap(nu);
+  }
+  void apply_diag(const std::vector<uint32_t>& gq, const std::vector<CplxD>& dg) {
+    const size_t d = size_t(1) << q.size();
+    std::vector<int> pos(gq.size());
+    for (size_t j = 0; j < gq.size(); ++j) pos[j] = local_of(gq[j]);
+    for (size_t row = 0; row < d; ++row) {
+      size_t a = 0;
+      for (size_t j = 0; j < gq.size(); ++j) a |= ((row >> pos[j]) & 1) << j;
+      for (size_t c = 0; c < d; ++c) u[row * d + c] = mul(dg[a], u[row * d + c]);
+    }
+  }
+};
+
+std::vector<Term> merge_terms(const std::vector<Term>& in) {
+  std::map<uint64_t, CplxD> acc;
+  for (auto& t : in) {
+    auto it = acc.find(t.mask);
+    if (it == acc.end()) acc[t.mask] = t.c;
+    else it->second = mul(it->second, t.c);
+  }
+  std::vector<Term> out;
+  for (auto& kv : acc)
+    if (!exactly_one(kv.second)) out.push_back({kv.first, kv.second});
+  return out;
+}
+
+struct PassBuilder {
+  uint64_t window = 0;
+  Pass pass;
+  Group g;
+  std::vector<Term> pending;
+  uint64_t pending_mask = 0;
+  int emitted_unitaries = 0;
+  size_t term_count = 0;
+
+  void emit_group() {
+    if (!g.open) return;
+    // pad to exactly 5 window qubits (U (x) I)
+    for (int b = 0; b < 64 && g.q.size() < size_t(GROUP_QUBITS); ++b)
+      if (((window >> b) & 1) && g.local_of(uint32_t(b)) < 0) g.add_qubit(uint32_t(b));
+    FusedOp op;
+    op.kind = 0;
+    op.qubits = g.q;
+    op.u = g.u;
+    pass.ops.push_back(std::move(op));
+    ++emitted_unitaries;
+    g.open = false;
+  }
+  void emit_pending() {
+    if (pending.empty()) return;
+    FusedOp op;
+    op.kind = 1;
+    op.terms = merge_terms(pending);
+    if (!op.terms.empty()) pass.ops.push_back(std::move(op));
+    pending.clear();
+    pending_mask = 0;
+  }
+  // false: the gate does not fit this pass's limits (the caller cuts here)
+  bool add(const GInfo& gi, int maxk) {
+    if (gi.cls == GClass::Diag) {
+      if (g.open && (gi.mask & ~g.mask) == 0) {
+        g.apply_diag(gi.q, gi.d);
+        return true;
+      }
+      std::vector<Term> t;
+      diag_terms(gi, t);
+      if (term_count + t.size() > size_t(MAX_TERMS)) return false;
+      if (pass.ops.size() + 3 > size_t(MAX_OPS)) return false;
+      term_count += t.size();
+      pending.insert(pending.end(), t.begin(), t.end());
+      pending_mask |= gi.mask;
+      return true;
+    }
+    if (g.open && __builtin_popcountll(g.mask | gi.mask) <= maxk && !(gi.mask & pending_mask)) {
+      g.apply_dense(gi.q, gi.m);
+      return true;
+    }
+    // a new group
+    if (emitted_unitaries + (g.open ? 1 : 0) + 1 > MAX_UNITARIES) return false;
+    if (pass.ops.size() + 3 > size_t(MAX_OPS)) return false;
+    emit_group();
+    emit_pending();
+    g.start();
+    g.apply_dense(gi.q, gi.m);
+    return true;
+  }
+  Pass finish(uint32_t n) {
+    emit_group();
+    emit_pending();
+    // window: exactly TILE_BITS qubits, ascending
+    uint64_t w = window;
+    for (uint32_t b = 0; b < n && __builtin_popcountll(w) < TILE_BITS; ++b) w |= uint64_t(1) << b;
+    pass.window.clear();
+    for (uint32_t b = 0; b < 64; ++b)
+      if ((w >> b) & 1) pass.window.push_back(b);
+    pass.unitaries = emitted_unitaries;
+    return std::move(pass);
+  }
+};
+
+// Passes for a run of fusable gates, in dependency order.
+void plan_run(const std::vector<GInfo>& gs, uint32_t n, int maxk, std::vector<Pass>& out, Plan& stats) {
+  std::vector<size_t> remaining(gs.size());
+  for (size_t i = 0; i < gs.size(); ++i) remaining[i] = i;
+  const uint64_t low = (uint64_t(1) << LOW_BITS) - 1;
+  while (!remaining.empty()) {
+    // choose the window and the gates it can take (gates behind a blocked qubit wait)
+    uint64_t W = low, blocked = 0;
+    std::vector<size_t> inc, rest;
+    for (size_t i : remaining) {
+      const GInfo& g = gs[i];
+      if (g.mask & blocked) {
+        blocked |= g.mask;
+        rest.push_back(i);
+      } else if (g.cls == GClass::Diag) {
+        inc.push_back(i);
+      } else if (__builtin_popcountll(W | g.mask) <= TILE_BITS) {
+        W |= g.mask;
+        inc.push_back(i);
+      } else {
+        blocked |= g.mask;
+        rest.push_back(i);
+      }
+    }
+    // the window: exactly TILE_BITS qubits (filled with the lowest free ones)
+    for (uint32_t b = 0; b < n && __builtin_popcountll(W) < TILE_BITS; ++b) W |= uint64_t(1) << b;
+    // fuse; gates past the pass's limits go back (they depend on nothing left behind)
+    PassBuilder pb;
+    pb.window = W;
+    size_t taken = 0;
+    for (; taken < inc.size(); ++taken)
+      if (!pb.add(gs[inc[taken]], maxk)) break;
+    if (taken == 0) throw Error(NCSIM_ERR_INVALID, "fusion planner made no progress");
+    Pass p = pb.finish(n);
+    stats.unitaries += uint64_t(p.unitaries);
+    for (auto& op : p.ops) stats.terms += op.terms.size();
+    out.push_back(std::move(p));
+    std::vector<size_t> back(inc.begin() + taken, inc.end());
+    std::vector<size_t> merged;
+    std::merge(rest.begin(), rest.end(), back.begin(), back.end(), std::back_inserter(merged));
+    remaining.swap(merged);
+  }
+}
+
+}  // namespace
+
+Plan make_plan(const ncsim_circuit& c, uint32_t max_fuse) {
+  if (c.n < uint32_t(TILE_BITS)) throw Error(NCSIM_ERR_UNSUPPORTED, "the fused form needs at least 12 qubits");
+  const int maxk = int(std::min<uint32_t>(std::max<uint32_t>(max_fuse, 1), GROUP_QUBITS));
+  Plan p;
+  p.n = c.n;
+  std::vector<GInfo> run;
+  auto flush = [&] {
+    if (run.empty()) return;
+    Segment s;
+    s.fused = true;
+    plan_run(run, c.n, maxk, s.passes, p);
+    p.passes += s.passes.size();
+    p.segments.push_back(std::move(s));
+    run.clear();
+  };
+  for (size_t i = 0; i < c.ops.size(); ++i) {
+    const OpIR& op = c.ops[i];
+    if (op.kind == OpKind::Gate) ++p.source_gates;
+    GInfo g = classify(op);
+    if (g.cls == GClass::Skip) continue;
+    if (g.cls == GClass::Plain) {
+      flush();
+      Segment s;
+      s.fused = false;
+      s.op = i;
+      p.segments.push_back(std::move(s));
+      continue;
+    }
+    run.push_back(std::move(g));
+  }
+  flush();
+  return p;
+}
+
+// ---------------------------------------------------------------------------
+uint16_t bf16_bits(float x) {
+  uint32_t u;
+  std::memcpy(&u, &x, 4);
+  if ((u & 0x7f800000u) == 0x7f800000u) return uint16_t(u >> 16);  // inf / nan (never used)
+  const uint32_t rounding = 0x7fffu + ((u >> 16) & 1u);             // to nearest, ties to even
+  return uint16_t((u + rounding) >> 16);
+}
+
+float bf16_value(uint16_t b) {
+  const uint32_t u = uint32_t(b) << 16;
+  float f;
+  std::memcpy(&f, &u, 4);
+  return f;
+}
+
+void build_operand_image(const std::vector<CplxD>& u, uint8_t* out) {
+  // R[n][k]: n < 32 real output rows, n >= 32 imaginary; k < 32 real inputs, k >= 32 imaginary
+  std::memset(out, 0, 16384);
+  uint16_t* hi = reinterpret_cast<uint16_t*>(out);
+  uint16_t* lo = reinterpret_cast<uint16_t*>(out + 8192);
+  for (uint32_t n = 0; n < 64; ++n)
+    for (uint32_t k = 0; k < 64; ++k) {
+      const CplxD e = u[(n & 31) * 32 + (k & 31)];
+      double r;
+      if (n < 32 && k < 32) r = e.re;
+      else if (n < 32) r = -e.im;
+      else if (k < 32) r = e.im;
+      else r = e.re;
+      const float rf = float(r);
+      const uint16_t h = bf16_bits(rf);
+      const uint16_t l = bf16_bits(float(r - double(bf16_value(h))));
+      const uint32_t off = sw128_offset(n, k >> 3) + (k & 7) * 2;
+      hi[off / 2] = h;
+      lo[off / 2] = l;
+    }
+}
+
+// a lowered gate on host amplitudes (the plain segments of the emulation)
+static void apply_lowered_host(const LoweredOp& op, std::vector<CplxD>& a, uint32_t n) {
+  const uint64_t len = uint64_t(1) << n;
+  const size_t k = op.qubits.size();
+  auto local = [&](uint64_t i) {
+    uint64_t x = 0;
+    for (size_t j = 0; j < k; ++j) x |= ((i >> op.qubits[j]) & 1) << j;
+    return x;
+  };
+  auto with_local = [&](uint64_t i, uint64_t y) {
+    for (size_t j = 0; j < k; ++j) i = (i & ~(uint64_t(1) << op.qubits[j])) | (((y >> j) & 1) << op.qubits[j]);
+    return i;
+  };
+  std::vector<CplxD> out(a.size(), CplxD{0, 0});
+  switch (op.kind) {
+    case LoweredKind::Nothing: return;
+    case LoweredKind::Pauli:
+      for (uint64_t c = 0; c < len; ++c) {
+        const int kk = int(op.phase + 2 * __builtin_popcountll(op.z & c)) & 3;
+        static const CplxD ip[4] = {{1, 0}, {0, 1}, {-1, 0}, {0, -1}};
+        out[c ^ op.x] = mul(ip[kk], a[c]);
+      }
+      break;
+    case LoweredKind::PhasePoly:
+      for (uint64_t i = 0; i < len; ++i) {
+        uint64_t f = op.poly.constant;
+        for (size_t t = 0; t + 1 < op.poly.term_start.size(); ++t) {
+          bool all = true;
+          for (uint32_t l = op.poly.term_start[t]; l < op.poly.term_start[t + 1]; ++l)
+            all &= bool(__builtin_popcountll(op.poly.parities[l] & i) & 1);
+          if (all) f += op.poly.coeffs[t];
+        }
+        f &= (uint64_t(1) << op.poly.bits) - 1;
+        Cd r = root_value(int64_t(f), op.poly.bits);
+        CplxD c = op.poly.root_table.empty() ? mul(op.poly.scalar, CplxD{r.re, r.im}) : op.poly.root_table[f];
+        out[i] = mul(c, a[i]);
+      }
+      break;
+    case LoweredKind::Monomial:
+      for (uint64_t i = 0; i < len; ++i) {
+        const uint64_t x = local(i);
+        out[with_local(i, op.image[x])] = mul(op.matrix[x], a[i]);
+      }
+      break;
+    case LoweredKind::Dense: {
+      const size_t d = size_t(1) << k;
+      for (uint64_t i = 0; i < len; ++i) {
+        const uint64_t x = local(i);
+        for (size_t y = 0; y < d; ++y) {
+          CplxD m = mul(op.matrix[y * d + x], a[i]);
+          CplxD& o = out[with_local(i, y)];
+          o.re += m.re;
+          o.im += m.im;
+        }
+      }
+      break;
+    }
+  }
+  a.swap(out);
+}
+
+void emulate(const Plan& p, const ncsim_circuit& c, std::vector<CplxD>& a) {
+  const uint64_t len = uint64_t(1) << p.n;
+  for (const Segment& s : p.segments) {
+    if (!s.fused) {
+      const OpIR& op = c.ops[s.op];
+      if (op.kind != OpKind::Gate) throw Error(NCSIM_ERR_UNSUPPORTED, "emulation covers gates only");
+      apply_lowered_host(op.lowered, a, p.n);
+      continue;
+    }
+    for (const Pass& ps : s.passes) {
+      uint64_t wmask = 0;
+      for (uint32_t b : ps.window) wmask |= uint64_t(1) << b;
+      const uint64_t ntiles = len >> TILE_BITS;
+      std::vector<CplxD> t(size_t(1) << TILE_BITS);
+      for (uint64_t tile = 0; tile < ntiles; ++tile) {
+        // base: tile bits deposited outside the window
+        uint64_t base = 0;
+        for (uint32_t b = 0, j = 0; b < p.n; ++b)
+          if (!((wmask >> b) & 1)) base |= ((tile >> j++) & 1) << b;
+        auto gidx = [&](uint32_t e) {
+          uint64_t g = base;
+          for (int j = 0; j < TILE_BITS; ++j) g |= uint64_t((e >> j) & 1) << ps.window[j];
+          return g;
+        };
+        for (uint32_t e = 0; e < t.size(); ++e) t[e] = a[gidx(e)];
+        for (const FusedOp& op : ps.ops) {
+          if (op.kind == 1) {
+            for (uint32_t e = 0; e < t.size(); ++e) {
+              const uint64_t gi = gidx(e);
+              for (const Term& tm : op.terms)
+                if ((gi & tm.mask) == tm.mask) t[e] = mul(tm.c, t[e]);
+            }
+            continue;
+          }
+          int pos[GROUP_QUBITS];
+          uint32_t gt = 0;
+          for (int j = 0; j < GROUP_QUBITS; ++j) {
+            pos[j] = int(std::find(ps.window.begin(), ps.window.end(), op.qubits[j]) - ps.window.begin());
+            gt |= 1u << pos[j];
+          }
+          std::vector<CplxD> in(32), outv(32);
+          for (uint32_t e = 0; e < t.size(); ++e) {
+            if (e & gt) continue;  // one column: the gate bits zero
+            for (uint32_t r = 0; r < 32; ++r) {
+              uint32_t ee = e;
+              for (int j = 0; j < GROUP_QUBITS; ++j) ee |= ((r >> j) & 1) << pos[j];
+              in[r] = t[ee];
+            }
+            for (uint32_t r = 0; r < 32; ++r) {
+              CplxD acc{0, 0};
+              for (uint32_t k = 0; k < 32; ++k) {
+                CplxD m = mul(op.u[r * 32 + k], in[k]);
+                acc.re += m.re;
+                acc.im += m.im;
+              }
+              outv[r] = acc;
+            }
+            for (uint32_t r = 0; r < 32; ++r) {
+              uint32_t ee = e;
+              for (int j = 0; j < GROUP_QUBITS; ++j) ee |= ((r >> j) & 1) << pos[j];
+              t[ee] = outv[r];
+            }
+          }
+        }
+        for (uint32_t e = 0; e < t.size(); ++e) a[gidx(e)] = t[e];
+      }
+    }
+  }
+}
+
+}  // namespace fused
+}  // namespace ncsim

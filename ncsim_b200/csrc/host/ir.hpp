@@ -5,6 +5,7 @@
 #pragma once
 
 #include <cstdint>
+#include <memory>
 #include <string>
 #include <vector>
 
@@ -111,6 +112,10 @@ struct OpIR {
 struct ncsim_circuit {
   uint32_t n = 0;
   std::vector<ncsim::OpIR> ops;
+  // the fused form's device plan, built on first use (freed with the circuit)
+  mutable std::shared_ptr<void> fused_plan;
+  mutable uint32_t fused_plan_fuse = 0;
+  mutable int fused_plan_device = -1;
   uint64_t num_gates() const;
   uint64_t num_measurements() const;
   std::string text() const;
