@@ -299,8 +299,8 @@ def main():
     fused_ok = args.path in ("auto", "fused")
     if fused_ok:
         try:
-            probe = nb.GpuStateVector(8, nb.C64)
-            probe.run_fused(nb.Circuit.random_layers(8, 1, 1), nb.StdRng(0))
+            probe = nb.GpuStateVector(12, nb.C64)
+            probe.run_fused(nb.Circuit.random_layers(12, 1, 1), nb.StdRng(0))
             del probe
         except nb.SimError:
             if args.path == "fused":
