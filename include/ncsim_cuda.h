@@ -276,13 +276,15 @@ typedef struct ncsim_fused_stats {
   uint64_t fused_unitaries;  /* unitaries after fusion */
   uint64_t passes;           /* HBM read+write passes over the state */
   uint64_t remap_passes;     /* of which qubit-permutation passes */
-  uint64_t gemm_launches;    /* tensor-core kernel launches */
+  uint64_t gemm_launches;    /* tensor-core pass kernel launches */
+  uint64_t diagonal_terms;   /* elementwise phase terms left after folding diagonals into unitaries */
 } ncsim_fused_stats;
 ncsim_status ncsim_sv_run_fused(ncsim_state* s, const ncsim_circuit* c, ncsim_rng* rng, uint32_t max_fuse,
                                 uint8_t* rec, size_t cap, size_t* len, ncsim_fused_stats* stats);
 /* Host-only check of the fusion planner: applies the fused form's plan of a
  * gates-only circuit (n <= 22) to complex128 host amplitudes in FP64, in the
- * pass, tile and op order the device uses. */
+ * pass, tile and op order the device uses.  With amps NULL it only plans
+ * (any n) and fills the statistics. */
 ncsim_status ncsim_fused_emulate(const ncsim_circuit* c, uint32_t max_fuse, double* amps, uint64_t len,
                                  ncsim_fused_stats* stats);
 

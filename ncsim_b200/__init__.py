@@ -347,6 +347,7 @@ class FusedStats(C.Structure):
         ("passes", _u64),
         ("remap_passes", _u64),
         ("gemm_launches", _u64),
+        ("diagonal_terms", _u64),
     ]
 
 

@@ -3,20 +3,24 @@
 // A persistent CTA per SM streams tiles of 2^12 complex64 amplitudes (32 KB)
 // through shared memory with the bulk-copy engine (cp.async.bulk, runs of
 // >= 128 contiguous bytes, double-buffered: tile i+1 loads and tile i-1
-// stores while tile i computes).  Four warps run the pass's program on each
+// stores while tile i computes).  Eight warps run the pass's program on each
 // tile:
 //   unitary op: the tile as 32 rows (the unitary's 5 qubits) x 128 columns;
-//     each thread owns a column, splits its 32 amplitudes into bf16 hi/lo and
-//     writes them K-major, 128-byte swizzled (A = X^T, 128 x 64 per half);
-//     one thread issues 12 tcgen05.mma (M=128, N=64, K=16, bf16 in, f32
-//     accumulate in TMEM): D = Xhi.Rhi + Xlo.Rhi + Xhi.Rlo with R the real
-//     form [[Ur, -Ui], [Ui, Ur]] of the fused unitary (bf16 hi/lo images made
-//     on the host); each thread reads its D row back (tcgen05.ld) and writes
-//     the 32 new amplitudes into the tile;
-//   diagonal op: every amplitude times the product of the active terms.
-// The fifth warp issues the bulk copies.  Every wait on an mbarrier is
-// bounded in time: on timeout the CTA records an error code, stops, waits for
-// its own copies and frees its TMEM.
+//     two threads share a column (16 rows each), split its amplitudes into
+//     bf16 hi/lo and write them K-major, 128-byte swizzled (A = X^T,
+//     128 x 64 per half); one thread issues 12 tcgen05.mma (M=128, N=64,
+//     K=16, bf16 in, f32 accumulate in TMEM):
+//       D = Xhi.Rhi + Xlo.Rhi + Xhi.Rlo
+//     with R the real form [[Ur, -Ui], [Ui, Ur]] of the fused unitary (bf16
+//     hi/lo images made on the host); each thread reads its half of its D row
+//     back (tcgen05.ld) and writes the 16 new amplitudes into the tile;
+//   diagonal op: the tile index splits into two 6-bit halves; per tile, the
+//     active terms are folded into a 64-entry phase table per half and a
+//     parity table for the cross-half sign terms (CZ-like), so an amplitude
+//     costs two table reads and a parity, whatever the number of terms.
+// A ninth warp issues the bulk copies.  Every wait on an mbarrier is bounded
+// in time: on timeout the CTA records an error code, stops, waits for its own
+// copies and frees its TMEM.
 #include <cuda_bf16.h>
 
 #include "engine.cuh"
@@ -30,7 +34,8 @@ namespace fused {
 
 namespace {
 
-constexpr int THREADS = 160;  // warps 0-3: tensor-core program; warp 4: bulk copies
+constexpr int COMPUTE_THREADS = 256;           // warps 0-7: tensor-core program
+constexpr int THREADS = COMPUTE_THREADS + 32;  // warp 8: bulk copies
 constexpr int TILE = 1 << TILE_BITS;
 constexpr uint32_t TILE_BYTES = uint32_t(TILE) * 8u;
 constexpr int OPERAND_BYTES = 16384;
@@ -40,14 +45,19 @@ constexpr int SM_AHI = SM_ROPS + MAX_UNITARIES * OPERAND_BYTES;
 constexpr int SM_ALO = SM_AHI + A_BYTES;
 constexpr int SM_TILE0 = SM_ALO + A_BYTES;
 constexpr int SM_TOTAL = SM_TILE0 + 2 * int(TILE_BYTES);
-constexpr int SM_DYNAMIC = SM_TOTAL + 1024;  // slack to align the base to 1024 bytes
+constexpr int SM_DYNAMIC = SM_TOTAL + 1008;  // the dynamic base is 16-byte aligned: slack to reach 1024
 constexpr uint32_t TMEM_COLS = 64;
 constexpr long long WAIT_CYCLES = 4000000000ll;  // about 2 s at 1.9 GHz
+constexpr int HALF = TILE_BITS / 2;              // 6-bit halves of the tile index
+
+enum TermClass : uint8_t { T_LOW = 0, T_HIGH = 1, T_CROSS_SIGN = 2, T_GENERIC = 3 };
 
 struct OpDesc {
   uint8_t kind;  // 0 unitary, 1 terms
   uint8_t u;     // unitary index (operand slot)
-  uint16_t t0, t1;
+  // terms [t0, t1) sorted by class: low half [t0,tl), high half [tl,th),
+  // cross-half signs [th,tc), the rest [tc,t1)
+  uint16_t t0, tl, th, tc, t1;
 };
 
 struct TermDesc {
@@ -113,7 +123,7 @@ __device__ __forceinline__ void bulk_commit() { asm volatile("cp.async.bulk.comm
 __device__ __forceinline__ void bulk_wait_read_all() { asm volatile("cp.async.bulk.wait_group.read 0;" ::: "memory"); }
 __device__ __forceinline__ void bulk_wait_all() { asm volatile("cp.async.bulk.wait_group 0;" ::: "memory"); }
 __device__ __forceinline__ void fence_async_smem() { asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); }
-__device__ __forceinline__ void bar_compute() { asm volatile("bar.sync 1, 128;" ::: "memory"); }
+__device__ __forceinline__ void bar_compute() { asm volatile("bar.sync 1, 256;" ::: "memory"); }
 
 __device__ __forceinline__ void tc_fence_before() { asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory"); }
 __device__ __forceinline__ void tc_fence_after() { asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory"); }
@@ -139,21 +149,23 @@ __device__ __forceinline__ void mma_commit(uint32_t bar) {
   asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(bar) : "memory");
 }
 
-#define NCSIM_TMEM_LD32(taddr, r)                                                                                    \
-  asm volatile(                                                                                                      \
-      "tcgen05.ld.sync.aligned.32x32b.x32.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15,%16,%17,%18,%19," \
-      "%20,%21,%22,%23,%24,%25,%26,%27,%28,%29,%30,%31}, [%32];"                                                     \
-      : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]), "=r"(r[8]),  \
-        "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15]), "=r"(r[16]),       \
-        "=r"(r[17]), "=r"(r[18]), "=r"(r[19]), "=r"(r[20]), "=r"(r[21]), "=r"(r[22]), "=r"(r[23]), "=r"(r[24]),      \
-        "=r"(r[25]), "=r"(r[26]), "=r"(r[27]), "=r"(r[28]), "=r"(r[29]), "=r"(r[30]), "=r"(r[31])                    \
-      : "r"(taddr))
+#define NCSIM_TMEM_LD16(taddr, r)                                                                                     \
+  asm volatile("tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, [%16];" \
+               : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),        \
+                 "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15])    \
+               : "r"(taddr))
 
 __device__ __forceinline__ uint32_t pack_bf16(float a, float b) {
   __nv_bfloat162 v = __floats2bfloat162_rn(a, b);
   return *reinterpret_cast<uint32_t*>(&v);
 }
-__device__ __forceinline__ float bf16_round(float a) { return __bfloat162float(__float2bfloat16_rn(a)); }
+// the two bf16 of a packed pair as floats (low half = first element)
+__device__ __forceinline__ float lo_half(uint32_t p) { return __uint_as_float(p << 16); }
+__device__ __forceinline__ float hi_half(uint32_t p) { return __uint_as_float(p & 0xffff0000u); }
+
+__device__ __forceinline__ float2 cmulf(float2 a, float2 b) {
+  return make_float2(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x);
+}
 
 // index of tile-local element e of a tile whose base index is `base`
 __device__ __forceinline__ uint64_t global_index(uint64_t base, uint32_t e, const PassParams& P) {
@@ -177,8 +189,9 @@ __global__ void __launch_bounds__(THREADS, 1) k_fused_pass(const __grid_constant
   __shared__ __align__(8) uint64_t bars[5];  // full[2], done[2], mma
   __shared__ uint32_t tmem_base_sh;
   __shared__ volatile int abort_sh;
-  __shared__ uint16_t rowoff[MAX_UNITARIES][32];
   __shared__ uint8_t nongate[MAX_UNITARIES][TILE_BITS - GROUP_QUBITS];
+  __shared__ float2 tab_lo[1 << HALF], tab_hi[1 << HALF];
+  __shared__ uint8_t tab_cross[1 << HALF];
 
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
   const uint32_t bar_full0 = smem_u32(&bars[0]), bar_done0 = smem_u32(&bars[2]), bar_mma = smem_u32(&bars[4]);
@@ -192,8 +205,8 @@ __global__ void __launch_bounds__(THREADS, 1) k_fused_pass(const __grid_constant
   if (tid == 0) {
     mbar_init(bar_full(0), 1);
     mbar_init(bar_full(1), 1);
-    mbar_init(bar_done(0), 128);
-    mbar_init(bar_done(1), 128);
+    mbar_init(bar_done(0), COMPUTE_THREADS);
+    mbar_init(bar_done(1), COMPUTE_THREADS);
     mbar_init(bar_mma, 1);
     abort_sh = 0;
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
@@ -203,17 +216,11 @@ __global__ void __launch_bounds__(THREADS, 1) k_fused_pass(const __grid_constant
                  "r"(TMEM_COLS));
     asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
   }
-  // operand images and per-unitary index tables
+  // operand images and the per-unitary column bits
   {
     uint4* dst = reinterpret_cast<uint4*>(smem + SM_ROPS);
     const int n16 = P.nu * (OPERAND_BYTES / 16);
     for (int i = tid; i < n16; i += THREADS) dst[i] = P.rops[i];
-    for (int i = tid; i < P.nu * 32; i += THREADS) {
-      const int u = i >> 5, r = i & 31;
-      uint32_t o = 0;
-      for (int j = 0; j < GROUP_QUBITS; ++j) o |= uint32_t((r >> j) & 1) << P.pos[u][j];
-      rowoff[u][r] = uint16_t(o);
-    }
     for (int u = tid; u < P.nu; u += THREADS) {
       uint32_t gm = 0;
       for (int j = 0; j < GROUP_QUBITS; ++j) gm |= 1u << P.pos[u][j];
@@ -230,9 +237,9 @@ __global__ void __launch_bounds__(THREADS, 1) k_fused_pass(const __grid_constant
   const uint64_t my_tiles = P.ntiles > blockIdx.x ? (P.ntiles - 1 - blockIdx.x) / gridDim.x + 1 : 0;
   float2* tiles = reinterpret_cast<float2*>(smem + SM_TILE0);
 
-  if (warp == 4) {
+  if (warp == COMPUTE_THREADS / 32) {
     // ---------------- bulk-copy producer ----------------
-    const uint32_t run_elems = 1u << P.wl, run_bytes = run_elems * 8u, nruns = uint32_t(TILE) >> P.wl;
+    const uint32_t run_bytes = (1u << P.wl) * 8u, nruns = uint32_t(TILE) >> P.wl;
     auto copy_tile = [&](uint64_t it, int b, bool load) {
       const uint64_t t = uint64_t(blockIdx.x) + it * gridDim.x;
       const uint64_t base = tile_base(t, P);
@@ -285,10 +292,14 @@ __global__ void __launch_bounds__(THREADS, 1) k_fused_pass(const __grid_constant
     }
     bulk_wait_all();
   } else {
-    // ---------------- tensor-core program ----------------
+    // ---------------- tensor-core program (256 threads) ----------------
     const uint32_t idesc = (1u << 4) | (1u << 7) | (1u << 10) | ((64u >> 3) << 17) | ((128u >> 4) << 24);
     const uint32_t a_hi = smem_u32(smem + SM_AHI), a_lo = smem_u32(smem + SM_ALO);
-    const uint32_t taddr = tmem + (uint32_t(warp * 32) << 16);
+    const int col = tid & 127, half = tid >> 7;  // A row / TMEM lane, and which 16 of the 32 rows
+    const uint32_t taddr = tmem + (uint32_t((warp & 3) * 32) << 16) + uint32_t(16 * half);
+    const uint32_t row7 = uint32_t(col) & 7u;
+    uint8_t* ahi_row = smem + SM_AHI + (col >> 3) * 1024 + row7 * 128;
+    uint8_t* alo_row = smem + SM_ALO + (col >> 3) * 1024 + row7 * 128;
     uint32_t mma_phase = 0;
     for (uint64_t it = 0; it < my_tiles; ++it) {
       const int b = int(it & 1);
@@ -301,24 +312,47 @@ __global__ void __launch_bounds__(THREADS, 1) k_fused_pass(const __grid_constant
       for (int oi = 0; oi < P.nops; ++oi) {
         const OpDesc op = P.ops[oi];
         if (op.kind == 1) {
-          float2 v[32];
-#pragma unroll
-          for (int i = 0; i < 32; ++i) v[i] = T[tid + 128 * i];
-          for (int k = op.t0; k < op.t1; ++k) {
-            const TermDesc tm = P.terms[k];
-            if ((base & tm.cmask) != tm.cmask) continue;
-#pragma unroll
-            for (int i = 0; i < 32; ++i) {
-              const uint32_t e = uint32_t(tid + 128 * i);
-              if ((e & tm.tmask) == tm.tmask) {
-                const float x = v[i].x, y = v[i].y;
-                v[i].x = tm.cr * x - tm.ci * y;
-                v[i].y = tm.cr * y + tm.ci * x;
-              }
+          // ---- diagonal terms: per-tile tables, then one sweep of the tile ----
+          if (tid < 64) {
+            float2 c = make_float2(1.f, 0.f);
+            for (int k = op.t0; k < op.tl; ++k) {
+              const TermDesc tm = P.terms[k];
+              if ((base & tm.cmask) == tm.cmask && (uint32_t(tid) & tm.tmask) == tm.tmask)
+                c = cmulf(c, make_float2(tm.cr, tm.ci));
             }
+            tab_lo[tid] = c;
+          } else if (tid < 128) {
+            const uint32_t x = uint32_t(tid - 64);
+            float2 c = make_float2(1.f, 0.f);
+            for (int k = op.tl; k < op.th; ++k) {
+              const TermDesc tm = P.terms[k];
+              const uint32_t hm = tm.tmask >> HALF;
+              if ((base & tm.cmask) == tm.cmask && (x & hm) == hm) c = cmulf(c, make_float2(tm.cr, tm.ci));
+            }
+            tab_hi[x] = c;
+          } else if (tid < 192) {
+            const uint32_t x = uint32_t(tid - 128);
+            uint32_t v = 0;
+            for (int k = op.th; k < op.tc; ++k) {
+              const TermDesc tm = P.terms[k];
+              if ((base & tm.cmask) != tm.cmask) continue;
+              if (x & (tm.tmask >> HALF)) v ^= tm.tmask & ((1u << HALF) - 1);
+            }
+            tab_cross[x] = uint8_t(v);
           }
-#pragma unroll
-          for (int i = 0; i < 32; ++i) T[tid + 128 * i] = v[i];
+          bar_compute();
+#pragma unroll 4
+          for (int i = 0; i < TILE / COMPUTE_THREADS; ++i) {
+            const uint32_t e = uint32_t(tid + COMPUTE_THREADS * i);
+            const uint32_t lo = e & ((1u << HALF) - 1), hi = e >> HALF;
+            float2 c = cmulf(tab_lo[lo], tab_hi[hi]);
+            if (__popc(lo & tab_cross[hi]) & 1) c = make_float2(-c.x, -c.y);
+            for (int k = op.tc; k < op.t1; ++k) {
+              const TermDesc tm = P.terms[k];
+              if ((base & tm.cmask) == tm.cmask && (e & tm.tmask) == tm.tmask) c = cmulf(c, make_float2(tm.cr, tm.ci));
+            }
+            T[e] = cmulf(c, T[e]);
+          }
           bar_compute();
           continue;
         }
@@ -326,30 +360,33 @@ __global__ void __launch_bounds__(THREADS, 1) k_fused_pass(const __grid_constant
         const int u = op.u;
         uint32_t cb = 0;
 #pragma unroll
-        for (int j = 0; j < TILE_BITS - GROUP_QUBITS; ++j) cb |= uint32_t((tid >> j) & 1) << nongate[u][j];
-        float2 x[32];
+        for (int j = 0; j < TILE_BITS - GROUP_QUBITS; ++j) cb |= uint32_t((col >> j) & 1) << nongate[u][j];
+        const uint32_t p0 = 1u << P.pos[u][0], p1 = 1u << P.pos[u][1], p2 = 1u << P.pos[u][2],
+                       p3 = 1u << P.pos[u][3];
+        const uint32_t rb = cb | (half ? (1u << P.pos[u][4]) : 0u);
+        uint32_t ro[16];  // tile offsets of this thread's rows 16*half + i
 #pragma unroll
-        for (int r = 0; r < 32; ++r) x[r] = T[cb | rowoff[u][r]];
-        const uint32_t row7 = uint32_t(tid) & 7u;
-        uint8_t* ahi = smem + SM_AHI + (tid >> 3) * 1024 + row7 * 128;
-        uint8_t* alo = smem + SM_ALO + (tid >> 3) * 1024 + row7 * 128;
+        for (int i = 0; i < 16; ++i)
+          ro[i] = rb | ((i & 1) ? p0 : 0u) | ((i & 2) ? p1 : 0u) | ((i & 4) ? p2 : 0u) | ((i & 8) ? p3 : 0u);
 #pragma unroll
-        for (int j = 0; j < 4; ++j) {
+        for (int s = 0; s < 2; ++s) {
+          float2 x[8];
+#pragma unroll
+          for (int i = 0; i < 8; ++i) x[i] = T[ro[8 * s + i]];
           uint32_t hr[4], lr[4], hm[4], lm[4];
 #pragma unroll
           for (int i = 0; i < 4; ++i) {
-            const float2 p0 = x[8 * j + 2 * i], p1 = x[8 * j + 2 * i + 1];
-            const float h0 = bf16_round(p0.x), h1 = bf16_round(p1.x);
-            const float g0 = bf16_round(p0.y), g1 = bf16_round(p1.y);
-            hr[i] = pack_bf16(h0, h1);
-            lr[i] = pack_bf16(p0.x - h0, p1.x - h1);
-            hm[i] = pack_bf16(g0, g1);
-            lm[i] = pack_bf16(p0.y - g0, p1.y - g1);
+            const float2 a = x[2 * i], c = x[2 * i + 1];
+            hr[i] = pack_bf16(a.x, c.x);
+            hm[i] = pack_bf16(a.y, c.y);
+            lr[i] = pack_bf16(a.x - lo_half(hr[i]), c.x - hi_half(hr[i]));
+            lm[i] = pack_bf16(a.y - lo_half(hm[i]), c.y - hi_half(hm[i]));
           }
-          *reinterpret_cast<uint4*>(ahi + ((uint32_t(j) ^ row7) << 4)) = make_uint4(hr[0], hr[1], hr[2], hr[3]);
-          *reinterpret_cast<uint4*>(alo + ((uint32_t(j) ^ row7) << 4)) = make_uint4(lr[0], lr[1], lr[2], lr[3]);
-          *reinterpret_cast<uint4*>(ahi + ((uint32_t(j + 4) ^ row7) << 4)) = make_uint4(hm[0], hm[1], hm[2], hm[3]);
-          *reinterpret_cast<uint4*>(alo + ((uint32_t(j + 4) ^ row7) << 4)) = make_uint4(lm[0], lm[1], lm[2], lm[3]);
+          const uint32_t cre = uint32_t(2 * half + s), cim = cre + 4u;  // 16-byte chunks of rows 16h+8s..+7
+          *reinterpret_cast<uint4*>(ahi_row + ((cre ^ row7) << 4)) = make_uint4(hr[0], hr[1], hr[2], hr[3]);
+          *reinterpret_cast<uint4*>(alo_row + ((cre ^ row7) << 4)) = make_uint4(lr[0], lr[1], lr[2], lr[3]);
+          *reinterpret_cast<uint4*>(ahi_row + ((cim ^ row7) << 4)) = make_uint4(hm[0], hm[1], hm[2], hm[3]);
+          *reinterpret_cast<uint4*>(alo_row + ((cim ^ row7) << 4)) = make_uint4(lm[0], lm[1], lm[2], lm[3]);
         }
         fence_async_smem();
         bar_compute();
@@ -369,12 +406,12 @@ __global__ void __launch_bounds__(THREADS, 1) k_fused_pass(const __grid_constant
         if (!mbar_wait(bar_mma, mma_phase)) fail(2);
         mma_phase ^= 1u;
         tc_fence_after();
-        uint32_t re[32], im[32];
-        NCSIM_TMEM_LD32(taddr, re);
-        NCSIM_TMEM_LD32(taddr + 32u, im);
+        uint32_t re[16], im[16];
+        NCSIM_TMEM_LD16(taddr, re);
+        NCSIM_TMEM_LD16(taddr + 32u, im);
         asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
 #pragma unroll
-        for (int r = 0; r < 32; ++r) T[cb | rowoff[u][r]] = make_float2(__uint_as_float(re[r]), __uint_as_float(im[r]));
+        for (int i = 0; i < 16; ++i) T[ro[i]] = make_float2(__uint_as_float(re[i]), __uint_as_float(im[i]));
         tc_fence_before();
         bar_compute();
         if (abort_sh) break;
@@ -403,6 +440,15 @@ struct DevicePlan {
     if (rops) cudaFree(rops);
   }
 };
+
+// which device table a term goes to (tile-local mask tm over the two 6-bit halves)
+TermClass term_class(uint32_t tm, const CplxD& c) {
+  const uint32_t lo = tm & ((1u << HALF) - 1), hi = tm >> HALF;
+  if (hi == 0) return T_LOW;
+  if (lo == 0) return T_HIGH;
+  if (__builtin_popcount(lo) == 1 && __builtin_popcount(hi) == 1 && c.re == -1.0 && c.im == 0.0) return T_CROSS_SIGN;
+  return T_GENERIC;
+}
 
 std::unique_ptr<DevicePlan> build_device_plan(const ncsim_circuit& c, uint32_t max_fuse) {
   auto dp = std::make_unique<DevicePlan>();
@@ -439,9 +485,9 @@ std::unique_ptr<DevicePlan> build_device_plan(const ncsim_circuit& c, uint32_t m
           ++nu;
         } else {
           d.kind = 1;
-          d.t0 = uint16_t(nt);
+          if (nt + int(op.terms.size()) > MAX_TERMS) throw Error(NCSIM_ERR_INVALID, "fused pass has too many terms");
+          std::vector<std::pair<int, TermDesc>> ts;
           for (const Term& t : op.terms) {
-            if (nt >= MAX_TERMS) throw Error(NCSIM_ERR_INVALID, "fused pass has too many terms");
             TermDesc td{};
             uint32_t tm = 0;
             for (int j = 0; j < TILE_BITS; ++j)
@@ -450,9 +496,22 @@ std::unique_ptr<DevicePlan> build_device_plan(const ncsim_circuit& c, uint32_t m
             td.cmask = t.mask & ~wmask;
             td.cr = float(t.c.re);
             td.ci = float(t.c.im);
-            P.terms[nt++] = td;
+            ts.push_back({int(term_class(tm, t.c)), td});
           }
-          d.t1 = uint16_t(nt);
+          std::stable_sort(ts.begin(), ts.end(), [](const auto& a, const auto& b) { return a.first < b.first; });
+          uint16_t bound[5];  // start of each class, then the end
+          bound[0] = uint16_t(nt);
+          int cls = 0;
+          for (const auto& e : ts) {
+            while (cls < e.first) bound[++cls] = uint16_t(nt);
+            P.terms[nt++] = e.second;
+          }
+          while (cls < 4) bound[++cls] = uint16_t(nt);
+          d.t0 = bound[0];
+          d.tl = bound[1];
+          d.th = bound[2];
+          d.tc = bound[3];
+          d.t1 = bound[4];
         }
         if (no >= MAX_OPS) throw Error(NCSIM_ERR_INVALID, "fused pass has too many ops");
         P.ops[no++] = d;
@@ -530,7 +589,7 @@ extern "C" ncsim_status ncsim_sv_run_fused(ncsim_state* s, const ncsim_circuit* 
         fused::PassParams P = dp->params[pi];
         P.amp = reinterpret_cast<float2*>(s->amp);
         P.err = d_err;
-        gemm += uint64_t(P.nu);
+        ++gemm;  // one pass kernel launch
         ProfScope ps(s, K_FUSED_GEMM, 2.0 * double(s->bytes()));
         fused::k_fused_pass<<<grid, fused::THREADS, fused::SM_DYNAMIC, s->stream>>>(P);
         NCSIM_LAUNCHED("fused pass");
@@ -548,6 +607,7 @@ extern "C" ncsim_status ncsim_sv_run_fused(ncsim_state* s, const ncsim_circuit* 
       stats->passes = dp->plan.passes;
       stats->remap_passes = 0;
       stats->gemm_launches = gemm;
+      stats->diagonal_terms = dp->plan.terms;
     }
   });
 }
@@ -555,20 +615,23 @@ extern "C" ncsim_status ncsim_sv_run_fused(ncsim_state* s, const ncsim_circuit* 
 extern "C" ncsim_status ncsim_fused_emulate(const ncsim_circuit* c, uint32_t max_fuse, double* amps, uint64_t len,
                                             ncsim_fused_stats* stats) {
   return guarded([&] {
-    if (!c || !amps) throw Error(NCSIM_ERR_INVALID, "null argument");
-    if (c->n > 22) throw Error(NCSIM_ERR_UNSUPPORTED, "emulation is for registers of at most 22 qubits");
-    if (len != (uint64_t(1) << c->n)) throw Error(NCSIM_ERR_INVALID, "amplitude buffer length differs from 2^n");
+    if (!c) throw Error(NCSIM_ERR_INVALID, "null circuit");
     fused::Plan p = fused::make_plan(*c, max_fuse ? max_fuse : 5);
-    std::vector<CplxD> a(len);
-    for (uint64_t i = 0; i < len; ++i) a[i] = {amps[2 * i], amps[2 * i + 1]};
-    fused::emulate(p, *c, a);
-    for (uint64_t i = 0; i < len; ++i) amps[2 * i] = a[i].re, amps[2 * i + 1] = a[i].im;
+    if (amps) {  // without amplitudes: the plan's statistics only
+      if (c->n > 22) throw Error(NCSIM_ERR_UNSUPPORTED, "emulation is for registers of at most 22 qubits");
+      if (len != (uint64_t(1) << c->n)) throw Error(NCSIM_ERR_INVALID, "amplitude buffer length differs from 2^n");
+      std::vector<CplxD> a(len);
+      for (uint64_t i = 0; i < len; ++i) a[i] = {amps[2 * i], amps[2 * i + 1]};
+      fused::emulate(p, *c, a);
+      for (uint64_t i = 0; i < len; ++i) amps[2 * i] = a[i].re, amps[2 * i + 1] = a[i].im;
+    }
     if (stats) {
       stats->source_gates = p.source_gates;
       stats->fused_unitaries = p.unitaries;
       stats->passes = p.passes;
       stats->remap_passes = 0;
       stats->gemm_launches = p.passes;
+      stats->diagonal_terms = p.terms;
     }
   });
 }

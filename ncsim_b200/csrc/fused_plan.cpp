@@ -181,19 +181,44 @@ std::vector<Term> merge_terms(const std::vector<Term>& in) {
   return out;
 }
 
+// d (on gate qubits gq) folded into an emitted unitary op: U <- D U
+void fold_diag_into(FusedOp& op, const GInfo& d) {
+  Group tmp;
+  tmp.q = op.qubits;
+  tmp.u = op.u;
+  for (uint32_t q : op.qubits) tmp.mask |= uint64_t(1) << q;
+  tmp.apply_diag(d.q, d.d);
+  op.u.swap(tmp.u);
+}
+
+uint64_t qubit_mask(const std::vector<uint32_t>& qs) {
+  uint64_t m = 0;
+  for (uint32_t q : qs) m |= uint64_t(1) << q;
+  return m;
+}
+
+// Builds one pass's program.  Diagonal gates are folded into a unitary on
+// their qubits whenever the order allows: into the most recent unitary that
+// touches them (everything applied to those qubits after it is diagonal, and
+// diagonals commute), or into the unitary that a later gate on the same
+// qubits opens; only the rest become elementwise terms.  Global phases are
+// folded into any unitary of the pass.
 struct PassBuilder {
   uint64_t window = 0;
   Pass pass;
   Group g;
-  std::vector<Term> pending;
+  std::vector<GInfo> pending;  // diagonal gates waiting, in order
   uint64_t pending_mask = 0;
   int emitted_unitaries = 0;
   size_t term_count = 0;
+  CplxD global{1.0, 0.0};
 
   void emit_group() {
     if (!g.open) return;
-    // pad to exactly 5 window qubits (U (x) I)
-    for (int b = 0; b < 64 && g.q.size() < size_t(GROUP_QUBITS); ++b)
+    // pad to exactly 5 window qubits (U (x) I) with the highest free window
+    // qubits: the lowest tile bits then stay column bits, so the 32 columns a
+    // warp reads spread over all shared-memory banks
+    for (int b = 63; b >= 0 && g.q.size() < size_t(GROUP_QUBITS); --b)
       if (((window >> b) & 1) && g.local_of(uint32_t(b)) < 0) g.add_qubit(uint32_t(b));
     FusedOp op;
     op.kind = 0;
@@ -203,28 +228,55 @@ struct PassBuilder {
     ++emitted_unitaries;
     g.open = false;
   }
-  void emit_pending() {
-    if (pending.empty()) return;
+  void emit_terms(const std::vector<GInfo>& ds) {
+    std::vector<Term> t;
+    for (const GInfo& d : ds) diag_terms(d, t);
+    std::vector<Term> merged = merge_terms(t);
     FusedOp op;
     op.kind = 1;
-    op.terms = merge_terms(pending);
+    for (const Term& tm : merged) {
+      if (tm.mask == 0) global = mul(global, tm.c);
+      else op.terms.push_back(tm);
+    }
+    term_count += op.terms.size();
     if (!op.terms.empty()) pass.ops.push_back(std::move(op));
+  }
+  void emit_pending() {
+    if (pending.empty()) return;
+    emit_terms(pending);
     pending.clear();
     pending_mask = 0;
+  }
+  // worst-case number of terms the pending gates could add
+  size_t pending_term_bound() const {
+    size_t s = 0;
+    for (const GInfo& d : pending) s += size_t(1) << d.q.size();
+    return s;
   }
   // false: the gate does not fit this pass's limits (the caller cuts here)
   bool add(const GInfo& gi, int maxk) {
     if (gi.cls == GClass::Diag) {
-      if (g.open && (gi.mask & ~g.mask) == 0) {
-        g.apply_diag(gi.q, gi.d);
-        return true;
+      // backward: the most recent unitary touching these qubits
+      if (g.open && (g.mask & gi.mask)) {
+        if ((gi.mask & ~g.mask) == 0) {
+          g.apply_diag(gi.q, gi.d);
+          return true;
+        }
+      } else {
+        for (size_t i = pass.ops.size(); i-- > 0;) {
+          if (pass.ops[i].kind != 0) continue;
+          const uint64_t m = qubit_mask(pass.ops[i].qubits);
+          if (!(m & gi.mask)) continue;
+          if ((gi.mask & ~m) == 0) {
+            fold_diag_into(pass.ops[i], gi);
+            return true;
+          }
+          break;
+        }
       }
-      std::vector<Term> t;
-      diag_terms(gi, t);
-      if (term_count + t.size() > size_t(MAX_TERMS)) return false;
+      if (term_count + pending_term_bound() + (size_t(1) << gi.q.size()) > size_t(MAX_TERMS)) return false;
       if (pass.ops.size() + 3 > size_t(MAX_OPS)) return false;
-      term_count += t.size();
-      pending.insert(pending.end(), t.begin(), t.end());
+      pending.push_back(gi);
       pending_mask |= gi.mask;
       return true;
     }
@@ -236,14 +288,39 @@ struct PassBuilder {
     if (emitted_unitaries + (g.open ? 1 : 0) + 1 > MAX_UNITARIES) return false;
     if (pass.ops.size() + 3 > size_t(MAX_OPS)) return false;
     emit_group();
-    emit_pending();
+    // forward: waiting diagonals on this gate's qubits open the new group
+    // (they come after every emitted op on their qubits and before this gate)
+    std::vector<GInfo> fold, keep;
+    for (const GInfo& d : pending) ((d.mask & ~gi.mask) == 0 ? fold : keep).push_back(d);
+    if (!keep.empty()) emit_terms(keep);
+    pending.clear();
+    pending_mask = 0;
     g.start();
+    for (uint32_t q : gi.q) g.add_qubit(q);
+    for (const GInfo& d : fold) g.apply_diag(d.q, d.d);
     g.apply_dense(gi.q, gi.m);
     return true;
   }
   Pass finish(uint32_t n) {
     emit_group();
     emit_pending();
+    // the global phase goes into a unitary when the pass has one
+    if (!exactly_one(global)) {
+      bool folded = false;
+      for (auto& op : pass.ops)
+        if (op.kind == 0) {
+          for (auto& e : op.u) e = mul(global, e);
+          folded = true;
+          break;
+        }
+      if (!folded) {
+        FusedOp op;
+        op.kind = 1;
+        op.terms.push_back({0, global});
+        pass.ops.push_back(std::move(op));
+        ++term_count;
+      }
+    }
     // window: exactly TILE_BITS qubits, ascending
     uint64_t w = window;
     for (uint32_t b = 0; b < n && __builtin_popcountll(w) < TILE_BITS; ++b) w |= uint64_t(1) << b;
