@@ -288,6 +288,65 @@ ncsim_status ncsim_sv_run_fused(ncsim_state* s, const ncsim_circuit* c, ncsim_rn
 ncsim_status ncsim_fused_emulate(const ncsim_circuit* c, uint32_t max_fuse, double* amps, uint64_t len,
                                  ncsim_fused_stats* stats);
 
+/* ---- batching form: many independent noisy trajectories ----
+ * Each trajectory is QuantumState::run (src/state/mod.rs:168-183) of a circuit
+ * on a register of 13..26 qubits that starts at |0...0>, with its own StdRng:
+ * one-qubit gates, two-qubit controlled phases (CZ, CS, CS_DAG, CPHASE), Pauli
+ * noise channels (one draw per application, src/circuit.rs:136-146) and a
+ * trailing block M 0, M 1, ..., M m-1 (a draw only when the outcome is
+ * uncertain, src/state/mod.rs:113-131).  All trajectories run in one
+ * persistent kernel (complex64 amplitudes, FP64 reductions) replayed through a
+ * CUDA graph, with a launch configuration picked by timing (autotuner).
+ * Results per trajectory: the record (bit k = outcome of M k), <Z0>/<psi|psi>
+ * just before the measurements, and <psi|psi> there. */
+typedef struct ncsim_batch ncsim_batch;
+typedef struct ncsim_batch_stats {
+  uint64_t trajectories;
+  uint64_t source_gates;   /* Op::Gate count over all circuits */
+  uint64_t noise_events;   /* sampled Pauli errors */
+  uint64_t folded_ops;     /* device ops after folding one-qubit runs */
+  uint64_t passes;         /* passes over trajectory states */
+  uint64_t tile_passes;    /* 8192-amplitude tiles streamed, over all passes */
+  uint64_t tile_stages;    /* register stages applied to tiles */
+  double state_bytes;      /* algorithmic HBM bytes of one run */
+  uint64_t program_bytes;  /* device program size */
+  uint32_t max_qubits;
+} ncsim_batch_stats;
+enum { NCSIM_BATCH_ORDER_LARGEST_FIRST = 0, NCSIM_BATCH_ORDER_GIVEN = 1 };
+typedef struct ncsim_batch_config {
+  uint32_t ctas_per_sm; /* 1, or 2 when single-buffered */
+  uint32_t buffers;     /* 2: tile prefetch, FP64 sums in shared memory; 1: no prefetch */
+  uint32_t order;       /* NCSIM_BATCH_ORDER_* */
+} ncsim_batch_config;
+/* Trajectory t: StdRng::seed_from_u64(seed0 + t), n = n_lo + gen_range(0..n_span),
+ * the random-layer circuit of `depth` layers with DEPOLARIZE2(p) after every
+ * CZ and M on every qubit (ncsim_workload_random_circuit_rng), run with the
+ * same generator. */
+ncsim_status ncsim_batch_random_layers(uint32_t count, uint64_t seed0, uint32_t n_lo, uint32_t n_span, uint32_t depth,
+                                       double p, ncsim_batch** out);
+/* Trajectory t: circuits[t] run with StdRng::seed_from_u64(seeds[t]). */
+ncsim_status ncsim_batch_from_circuits(uint32_t count, const ncsim_circuit* const* circuits, const uint64_t* seeds,
+                                       ncsim_batch** out);
+ncsim_status ncsim_batch_free(ncsim_batch* b);
+ncsim_status ncsim_batch_info(const ncsim_batch* b, ncsim_batch_stats* st);
+ncsim_status ncsim_batch_trajectory_qubits(const ncsim_batch* b, uint32_t* n);
+ncsim_status ncsim_batch_set_config(ncsim_batch* b, const ncsim_batch_config* cfg);
+/* The configuration the next run uses (tuned on the current device if unset). */
+ncsim_status ncsim_batch_get_config(ncsim_batch* b, ncsim_batch_config* cfg);
+/* Times each candidate configuration on an evenly strided sample of the
+ * batch (0 = the whole batch) and keeps the fastest; runs on first use when
+ * no configuration was set, once per (device, count, largest register). */
+ncsim_status ncsim_batch_tune(ncsim_batch* b, uint32_t sample, ncsim_batch_config* best);
+/* Runs every trajectory on the current device (one CUDA graph launch: counter
+ * reset, the kernel, result copies to pinned host memory); device_ms
+ * (optional) is the graph's time between CUDA events on its stream. */
+ncsim_status ncsim_batch_run(ncsim_batch* b, double* device_ms);
+/* Per trajectory (arrays of the batch's count; NULL skips): n, record, <Z0>/norm, norm. */
+ncsim_status ncsim_batch_results(ncsim_batch* b, uint32_t* n, uint64_t* records, double* z0, double* norm);
+/* Host-only check: trajectory t's device program run in FP64 on the host in
+ * the device's pass, tile, stage and op order (n <= 22). */
+ncsim_status ncsim_batch_emulate(const ncsim_batch* b, uint32_t t, uint64_t* record, double* z0, double* norm);
+
 #ifdef __cplusplus
 }
 #endif

@@ -119,6 +119,17 @@ _SIGNATURES = {
     "ncsim_sv_profile_enable": (_i32, [_vp, _i32]),
     "ncsim_sv_profile_read": (_i32, [_vp, _vp, _u32, _P(_u32)]),
     "ncsim_measure_stats_noalloc": (_i32, [_vp, _u32, _i32, _u64, _u64, _u32, _vp, _P(_dbl), _P(_dbl)]),
+    "ncsim_batch_random_layers": (_i32, [_u32, _u64, _u32, _u32, _u32, _dbl, _P(_vp)]),
+    "ncsim_batch_from_circuits": (_i32, [_u32, _P(_vp), _P(_u64), _P(_vp)]),
+    "ncsim_batch_free": (_i32, [_vp]),
+    "ncsim_batch_info": (_i32, [_vp, _vp]),
+    "ncsim_batch_trajectory_qubits": (_i32, [_vp, _P(_u32)]),
+    "ncsim_batch_set_config": (_i32, [_vp, _vp]),
+    "ncsim_batch_get_config": (_i32, [_vp, _vp]),
+    "ncsim_batch_tune": (_i32, [_vp, _u32, _vp]),
+    "ncsim_batch_run": (_i32, [_vp, _P(_dbl)]),
+    "ncsim_batch_results": (_i32, [_vp, _P(_u32), _P(_u64), _P(_dbl), _P(_dbl)]),
+    "ncsim_batch_emulate": (_i32, [_vp, _u32, _P(_u64), _P(_dbl), _P(_dbl)]),
 }
 
 
@@ -602,6 +613,117 @@ class GpuStateVector:
             arr[i].name.decode(): {"launches": arr[i].launches, "ms": arr[i].milliseconds, "bytes": arr[i].bytes}
             for i in range(min(cnt.value, 32))
         }
+
+
+# ---------------------------------------------------------------------------
+# batching form: many noisy trajectories in one persistent kernel
+# ---------------------------------------------------------------------------
+class BatchStats(C.Structure):
+    _fields_ = [
+        ("trajectories", _u64),
+        ("source_gates", _u64),
+        ("noise_events", _u64),
+        ("folded_ops", _u64),
+        ("passes", _u64),
+        ("tile_passes", _u64),
+        ("tile_stages", _u64),
+        ("state_bytes", _dbl),
+        ("program_bytes", _u64),
+        ("max_qubits", _u32),
+    ]
+
+
+class BatchConfig(C.Structure):
+    _fields_ = [("ctas_per_sm", _u32), ("buffers", _u32), ("order", _u32)]
+
+    def as_dict(self) -> dict:
+        return {"ctas_per_sm": self.ctas_per_sm, "buffers": self.buffers,
+                "order": "largest_first" if self.order == 0 else "given"}
+
+
+class TrajectoryBatch:
+    """Independent noisy trajectories, each ``QuantumState::run`` of its circuit
+    with its own ``StdRng`` (src/state/mod.rs:168-183), run together on the GPU.
+
+    ``results()`` gives per trajectory the register size, the record (bit k =
+    outcome of ``M k``), <Z0>/<psi|psi> just before the measurements and
+    <psi|psi> there."""
+
+    def __init__(self, handle):
+        self._h = handle
+
+    @classmethod
+    def random_layers(cls, count: int, seed0: int = 1, n_lo: int = 16, n_span: int = 7, depth: int = 30,
+                      p: float = 1e-3) -> "TrajectoryBatch":
+        """Trajectory t: StdRng(seed0 + t), n = n_lo + gen_range(0..n_span), the random
+        layer circuit with DEPOLARIZE2(p) after every CZ and M on every qubit."""
+        h = _vp()
+        _check(lib().ncsim_batch_random_layers(count, seed0, n_lo, n_span, depth, p, C.byref(h)))
+        return cls(h)
+
+    @classmethod
+    def from_circuits(cls, circuits: Sequence[Circuit], seeds: Sequence[int]) -> "TrajectoryBatch":
+        if len(circuits) != len(seeds):
+            raise ValueError("one seed per circuit")
+        hs = (_vp * len(circuits))(*[c._h for c in circuits])
+        sd = (_u64 * len(seeds))(*seeds)
+        h = _vp()
+        _check(lib().ncsim_batch_from_circuits(len(circuits), hs, sd, C.byref(h)))
+        return cls(h)
+
+    def __del__(self):
+        h = getattr(self, "_h", None)
+        if h and _lib is not None:
+            _lib.ncsim_batch_free(h)
+
+    def info(self) -> dict:
+        st = BatchStats()
+        _check(lib().ncsim_batch_info(self._h, C.byref(st)))
+        return {k: getattr(st, k) for k, _ in BatchStats._fields_}
+
+    def __len__(self) -> int:
+        return int(self.info()["trajectories"])
+
+    def qubits(self) -> np.ndarray:
+        n = np.empty(len(self), dtype=np.uint32)
+        _check(lib().ncsim_batch_trajectory_qubits(self._h, n.ctypes.data_as(_P(_u32))))
+        return n
+
+    def set_config(self, ctas_per_sm: int = 1, buffers: int = 2, order: str = "largest_first") -> None:
+        cfg = BatchConfig(ctas_per_sm, buffers, 0 if order == "largest_first" else 1)
+        _check(lib().ncsim_batch_set_config(self._h, C.byref(cfg)))
+
+    def config(self) -> dict:
+        cfg = BatchConfig()
+        _check(lib().ncsim_batch_get_config(self._h, C.byref(cfg)))
+        return cfg.as_dict()
+
+    def tune(self, sample: int = 0) -> dict:
+        cfg = BatchConfig()
+        _check(lib().ncsim_batch_tune(self._h, sample, C.byref(cfg)))
+        return cfg.as_dict()
+
+    def run(self) -> float:
+        """Runs every trajectory; returns the kernel's device milliseconds."""
+        ms = _dbl()
+        _check(lib().ncsim_batch_run(self._h, C.byref(ms)))
+        return ms.value
+
+    def results(self):
+        c = len(self)
+        n = np.empty(c, dtype=np.uint32)
+        rec = np.empty(c, dtype=np.uint64)
+        z0 = np.empty(c)
+        nn = np.empty(c)
+        _check(lib().ncsim_batch_results(self._h, n.ctypes.data_as(_P(_u32)), rec.ctypes.data_as(_P(_u64)),
+                                         _dp(z0), _dp(nn)))
+        return n, rec, z0, nn
+
+    def emulate(self, t: int):
+        """Host FP64 run of trajectory t's device program (tests): (record, z0, norm)."""
+        r, z, nn = _u64(), _dbl(), _dbl()
+        _check(lib().ncsim_batch_emulate(self._h, t, C.byref(r), C.byref(z), C.byref(nn)))
+        return r.value, z.value, nn.value
 
 
 def device_info() -> dict:

@@ -19,6 +19,8 @@ SOURCES = [
     "csrc/kernels_plain.cu",
     "csrc/fused.cu",
     "csrc/fused_plan.cpp",
+    "csrc/batch.cu",
+    "csrc/batch_plan.cpp",
     "csrc/host/ir.cpp",
     "csrc/host/runtime.cpp",
 ]
@@ -26,6 +28,7 @@ HEADERS = [
     "csrc/engine.cuh",
     "csrc/host_math.hpp",
     "csrc/fused_plan.hpp",
+    "csrc/batch_plan.hpp",
     "csrc/host/ir.hpp",
     "csrc/host/rng.hpp",
     "../include/ncsim_cuda.h",

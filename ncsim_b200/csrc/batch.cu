@@ -1,0 +1,894 @@
+// Batching form, device side: the persistent trajectory kernel, the batch
+// object (program upload, per-CTA state slots, CUDA graph replay) and its
+// autotuner.
+//
+// Kernel: a persistent grid; each CTA takes the next trajectory from a work
+// counter (largest registers first, by default) and runs all of its passes on
+// its own state slot, then its measurements, so CTAs never wait on one another
+// (no inter-CTA synchronisation at all).  A pass streams the state through
+// shared memory in tiles of 8192 complex64 amplitudes (64 KB), loaded with
+// cp.async (16-byte chunks, runs of 16 amplitudes = 128 B) and, in the
+// double-buffered variant, prefetched one tile ahead; each stage moves the
+// tile into registers (32 amplitudes per thread over five tile bits), applies
+// its 2x2 gates, CZ sign masks and diagonals in FP32, and writes it back.
+// The last pass (window = qubits 0..12) sums |a|^2 per tile index in FP64;
+// the Z marginals of M 0 .. M m-1 come from those sums and from a gather of
+// the 2^(n-13) amplitudes that match the low outcomes.
+//
+// Shared-memory layout of a tile: amplitude i at i ^ (((i >> 5) & 7) << 1),
+// which keeps every 16-byte chunk whole and makes the three stage layouts,
+// the chunk copies and the FP64 sums conflict-free.
+#include <algorithm>
+#include <atomic>
+#include <cmath>
+#include <map>
+#include <numeric>
+#include <thread>
+
+#include "batch_plan.hpp"
+#include "engine.cuh"
+
+using namespace ncsim;
+using namespace ncsim::batch;
+
+namespace {
+
+struct KParams {
+  const DevTraj* traj;
+  const DevPass* pass;
+  const DevStage* stage;
+  const DevOp* op;
+  const double* draws;
+  const uint32_t* order;
+  uint32_t count;
+  uint32_t max_n;
+  float2* slots;
+  uint64_t slot_elems;
+  double* gscratch;  // TILE doubles per CTA (single-buffered variant)
+  uint32_t* queue;
+  uint64_t* out_rec;
+  double* out_z0;
+  double* out_norm;
+  uint32_t* err;
+};
+
+__device__ __forceinline__ uint32_t spos(uint32_t i) { return i ^ (((i >> 5) & 7u) << 1); }
+
+__device__ __forceinline__ void cp_async16(void* smem, const void* gmem) {
+  const uint32_t s = uint32_t(__cvta_generic_to_shared(smem));
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(s), "l"(gmem) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+template <int N>
+__device__ __forceinline__ void cp_async_wait() {
+  asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory");
+}
+
+template <int R>
+__device__ __forceinline__ uint32_t fixed_index(uint32_t tid) {
+  if (R == 0) return tid << 5;
+  if (R == 1) return (tid & 31u) | ((tid >> 5) << 10);
+  return tid;
+}
+
+template <int R>
+__device__ __forceinline__ void load_stage(const float2* buf, uint32_t tid, float2 (&a)[32]) {
+  if (R == 0) {
+    const float4* b4 = reinterpret_cast<const float4*>(buf) + (tid << 4);
+    const uint32_t x = tid & 7u;
+#pragma unroll
+    for (uint32_t m = 0; m < 16; ++m) {
+      const float4 v = b4[m ^ x];
+      a[2 * m] = make_float2(v.x, v.y);
+      a[2 * m + 1] = make_float2(v.z, v.w);
+    }
+  } else if (R == 1) {
+    const uint32_t f = fixed_index<1>(tid);
+#pragma unroll
+    for (uint32_t j = 0; j < 32; ++j) a[j] = buf[(f ^ ((j & 7u) << 1)) + (j << 5)];
+  } else {
+    const uint32_t f = tid ^ (((tid >> 5) & 7u) << 1);
+#pragma unroll
+    for (uint32_t j = 0; j < 32; ++j) a[j] = buf[f + (j << 8)];
+  }
+}
+
+template <int R>
+__device__ __forceinline__ void store_stage(float2* buf, uint32_t tid, const float2 (&a)[32]) {
+  if (R == 0) {
+    float4* b4 = reinterpret_cast<float4*>(buf) + (tid << 4);
+    const uint32_t x = tid & 7u;
+#pragma unroll
+    for (uint32_t m = 0; m < 16; ++m) b4[m ^ x] = make_float4(a[2 * m].x, a[2 * m].y, a[2 * m + 1].x, a[2 * m + 1].y);
+  } else if (R == 1) {
+    const uint32_t f = fixed_index<1>(tid);
+#pragma unroll
+    for (uint32_t j = 0; j < 32; ++j) buf[(f ^ ((j & 7u) << 1)) + (j << 5)] = a[j];
+  } else {
+    const uint32_t f = tid ^ (((tid >> 5) & 7u) << 1);
+#pragma unroll
+    for (uint32_t j = 0; j < 32; ++j) buf[f + (j << 8)] = a[j];
+  }
+}
+
+// 32-bit mask over the thread's amplitudes j whose bit of the located qubit is 1
+__device__ __forceinline__ uint32_t loc_mask(uint32_t loc, uint32_t fixed, uint32_t tile) {
+  const uint32_t type = loc >> 5, idx = loc & 31u;
+  if (type == LOC_REG) {
+    switch (idx) {
+      case 0: return 0xAAAAAAAAu;
+      case 1: return 0xCCCCCCCCu;
+      case 2: return 0xF0F0F0F0u;
+      case 3: return 0xFF00FF00u;
+      default: return 0xFFFF0000u;
+    }
+  }
+  const uint32_t bit = ((type == LOC_FIXED ? fixed : tile) >> idx) & 1u;
+  return 0u - bit;
+}
+
+template <int K>
+__device__ __forceinline__ void gate_k(float2 (&a)[32], const float4 u0, const float4 u1) {
+#pragma unroll
+  for (int j = 0; j < 32; ++j) {
+    if (j & (1 << K)) continue;
+    const float2 x = a[j], y = a[j + (1 << K)];
+    a[j].x = u0.x * x.x - u0.y * x.y + u0.z * y.x - u0.w * y.y;
+    a[j].y = u0.x * x.y + u0.y * x.x + u0.z * y.y + u0.w * y.x;
+    a[j + (1 << K)].x = u1.x * x.x - u1.y * x.y + u1.z * y.x - u1.w * y.y;
+    a[j + (1 << K)].y = u1.x * x.y + u1.y * x.x + u1.z * y.y + u1.w * y.x;
+  }
+}
+
+__device__ __forceinline__ void flush_neg(float2 (&a)[32], uint32_t neg) {
+  if (neg == 0) return;
+#pragma unroll
+  for (int j = 0; j < 32; ++j) {
+    const uint32_t s = (neg << (31 - j)) & 0x80000000u;
+    a[j].x = __uint_as_float(__float_as_uint(a[j].x) ^ s);
+    a[j].y = __uint_as_float(__float_as_uint(a[j].y) ^ s);
+  }
+}
+
+__device__ __forceinline__ float2 cmulf(float2 a, float2 b) {
+  return make_float2(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x);
+}
+
+template <int R>
+__device__ __forceinline__ void stage_body(float2* buf, uint32_t tid, uint32_t tile, const DevOp* __restrict__ ops,
+                                           uint32_t nops) {
+  float2 a[32];
+  load_stage<R>(buf, tid, a);
+  const uint32_t fixed = fixed_index<R>(tid);
+  uint32_t neg = 0;
+  for (uint32_t o = 0; o < nops; ++o) {
+    const DevOp* op = ops + o;
+    const uint32_t hdr = __ldg(&op->hdr);
+    const uint32_t code = hdr & 3u, la = (hdr >> 2) & 127u, lb = (hdr >> 9) & 127u;
+    if (code == OP_CZ) {
+      neg ^= loc_mask(la, fixed, tile) & loc_mask(lb, fixed, tile);
+      continue;
+    }
+    flush_neg(a, neg);
+    neg = 0;
+    const float4 u0 = __ldg(reinterpret_cast<const float4*>(op->v));
+    const float4 u1 = __ldg(reinterpret_cast<const float4*>(op->v) + 1);
+    if (code == OP_GATE) {
+      switch (la & 31u) {
+        case 0: gate_k<0>(a, u0, u1); break;
+        case 1: gate_k<1>(a, u0, u1); break;
+        case 2: gate_k<2>(a, u0, u1); break;
+        case 3: gate_k<3>(a, u0, u1); break;
+        default: gate_k<4>(a, u0, u1); break;
+      }
+    } else if (code == OP_DIAG) {
+      const uint32_t m = loc_mask(la, fixed, tile);
+#pragma unroll
+      for (int j = 0; j < 32; ++j) {
+        const bool b = (m >> j) & 1u;
+        a[j] = cmulf(a[j], make_float2(b ? u0.z : u0.x, b ? u0.w : u0.y));
+      }
+    } else {
+      const uint32_t m = loc_mask(la, fixed, tile) & loc_mask(lb, fixed, tile);
+#pragma unroll
+      for (int j = 0; j < 32; ++j)
+        if ((m >> j) & 1u) a[j] = cmulf(a[j], make_float2(u0.x, u0.y));
+    }
+  }
+  flush_neg(a, neg);
+  store_stage<R>(buf, tid, a);
+}
+
+__device__ __forceinline__ void load_tile(float2* buf, const float2* st, uint32_t base, const uint32_t* off_lo,
+                                          const uint32_t* off_hi, uint32_t tid) {
+#pragma unroll 4
+  for (uint32_t r = 0; r < TILE / 2 / THREADS; ++r) {
+    const uint32_t i = 2u * (tid + THREADS * r);
+    cp_async16(buf + spos(i), st + (base + off_lo[i & 127u] + off_hi[i >> 7]));
+  }
+}
+
+__device__ __forceinline__ void zero_tile(float2* buf, uint32_t tid, bool first) {
+  float4* b4 = reinterpret_cast<float4*>(buf);
+#pragma unroll 4
+  for (uint32_t r = 0; r < TILE / 2 / THREADS; ++r) {
+    const uint32_t i = 2u * (tid + THREADS * r);
+    b4[spos(i) >> 1] = make_float4(0.f, 0.f, 0.f, 0.f);
+  }
+  if (first && tid == 0) buf[0] = make_float2(1.f, 0.f);  // chunk 0 is thread 0's
+}
+
+// block-wide FP64 sums of two values in a fixed order; thread 0 gets them
+__device__ __forceinline__ void block_sum2(double& s0, double& s1, double (*red)[2], uint32_t tid) {
+#pragma unroll
+  for (int d = 16; d > 0; d >>= 1) {
+    s0 += __shfl_xor_sync(0xffffffffu, s0, d);
+    s1 += __shfl_xor_sync(0xffffffffu, s1, d);
+  }
+  if ((tid & 31u) == 0) {
+    red[tid >> 5][0] = s0;
+    red[tid >> 5][1] = s1;
+  }
+  __syncthreads();
+  if (tid == 0) {
+    s0 = red[0][0];
+    s1 = red[0][1];
+    for (uint32_t w = 1; w < THREADS / 32; ++w) {
+      s0 += red[w][0];
+      s1 += red[w][1];
+    }
+  }
+}
+
+// QuantumState::measure's decision (src/state/mod.rs:113-131)
+__device__ __forceinline__ uint32_t decide(double e, double nn, const double* draws, uint32_t& used) {
+  double p = (1.0 + e / nn) / 2.0;
+  if (!isnan(p)) p = fmin(1.0, fmax(0.0, p));
+  if (p > 1.0 - 1e-12) return 0;
+  if (p < 1e-12) return 1;
+  return draws[used++] >= p ? 1u : 0u;
+}
+
+template <int NBUF>
+__global__ void __launch_bounds__(THREADS, NBUF == 2 ? 1 : 2) k_batch(const __grid_constant__ KParams P) {
+  extern __shared__ __align__(1024) unsigned char dsm[];
+  __shared__ uint32_t off_lo[128], off_hi[64];
+  __shared__ DevPass sp;
+  __shared__ double red[THREADS / 32][2];
+  __shared__ uint32_t s_job, s_bit;
+  float2* bufs = reinterpret_cast<float2*>(dsm);
+  double* T = NBUF == 2 ? reinterpret_cast<double*>(bufs + 2 * TILE) : P.gscratch + size_t(blockIdx.x) * TILE;
+  double* G = NBUF == 2 ? T : reinterpret_cast<double*>(bufs);
+  const uint32_t tid = threadIdx.x;
+  float2* st = P.slots + size_t(blockIdx.x) * P.slot_elems;
+
+  for (;;) {
+    if (tid == 0) s_job = atomicAdd(P.queue, 1u);
+    __syncthreads();
+    const uint32_t job = s_job;
+    __syncthreads();
+    if (job >= P.count) break;
+    const uint32_t t = P.order[job];
+    const DevTraj tr = P.traj[t];
+    if (tr.n < MIN_QUBITS || tr.n > P.max_n || tr.nmeas > tr.n) {
+      if (tid == 0) atomicOr(P.err, 1u);
+      continue;
+    }
+    const uint32_t ntiles = 1u << (tr.n - TILE_BITS);
+    for (uint32_t pi = 0; pi < tr.npass; ++pi) {
+      if (tid < sizeof(DevPass) / 4)
+        reinterpret_cast<uint32_t*>(&sp)[tid] = reinterpret_cast<const uint32_t*>(P.pass + tr.pass0 + pi)[tid];
+      __syncthreads();
+      if (tid < 128) {
+        uint32_t v = 0;
+        for (uint32_t b = 0; b < 7; ++b)
+          if ((tid >> b) & 1u) v += 1u << sp.win[b];
+        off_lo[tid] = v;
+      } else if (tid < 192) {
+        const uint32_t i = tid - 128;
+        uint32_t v = 0;
+        for (uint32_t b = 0; b < 6; ++b)
+          if ((i >> b) & 1u) v += 1u << sp.win[7 + b];
+        off_hi[i] = v;
+      }
+      const bool zero = sp.flags & PASS_ZERO_INIT, accum = sp.flags & PASS_ACCUM,
+                 write = !(sp.flags & PASS_NO_WRITE);
+      if (accum) {
+#pragma unroll 4
+        for (uint32_t r = 0; r < TILE / 2 / THREADS; ++r) {
+          const uint32_t i = 2u * (tid + THREADS * r);
+          *reinterpret_cast<double2*>(T + spos(i)) = make_double2(0.0, 0.0);
+        }
+      }
+      __syncthreads();
+      auto base_of = [&](uint32_t k) {
+        uint32_t b = 0;
+        for (uint32_t i = 0; i < sp.nnon; ++i)
+          if ((k >> i) & 1u) b += 1u << sp.non[i];
+        return b;
+      };
+      const DevStage* stages = P.stage + sp.stage0;
+      const uint32_t nstage = sp.nstage;
+      if (NBUF == 2 && !zero) {
+        load_tile(bufs, st, base_of(0), off_lo, off_hi, tid);
+        cp_async_commit();
+      }
+      for (uint32_t k = 0; k < ntiles; ++k) {
+        float2* cur = bufs + (NBUF == 2 ? (k & 1u) * TILE : 0u);
+        const uint32_t base = base_of(k);
+        if (zero) {
+          zero_tile(cur, tid, k == 0);
+        } else if (NBUF == 2) {
+          if (k + 1 < ntiles) {
+            load_tile(bufs + ((k + 1) & 1u) * TILE, st, base_of(k + 1), off_lo, off_hi, tid);
+            cp_async_commit();
+            cp_async_wait<1>();
+          } else {
+            cp_async_wait<0>();
+          }
+        } else {
+          load_tile(cur, st, base, off_lo, off_hi, tid);
+          cp_async_commit();
+          cp_async_wait<0>();
+        }
+        __syncthreads();
+        for (uint32_t s = 0; s < nstage; ++s) {
+          const uint32_t info = __ldg(&stages[s].info), op0 = __ldg(&stages[s].op0);
+          const uint32_t r = info & 3u, nops = info >> 2;
+          if (r == 0) stage_body<0>(cur, tid, k, P.op + op0, nops);
+          else if (r == 1) stage_body<1>(cur, tid, k, P.op + op0, nops);
+          else stage_body<2>(cur, tid, k, P.op + op0, nops);
+          __syncthreads();
+        }
+        if (write || accum) {
+#pragma unroll 4
+          for (uint32_t r = 0; r < TILE / 2 / THREADS; ++r) {
+            const uint32_t i = 2u * (tid + THREADS * r);
+            const float4 v = *reinterpret_cast<const float4*>(cur + spos(i));
+            if (write) *reinterpret_cast<float4*>(st + (base + off_lo[i & 127u] + off_hi[i >> 7])) = v;
+            if (accum) {
+              double2* tp = reinterpret_cast<double2*>(T + spos(i));
+              double2 tv = *tp;
+              tv.x += double(v.x) * double(v.x) + double(v.y) * double(v.y);
+              tv.y += double(v.z) * double(v.z) + double(v.w) * double(v.w);
+              *tp = tv;
+            }
+          }
+        }
+        __syncthreads();
+      }
+      __threadfence();
+      __syncthreads();
+    }
+
+    // measurements M 0 .. M m-1 from the FP64 sums
+    const double* draws = P.draws + tr.draw0;
+    uint32_t used = 0;  // meaningful in thread 0
+    uint32_t o = 0;
+    double z0 = 0.0, norm = 0.0;
+    const uint32_t kl = min(tr.nmeas, TILE_BITS);
+    for (uint32_t k = 0; k < max(kl, 1u); ++k) {
+      double s0 = 0.0, s1 = 0.0;
+      const uint32_t cnt = TILE >> k;
+      for (uint32_t r = tid; r < cnt; r += THREADS) {
+        const double v = T[spos(o | (r << k))];
+        if (r & 1u) s1 += v;
+        else s0 += v;
+      }
+      block_sum2(s0, s1, red, tid);
+      if (tid == 0) {
+        const double e = s0 - s1, nn = s0 + s1;
+        if (k == 0) {
+          z0 = e / nn;
+          norm = nn;
+        }
+        s_bit = k < tr.nmeas ? decide(e, nn, draws, used) : 0u;
+      }
+      __syncthreads();
+      o |= s_bit << k;
+      __syncthreads();
+    }
+    uint64_t rec = o;
+    if (tr.nmeas > TILE_BITS) {
+      const uint32_t nh = ntiles;
+      for (uint32_t h = tid; h < nh; h += THREADS) {
+        const float2 v = st[o | (h << TILE_BITS)];
+        G[h] = double(v.x) * double(v.x) + double(v.y) * double(v.y);
+      }
+      __syncthreads();
+      uint32_t oh = 0;
+      for (uint32_t k = TILE_BITS; k < tr.nmeas; ++k) {
+        const uint32_t kk = k - TILE_BITS;
+        double s0 = 0.0, s1 = 0.0;
+        for (uint32_t r = tid; r < (nh >> kk); r += THREADS) {
+          const double v = G[oh | (r << kk)];
+          if (r & 1u) s1 += v;
+          else s0 += v;
+        }
+        block_sum2(s0, s1, red, tid);
+        if (tid == 0) s_bit = decide(s0 - s1, s0 + s1, draws, used);
+        __syncthreads();
+        oh |= s_bit << kk;
+        __syncthreads();
+      }
+      rec |= uint64_t(oh) << TILE_BITS;
+    }
+    if (tid == 0) {
+      P.out_rec[t] = rec;
+      P.out_z0[t] = z0;
+      P.out_norm[t] = norm;
+    }
+  }
+}
+
+constexpr size_t SMEM_NBUF2 = 3 * TILE * 8;  // two tiles and the FP64 sums
+constexpr size_t SMEM_NBUF1 = TILE * 8;
+
+}  // namespace
+
+// ---------------------------------------------------------------------------
+// the batch object
+// ---------------------------------------------------------------------------
+struct ncsim_batch {
+  Program prog;
+  std::vector<uint32_t> order_lpt, order_seq;
+  std::mutex mu;
+  int device = -1;
+  cudaStream_t stream = nullptr;
+  cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+  char* d_prog = nullptr;
+  size_t off_traj = 0, off_pass = 0, off_stage = 0, off_op = 0, off_draws = 0, off_lpt = 0, off_seq = 0,
+         off_sample = 0;
+  uint32_t* d_queue = nullptr;  // [0] work counter, [1] error flags
+  uint64_t* d_rec = nullptr;
+  double* d_z0 = nullptr;
+  double* d_norm = nullptr;
+  float2* d_slots = nullptr;
+  double* d_scratch = nullptr;
+  uint32_t slot_ctas = 0;
+  uint64_t* h_rec = nullptr;
+  double* h_z0 = nullptr;
+  double* h_norm = nullptr;
+  uint32_t* h_err = nullptr;
+  ncsim_batch_config cfg{0, 0, 0};  // unset until tuned or set
+  cudaGraphExec_t graph = nullptr;
+  ncsim_batch_config graph_cfg{0, 0, 0};
+  uint32_t sample_count = 0;
+  bool have_results = false;
+  double last_ms = 0.0;
+
+  ~ncsim_batch() { release(); }
+  void release() {
+    if (device < 0) return;
+    cudaSetDevice(device);
+    if (graph) cudaGraphExecDestroy(graph);
+    if (stream) cudaStreamSynchronize(stream);
+    cudaFree(d_prog);
+    cudaFree(d_queue);
+    cudaFree(d_rec);
+    cudaFree(d_z0);
+    cudaFree(d_norm);
+    cudaFree(d_slots);
+    cudaFree(d_scratch);
+    cudaFreeHost(h_rec);
+    cudaFreeHost(h_z0);
+    cudaFreeHost(h_norm);
+    cudaFreeHost(h_err);
+    if (ev0) cudaEventDestroy(ev0);
+    if (ev1) cudaEventDestroy(ev1);
+    if (stream) cudaStreamDestroy(stream);
+    graph = nullptr;
+    device = -1;
+  }
+  uint32_t count() const { return uint32_t(prog.traj.size()); }
+};
+
+namespace {
+
+size_t align_up(size_t v, size_t a) { return (v + a - 1) / a * a; }
+
+template <class T>
+T* dev_ptr(ncsim_batch* b, size_t off) {
+  return reinterpret_cast<T*>(b->d_prog + off);
+}
+
+void ensure_device(ncsim_batch* b) {
+  int dev = 0;
+  NCSIM_CUDA(cudaGetDevice(&dev));
+  if (b->device == dev) return;
+  if (b->device >= 0) b->release();
+  b->device = dev;
+  NCSIM_CUDA(cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking));
+  NCSIM_CUDA(cudaEventCreate(&b->ev0));
+  NCSIM_CUDA(cudaEventCreate(&b->ev1));
+  const Program& P = b->prog;
+  const uint32_t c = b->count();
+  size_t off = 0;
+  auto take = [&](size_t bytes) {
+    const size_t o = off;
+    off = align_up(off + bytes, 256);
+    return o;
+  };
+  b->off_traj = take(P.traj.size() * sizeof(DevTraj));
+  b->off_pass = take(P.pass.size() * sizeof(DevPass));
+  b->off_stage = take(P.stage.size() * sizeof(DevStage));
+  b->off_op = take(std::max<size_t>(1, P.op.size()) * sizeof(DevOp));
+  b->off_draws = take(std::max<size_t>(1, P.draws.size()) * sizeof(double));
+  b->off_lpt = take(size_t(c) * 4);
+  b->off_seq = take(size_t(c) * 4);
+  b->off_sample = take(size_t(c) * 4);
+  NCSIM_CUDA(cudaMalloc(&b->d_prog, off));
+  auto up = [&](size_t o, const void* src, size_t bytes) {
+    if (bytes) NCSIM_CUDA(cudaMemcpyAsync(b->d_prog + o, src, bytes, cudaMemcpyHostToDevice, b->stream));
+  };
+  up(b->off_traj, P.traj.data(), P.traj.size() * sizeof(DevTraj));
+  up(b->off_pass, P.pass.data(), P.pass.size() * sizeof(DevPass));
+  up(b->off_stage, P.stage.data(), P.stage.size() * sizeof(DevStage));
+  up(b->off_op, P.op.data(), P.op.size() * sizeof(DevOp));
+  up(b->off_draws, P.draws.data(), P.draws.size() * sizeof(double));
+  up(b->off_lpt, b->order_lpt.data(), size_t(c) * 4);
+  up(b->off_seq, b->order_seq.data(), size_t(c) * 4);
+  NCSIM_CUDA(cudaMalloc(&b->d_queue, 2 * sizeof(uint32_t)));
+  NCSIM_CUDA(cudaMalloc(&b->d_rec, size_t(c) * 8));
+  NCSIM_CUDA(cudaMalloc(&b->d_z0, size_t(c) * 8));
+  NCSIM_CUDA(cudaMalloc(&b->d_norm, size_t(c) * 8));
+  NCSIM_CUDA(cudaMallocHost(&b->h_rec, size_t(c) * 8));
+  NCSIM_CUDA(cudaMallocHost(&b->h_z0, size_t(c) * 8));
+  NCSIM_CUDA(cudaMallocHost(&b->h_norm, size_t(c) * 8));
+  NCSIM_CUDA(cudaMallocHost(&b->h_err, sizeof(uint32_t)));
+  NCSIM_CUDA(cudaStreamSynchronize(b->stream));
+  static bool attr_done[64] = {};
+  if (dev < 64 && !attr_done[dev]) {
+    NCSIM_CUDA(cudaFuncSetAttribute(k_batch<2>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(SMEM_NBUF2)));
+    NCSIM_CUDA(cudaFuncSetAttribute(k_batch<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(SMEM_NBUF1)));
+    attr_done[dev] = true;
+  }
+}
+
+uint32_t grid_for(const ncsim_batch_config& cfg) {
+  return uint32_t(sm_count()) * std::max<uint32_t>(1, cfg.ctas_per_sm);
+}
+
+void ensure_slots(ncsim_batch* b, uint32_t ctas) {
+  if (b->slot_ctas >= ctas) return;
+  NCSIM_CUDA(cudaStreamSynchronize(b->stream));
+  if (b->graph) {  // the captured launch holds the old slot pointers
+    NCSIM_CUDA(cudaGraphExecDestroy(b->graph));
+    b->graph = nullptr;
+  }
+  cudaFree(b->d_slots);
+  cudaFree(b->d_scratch);
+  b->d_slots = nullptr;
+  b->d_scratch = nullptr;
+  b->slot_ctas = 0;
+  const size_t elems = size_t(1) << b->prog.max_n;
+  NCSIM_CUDA(cudaMalloc(&b->d_slots, size_t(ctas) * elems * sizeof(float2)));
+  NCSIM_CUDA(cudaMalloc(&b->d_scratch, size_t(ctas) * TILE * sizeof(double)));
+  b->slot_ctas = ctas;
+}
+
+// one launch of the kernel over `count` jobs of the order array at order_off
+void enqueue_kernel(ncsim_batch* b, const ncsim_batch_config& cfg, size_t order_off, uint32_t count) {
+  KParams k{};
+  k.traj = dev_ptr<DevTraj>(b, b->off_traj);
+  k.pass = dev_ptr<DevPass>(b, b->off_pass);
+  k.stage = dev_ptr<DevStage>(b, b->off_stage);
+  k.op = dev_ptr<DevOp>(b, b->off_op);
+  k.draws = dev_ptr<double>(b, b->off_draws);
+  k.order = dev_ptr<uint32_t>(b, order_off);
+  k.count = count;
+  k.max_n = b->prog.max_n;
+  k.slots = b->d_slots;
+  k.slot_elems = uint64_t(1) << b->prog.max_n;
+  k.gscratch = b->d_scratch;
+  k.queue = b->d_queue;
+  k.err = b->d_queue + 1;
+  k.out_rec = b->d_rec;
+  k.out_z0 = b->d_z0;
+  k.out_norm = b->d_norm;
+  const uint32_t grid = std::min<uint32_t>(grid_for(cfg), std::max<uint32_t>(1, count));
+  if (cfg.buffers == 1) k_batch<1><<<grid, THREADS, SMEM_NBUF1, b->stream>>>(k);
+  else k_batch<2><<<grid, THREADS, SMEM_NBUF2, b->stream>>>(k);
+  NCSIM_LAUNCHED("k_batch");
+}
+
+size_t order_offset(const ncsim_batch* b, const ncsim_batch_config& cfg) {
+  return cfg.order == NCSIM_BATCH_ORDER_GIVEN ? b->off_seq : b->off_lpt;
+}
+
+// enqueue: reset counters, the kernel (between the two events when timed
+// directly; a graph launch is timed around the whole graph), results to the host
+void enqueue_run(ncsim_batch* b, const ncsim_batch_config& cfg, size_t order_off, uint32_t count, bool copy_back,
+                 bool events = true) {
+  NCSIM_CUDA(cudaMemsetAsync(b->d_queue, 0, 2 * sizeof(uint32_t), b->stream));
+  if (events) NCSIM_CUDA(cudaEventRecord(b->ev0, b->stream));
+  enqueue_kernel(b, cfg, order_off, count);
+  if (events) NCSIM_CUDA(cudaEventRecord(b->ev1, b->stream));
+  NCSIM_CUDA(cudaMemcpyAsync(b->h_err, b->d_queue + 1, sizeof(uint32_t), cudaMemcpyDeviceToHost, b->stream));
+  if (copy_back) {
+    const size_t c = b->count();
+    NCSIM_CUDA(cudaMemcpyAsync(b->h_rec, b->d_rec, c * 8, cudaMemcpyDeviceToHost, b->stream));
+    NCSIM_CUDA(cudaMemcpyAsync(b->h_z0, b->d_z0, c * 8, cudaMemcpyDeviceToHost, b->stream));
+    NCSIM_CUDA(cudaMemcpyAsync(b->h_norm, b->d_norm, c * 8, cudaMemcpyDeviceToHost, b->stream));
+  }
+}
+
+double finish_run(ncsim_batch* b) {
+  NCSIM_CUDA(cudaStreamSynchronize(b->stream));
+  if (*b->h_err) throw Error(NCSIM_ERR_DEVICE, "batched trajectory kernel rejected a trajectory descriptor");
+  float ms = 0.f;
+  NCSIM_CUDA(cudaEventElapsedTime(&ms, b->ev0, b->ev1));
+  return double(ms);
+}
+
+bool same_cfg(const ncsim_batch_config& a, const ncsim_batch_config& c) {
+  return a.ctas_per_sm == c.ctas_per_sm && a.buffers == c.buffers && a.order == c.order;
+}
+
+void validate_cfg(const ncsim_batch_config& c) {
+  if (c.buffers != 1 && c.buffers != 2) throw Error(NCSIM_ERR_INVALID, "batch config: buffers must be 1 or 2");
+  if (c.ctas_per_sm < 1 || c.ctas_per_sm > (c.buffers == 2 ? 1u : 2u))
+    throw Error(NCSIM_ERR_INVALID, "batch config: 1 CTA per SM double-buffered, 1..2 single-buffered");
+  if (c.order != NCSIM_BATCH_ORDER_LARGEST_FIRST && c.order != NCSIM_BATCH_ORDER_GIVEN)
+    throw Error(NCSIM_ERR_INVALID, "batch config: unknown order");
+}
+
+// tuned configurations, per (device, trajectory count, largest register)
+std::mutex g_tune_mu;
+std::map<std::tuple<int, uint32_t, uint32_t>, ncsim_batch_config> g_tuned;
+
+ncsim_batch_config tune(ncsim_batch* b, uint32_t sample) {
+  const uint32_t c = b->count();
+  // a small sample is all tail (the last CTAs' registers decide its time), so
+  // the default times the whole batch once per candidate after a warm-up
+  if (sample == 0) sample = c;
+  sample = std::max<uint32_t>(1, std::min(sample, c));
+  // an evenly strided sample keeps the batch's register-size mix
+  std::vector<uint32_t> pick(sample);
+  for (uint32_t i = 0; i < sample; ++i) pick[i] = uint32_t(uint64_t(i) * c / sample);
+  std::vector<uint32_t> lpt = pick;
+  std::stable_sort(lpt.begin(), lpt.end(),
+                   [&](uint32_t x, uint32_t y) { return b->prog.traj[x].n > b->prog.traj[y].n; });
+  const ncsim_batch_config cands[] = {{1, 2, NCSIM_BATCH_ORDER_LARGEST_FIRST},
+                                      {2, 1, NCSIM_BATCH_ORDER_LARGEST_FIRST},
+                                      {1, 1, NCSIM_BATCH_ORDER_LARGEST_FIRST},
+                                      {1, 2, NCSIM_BATCH_ORDER_GIVEN}};
+  ncsim_batch_config best = cands[0];
+  double best_ms = 1e300;
+  for (const auto& cf : cands) {
+    ensure_slots(b, grid_for(cf));
+    const auto& ord = cf.order == NCSIM_BATCH_ORDER_GIVEN ? pick : lpt;
+    NCSIM_CUDA(cudaMemcpyAsync(b->d_prog + b->off_sample, ord.data(), size_t(sample) * 4, cudaMemcpyHostToDevice,
+                               b->stream));
+    double ms = 1e300;
+    for (int rep = 0; rep < 2; ++rep) {  // the first is a warm-up
+      enqueue_run(b, cf, b->off_sample, sample, false);
+      const double t = finish_run(b);
+      if (rep > 0) ms = std::min(ms, t);
+    }
+    if (ms < best_ms) {
+      best_ms = ms;
+      best = cf;
+    }
+  }
+  b->sample_count = sample;
+  return best;
+}
+
+void ensure_config(ncsim_batch* b) {
+  if (b->cfg.buffers != 0) return;
+  const auto key = std::make_tuple(b->device, b->count(), b->prog.max_n);
+  {
+    std::lock_guard<std::mutex> lk(g_tune_mu);
+    auto it = g_tuned.find(key);
+    if (it != g_tuned.end()) {
+      b->cfg = it->second;
+      return;
+    }
+  }
+  b->cfg = tune(b, 0);
+  std::lock_guard<std::mutex> lk(g_tune_mu);
+  g_tuned[key] = b->cfg;
+}
+
+ncsim_batch* make_batch(std::vector<Trajectory>&& ts) {
+  auto* b = new ncsim_batch();
+  try {
+    PlanKnobs kn;
+    b->prog = compile(ts, kn);
+    const uint32_t c = b->count();
+    b->order_seq.resize(c);
+    std::iota(b->order_seq.begin(), b->order_seq.end(), 0u);
+    b->order_lpt = b->order_seq;
+    std::stable_sort(b->order_lpt.begin(), b->order_lpt.end(),
+                     [&](uint32_t x, uint32_t y) { return b->prog.traj[x].n > b->prog.traj[y].n; });
+  } catch (...) {
+    delete b;
+    throw;
+  }
+  return b;
+}
+
+template <class F>
+void parallel_for(size_t count, F&& f) {
+  std::atomic<size_t> next{0};
+  std::vector<std::string> errs(count);
+  auto work = [&] {
+    for (size_t i; (i = next.fetch_add(1)) < count;) {
+      try {
+        f(i);
+      } catch (const std::exception& e) {
+        errs[i] = e.what();
+      }
+    }
+  };
+  const unsigned hw = std::max(1u, std::min(32u, std::thread::hardware_concurrency()));
+  const unsigned nth = unsigned(std::min<size_t>(hw, std::max<size_t>(1, count / 8)));
+  std::vector<std::thread> th;
+  for (unsigned k = 1; k < nth; ++k) th.emplace_back(work);
+  work();
+  for (auto& x : th) x.join();
+  for (auto& e : errs)
+    if (!e.empty()) throw Error(NCSIM_ERR_UNSUPPORTED, e);
+}
+
+}  // namespace
+
+extern "C" {
+
+ncsim_status ncsim_batch_random_layers(uint32_t count, uint64_t seed0, uint32_t n_lo, uint32_t n_span, uint32_t depth,
+                                       double p, ncsim_batch** out) {
+  return guarded([&] {
+    if (!out) throw Error(NCSIM_ERR_INVALID, "out is null");
+    *out = nullptr;
+    if (count == 0) throw Error(NCSIM_ERR_INVALID, "a batch needs at least one trajectory");
+    if (n_span < 1) throw Error(NCSIM_ERR_INVALID, "register span must be at least 1");
+    if (n_lo < MIN_QUBITS || n_lo + n_span - 1 > MAX_QUBITS)
+      throw Error(NCSIM_ERR_UNSUPPORTED, "batched trajectories need 13..26 qubits");
+    if (!(p >= 0.0 && p <= 1.0)) throw Error(NCSIM_ERR_INVALID, "noise probability outside [0, 1]");
+    std::vector<Trajectory> ts(count);
+    parallel_for(count, [&](size_t i) { ts[i] = make_random_layers(seed0 + i, n_lo, n_span, depth, p); });
+    *out = make_batch(std::move(ts));
+  });
+}
+
+ncsim_status ncsim_batch_from_circuits(uint32_t count, const ncsim_circuit* const* circuits, const uint64_t* seeds,
+                                       ncsim_batch** out) {
+  return guarded([&] {
+    if (!out || !circuits || !seeds) throw Error(NCSIM_ERR_INVALID, "null argument");
+    *out = nullptr;
+    if (count == 0) throw Error(NCSIM_ERR_INVALID, "a batch needs at least one trajectory");
+    for (uint32_t i = 0; i < count; ++i)
+      if (!circuits[i]) throw Error(NCSIM_ERR_INVALID, "null circuit");
+    std::vector<Trajectory> ts(count);
+    parallel_for(count, [&](size_t i) { ts[i] = make_from_circuit(*circuits[i], seeds[i]); });
+    *out = make_batch(std::move(ts));
+  });
+}
+
+ncsim_status ncsim_batch_free(ncsim_batch* b) {
+  return guarded([&] { delete b; });
+}
+
+ncsim_status ncsim_batch_info(const ncsim_batch* b, ncsim_batch_stats* st) {
+  return guarded([&] {
+    if (!b || !st) throw Error(NCSIM_ERR_INVALID, "null argument");
+    const Program& P = b->prog;
+    st->trajectories = P.traj.size();
+    st->source_gates = P.source_gates;
+    st->noise_events = P.noise_events;
+    st->folded_ops = P.folded_ops;
+    st->passes = P.pass.size();
+    st->tile_passes = P.tile_passes;
+    st->tile_stages = P.tile_stages;
+    st->state_bytes = P.state_bytes;
+    st->max_qubits = P.max_n;
+    st->program_bytes = P.traj.size() * sizeof(DevTraj) + P.pass.size() * sizeof(DevPass) +
+                        P.stage.size() * sizeof(DevStage) + P.op.size() * sizeof(DevOp) + P.draws.size() * 8;
+  });
+}
+
+ncsim_status ncsim_batch_set_config(ncsim_batch* b, const ncsim_batch_config* cfg) {
+  return guarded([&] {
+    if (!b || !cfg) throw Error(NCSIM_ERR_INVALID, "null argument");
+    validate_cfg(*cfg);
+    std::lock_guard<std::mutex> lk(b->mu);
+    b->cfg = *cfg;
+  });
+}
+
+ncsim_status ncsim_batch_get_config(ncsim_batch* b, ncsim_batch_config* cfg) {
+  return guarded([&] {
+    if (!b || !cfg) throw Error(NCSIM_ERR_INVALID, "null argument");
+    std::lock_guard<std::mutex> lk(b->mu);
+    ensure_device(b);
+    ensure_config(b);
+    *cfg = b->cfg;
+  });
+}
+
+ncsim_status ncsim_batch_tune(ncsim_batch* b, uint32_t sample, ncsim_batch_config* best) {
+  return guarded([&] {
+    if (!b) throw Error(NCSIM_ERR_INVALID, "null batch");
+    std::lock_guard<std::mutex> lk(b->mu);
+    ensure_device(b);
+    b->cfg = tune(b, sample);
+    {
+      std::lock_guard<std::mutex> g(g_tune_mu);
+      g_tuned[std::make_tuple(b->device, b->count(), b->prog.max_n)] = b->cfg;
+    }
+    if (best) *best = b->cfg;
+  });
+}
+
+ncsim_status ncsim_batch_run(ncsim_batch* b, double* device_ms) {
+  return guarded([&] {
+    if (!b) throw Error(NCSIM_ERR_INVALID, "null batch");
+    std::lock_guard<std::mutex> lk(b->mu);
+    ensure_device(b);
+    ensure_config(b);
+    ensure_slots(b, grid_for(b->cfg));
+    if (!b->graph || !same_cfg(b->graph_cfg, b->cfg)) {
+      if (b->graph) {
+        NCSIM_CUDA(cudaGraphExecDestroy(b->graph));
+        b->graph = nullptr;
+      }
+      cudaGraph_t g = nullptr;
+      NCSIM_CUDA(cudaStreamBeginCapture(b->stream, cudaStreamCaptureModeThreadLocal));
+      try {
+        enqueue_run(b, b->cfg, order_offset(b, b->cfg), b->count(), true, false);
+      } catch (...) {
+        cudaStreamEndCapture(b->stream, &g);
+        if (g) cudaGraphDestroy(g);
+        throw;
+      }
+      NCSIM_CUDA(cudaStreamEndCapture(b->stream, &g));
+      const cudaError_t e = cudaGraphInstantiate(&b->graph, g, 0);
+      cudaGraphDestroy(g);
+      NCSIM_CUDA(e);
+      b->graph_cfg = b->cfg;
+    }
+    NCSIM_CUDA(cudaEventRecord(b->ev0, b->stream));
+    NCSIM_CUDA(cudaGraphLaunch(b->graph, b->stream));
+    NCSIM_CUDA(cudaEventRecord(b->ev1, b->stream));
+    b->last_ms = finish_run(b);
+    b->have_results = true;
+    if (device_ms) *device_ms = b->last_ms;
+  });
+}
+
+ncsim_status ncsim_batch_results(ncsim_batch* b, uint32_t* n, uint64_t* records, double* z0, double* norm) {
+  return guarded([&] {
+    if (!b) throw Error(NCSIM_ERR_INVALID, "null batch");
+    std::lock_guard<std::mutex> lk(b->mu);
+    if (!b->have_results) throw Error(NCSIM_ERR_INVALID, "the batch has not run");
+    const uint32_t c = b->count();
+    for (uint32_t i = 0; i < c; ++i) {
+      if (n) n[i] = b->prog.traj[i].n;
+      if (records) records[i] = b->h_rec[i];
+      if (z0) z0[i] = b->h_z0[i];
+      if (norm) norm[i] = b->h_norm[i];
+    }
+  });
+}
+
+ncsim_status ncsim_batch_emulate(const ncsim_batch* b, uint32_t t, uint64_t* record, double* z0, double* norm) {
+  return guarded([&] {
+    if (!b) throw Error(NCSIM_ERR_INVALID, "null batch");
+    if (t >= b->prog.traj.size()) throw Error(NCSIM_ERR_INVALID, "trajectory index out of range");
+    if (b->prog.traj[t].n > 22) throw Error(NCSIM_ERR_UNSUPPORTED, "host emulation is limited to 22 qubits");
+    const EmuResult r = emulate(b->prog, t);
+    if (record) *record = r.record;
+    if (z0) *z0 = r.z0;
+    if (norm) *norm = r.norm;
+  });
+}
+
+ncsim_status ncsim_batch_trajectory_qubits(const ncsim_batch* b, uint32_t* n) {
+  return guarded([&] {
+    if (!b || !n) throw Error(NCSIM_ERR_INVALID, "null argument");
+    for (size_t i = 0; i < b->prog.traj.size(); ++i) n[i] = b->prog.traj[i].n;
+  });
+}
+
+}  // extern "C"

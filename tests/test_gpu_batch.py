@@ -1,0 +1,108 @@
+"""The batching form on the device: one persistent kernel over many noisy
+trajectories (complex64 amplitudes, FP32 gate arithmetic, FP64 reductions),
+against the FP64 oracle's trajectories and the host emulator of the same
+device program.
+
+Bar: the same record for every trajectory (no outcome probability here lies
+within 1e-5 of its draw), <Z0>/<psi|psi> within 1e-5 of the oracle; results
+independent of the launch configuration (bit-identical), and stable across
+CUDA graph replays.
+"""
+from __future__ import annotations
+
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+Z0_TOL = 1e-5
+
+CONFIGS = [
+    dict(ctas_per_sm=1, buffers=2, order="largest_first"),
+    dict(ctas_per_sm=2, buffers=1, order="largest_first"),
+    dict(ctas_per_sm=1, buffers=1, order="given"),
+]
+
+
+def _bits(rec):
+    return sum(int(v) << k for k, v in enumerate(rec))
+
+
+def test_batch_matches_oracle_trajectories(nb, oracle):
+    count = 24
+    b = nb.TrajectoryBatch.random_layers(count, seed0=1, n_lo=13, n_span=3, depth=8, p=0.05)
+    b.set_config(**CONFIGS[0])
+    b.run()
+    n, rec, z0, norm = b.results()
+    for t in range(count):
+        n_o, z0_o, rec_o = oracle.trajectory(1 + t, 13, 3, 8, 0.05)
+        assert n[t] == n_o
+        assert int(rec[t]) == _bits(rec_o), t
+        assert abs(z0[t] - z0_o) < Z0_TOL
+        assert abs(norm[t] - 1) < 1e-4
+
+
+@pytest.mark.parametrize("cfg", CONFIGS)
+def test_configurations_agree(nb, cfg):
+    b = nb.TrajectoryBatch.random_layers(40, seed0=100, n_lo=13, n_span=6, depth=12, p=0.01)
+    b.set_config(**CONFIGS[0])
+    b.run()
+    ref = b.results()
+    b.set_config(**cfg)
+    b.run()
+    got = b.results()
+    for x, y in zip(ref, got):
+        assert np.array_equal(x, y)
+
+
+def test_larger_registers_match_emulator(nb):
+    """Registers of 16..18 qubits (tile numbers, several windows, high-qubit
+    measurement gathers) against the FP64 host run of the same program."""
+    b = nb.TrajectoryBatch.random_layers(6, seed0=9, n_lo=16, n_span=3, depth=10, p=0.02)
+    b.run()
+    n, rec, z0, norm = b.results()
+    for t in range(6):
+        r, z, nn = b.emulate(t)
+        assert int(rec[t]) == r
+        assert abs(z0[t] - z) < Z0_TOL
+        assert abs(norm[t] - nn) < 1e-4
+
+
+def test_given_circuits_match_oracle(nb, oracle):
+    n = 14
+    text = oracle.random_circuit_text(n, 6, 5, 0.1, 0, n)
+    gates = "\n".join(l for l in text.splitlines() if not l.startswith("M ")) + "\n"
+    seeds = [21, 22, 23]
+    b = nb.TrajectoryBatch.from_circuits([nb.Circuit.parse(text)] * 3, seeds)
+    b.run()
+    _, rec, z0, _ = b.results()
+    for t, seed in enumerate(seeds):
+        o = oracle.StateVector(n)
+        rng = oracle.StdRng(seed)
+        o.run(oracle.Circuit(gates), rng)
+        z0_o = o.expectation("Z" + "_" * (n - 1)).real / o.norm_sq().real
+        rec_o = o.run(oracle.Circuit(f"QUBITS {n}\n" + "".join(f"M {q}\n" for q in range(n))), rng)
+        assert int(rec[t]) == _bits(rec_o)
+        assert abs(z0[t] - z0_o) < Z0_TOL
+
+
+def test_graph_replay_and_tuner(nb):
+    b = nb.TrajectoryBatch.random_layers(64, seed0=3, n_lo=13, n_span=4, depth=6, p=0.01)
+    best = b.tune(32)
+    assert best["buffers"] in (1, 2) and best["ctas_per_sm"] in (1, 2)
+    assert b.config() == best
+    ms1 = b.run()
+    r1 = b.results()
+    ms2 = b.run()
+    r2 = b.results()
+    assert ms1 > 0 and ms2 > 0
+    for x, y in zip(r1, r2):
+        assert np.array_equal(x, y)
+
+
+def test_results_before_run_refused(nb):
+    b = nb.TrajectoryBatch.random_layers(2, seed0=1, n_lo=13, n_span=1, depth=2, p=0.0)
+    with pytest.raises(nb.SimError):
+        b.results()
+    with pytest.raises(nb.SimError):
+        b.set_config(ctas_per_sm=2, buffers=2)
