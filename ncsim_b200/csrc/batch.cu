@@ -71,132 +71,194 @@ __device__ __forceinline__ uint32_t fixed_index(uint32_t tid) {
   return tid;
 }
 
+// A thread's 32 amplitudes, interleaved (re, im), over the stage's five tile bits.
+struct Regs {
+  float2 a[32];
+};
+
 template <int R>
-__device__ __forceinline__ void load_stage(const float2* buf, uint32_t tid, float2 (&a)[32]) {
+__device__ __forceinline__ void load_stage(const float2* buf, uint32_t tid, Regs& r) {
   if (R == 0) {
     const float4* b4 = reinterpret_cast<const float4*>(buf) + (tid << 4);
     const uint32_t x = tid & 7u;
 #pragma unroll
     for (uint32_t m = 0; m < 16; ++m) {
       const float4 v = b4[m ^ x];
-      a[2 * m] = make_float2(v.x, v.y);
-      a[2 * m + 1] = make_float2(v.z, v.w);
+      r.a[2 * m] = make_float2(v.x, v.y);
+      r.a[2 * m + 1] = make_float2(v.z, v.w);
     }
   } else if (R == 1) {
     const uint32_t f = fixed_index<1>(tid);
 #pragma unroll
-    for (uint32_t j = 0; j < 32; ++j) a[j] = buf[(f ^ ((j & 7u) << 1)) + (j << 5)];
+    for (uint32_t j = 0; j < 32; ++j) r.a[j] = buf[(f ^ ((j & 7u) << 1)) + (j << 5)];
   } else {
     const uint32_t f = tid ^ (((tid >> 5) & 7u) << 1);
 #pragma unroll
-    for (uint32_t j = 0; j < 32; ++j) a[j] = buf[f + (j << 8)];
+    for (uint32_t j = 0; j < 32; ++j) r.a[j] = buf[f + (j << 8)];
   }
 }
 
 template <int R>
-__device__ __forceinline__ void store_stage(float2* buf, uint32_t tid, const float2 (&a)[32]) {
+__device__ __forceinline__ void store_stage(float2* buf, uint32_t tid, const Regs& r) {
   if (R == 0) {
     float4* b4 = reinterpret_cast<float4*>(buf) + (tid << 4);
     const uint32_t x = tid & 7u;
 #pragma unroll
-    for (uint32_t m = 0; m < 16; ++m) b4[m ^ x] = make_float4(a[2 * m].x, a[2 * m].y, a[2 * m + 1].x, a[2 * m + 1].y);
+    for (uint32_t m = 0; m < 16; ++m)
+      b4[m ^ x] = make_float4(r.a[2 * m].x, r.a[2 * m].y, r.a[2 * m + 1].x, r.a[2 * m + 1].y);
   } else if (R == 1) {
     const uint32_t f = fixed_index<1>(tid);
 #pragma unroll
-    for (uint32_t j = 0; j < 32; ++j) buf[(f ^ ((j & 7u) << 1)) + (j << 5)] = a[j];
+    for (uint32_t j = 0; j < 32; ++j) buf[(f ^ ((j & 7u) << 1)) + (j << 5)] = r.a[j];
   } else {
     const uint32_t f = tid ^ (((tid >> 5) & 7u) << 1);
 #pragma unroll
-    for (uint32_t j = 0; j < 32; ++j) buf[f + (j << 8)] = a[j];
+    for (uint32_t j = 0; j < 32; ++j) buf[f + (j << 8)] = r.a[j];
+  }
+}
+
+// mask over j = 0..31 of the amplitudes whose register bit k is 1
+__device__ __forceinline__ uint32_t reg_pattern(uint32_t k) {
+  switch (k) {
+    case 0: return 0xAAAAAAAAu;
+    case 1: return 0xCCCCCCCCu;
+    case 2: return 0xF0F0F0F0u;
+    case 3: return 0xFF00FF00u;
+    default: return 0xFFFF0000u;
   }
 }
 
 // 32-bit mask over the thread's amplitudes j whose bit of the located qubit is 1
 __device__ __forceinline__ uint32_t loc_mask(uint32_t loc, uint32_t fixed, uint32_t tile) {
   const uint32_t type = loc >> 5, idx = loc & 31u;
-  if (type == LOC_REG) {
-    switch (idx) {
-      case 0: return 0xAAAAAAAAu;
-      case 1: return 0xCCCCCCCCu;
-      case 2: return 0xF0F0F0F0u;
-      case 3: return 0xFF00FF00u;
-      default: return 0xFFFF0000u;
-    }
-  }
+  if (type == LOC_REG) return reg_pattern(idx);
   const uint32_t bit = ((type == LOC_FIXED ? fixed : tile) >> idx) & 1u;
   return 0u - bit;
 }
 
-template <int K>
-__device__ __forceinline__ void gate_k(float2 (&a)[32], const float4 u0, const float4 u1) {
+// the sign bit (as a float bit mask) of bit j of m
+__device__ __forceinline__ uint32_t sgn(uint32_t m, int j) { return (m << (31 - j)) & 0x80000000u; }
+__device__ __forceinline__ float flip(float v, uint32_t s) { return __uint_as_float(__float_as_uint(v) ^ s); }
+
+// 2x2 gate on register bit K: u0 = (u00, u01), u1 = (u10, u11) as (re, im).
+// REL: the second amplitude of pair j is negated first where bit j of rel is set.
+template <int K, bool REL>
+__device__ __forceinline__ void gate_k(Regs& r, const float4 u0, const float4 u1, uint32_t rel) {
 #pragma unroll
   for (int j = 0; j < 32; ++j) {
     if (j & (1 << K)) continue;
-    const float2 x = a[j], y = a[j + (1 << K)];
-    a[j].x = u0.x * x.x - u0.y * x.y + u0.z * y.x - u0.w * y.y;
-    a[j].y = u0.x * x.y + u0.y * x.x + u0.z * y.y + u0.w * y.x;
-    a[j + (1 << K)].x = u1.x * x.x - u1.y * x.y + u1.z * y.x - u1.w * y.y;
-    a[j + (1 << K)].y = u1.x * x.y + u1.y * x.x + u1.z * y.y + u1.w * y.x;
+    float2 y = r.a[j + (1 << K)];
+    if (REL) {
+      const uint32_t sg = sgn(rel, j);
+      y = make_float2(flip(y.x, sg), flip(y.y, sg));
+    }
+    const float2 x = r.a[j];
+    r.a[j].x = u0.x * x.x - u0.y * x.y + u0.z * y.x - u0.w * y.y;
+    r.a[j].y = u0.x * x.y + u0.y * x.x + u0.z * y.y + u0.w * y.x;
+    r.a[j + (1 << K)].x = u1.x * x.x - u1.y * x.y + u1.z * y.x - u1.w * y.y;
+    r.a[j + (1 << K)].y = u1.x * x.y + u1.y * x.x + u1.z * y.y + u1.w * y.x;
   }
 }
 
-__device__ __forceinline__ void flush_neg(float2 (&a)[32], uint32_t neg) {
-  if (neg == 0) return;
+// balanced gate s [[1, w], [1, -w]] on register bit K: c = (s w.re, s w.im, s)
+template <int K, bool REL>
+__device__ __forceinline__ void bgate_k(Regs& r, const float4 c, uint32_t rel) {
 #pragma unroll
   for (int j = 0; j < 32; ++j) {
-    const uint32_t s = (neg << (31 - j)) & 0x80000000u;
-    a[j].x = __uint_as_float(__float_as_uint(a[j].x) ^ s);
-    a[j].y = __uint_as_float(__float_as_uint(a[j].y) ^ s);
+    if (j & (1 << K)) continue;
+    const float2 x = r.a[j], y = r.a[j + (1 << K)];
+    float tr = c.x * y.x - c.y * y.y, ti = c.x * y.y + c.y * y.x;
+    if (REL) {
+      const uint32_t sg = sgn(rel, j);
+      tr = flip(tr, sg);
+      ti = flip(ti, sg);
+    }
+    r.a[j] = make_float2(fmaf(c.z, x.x, tr), fmaf(c.z, x.y, ti));
+    r.a[j + (1 << K)] = make_float2(fmaf(c.z, x.x, -tr), fmaf(c.z, x.y, -ti));
   }
 }
 
-__device__ __forceinline__ float2 cmulf(float2 a, float2 b) {
-  return make_float2(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x);
+template <int K>
+__device__ __forceinline__ void any_gate(Regs& r, bool bal, float4 u0, float4 u1, uint32_t rel) {
+  // a relative sign on every pair is a sign on the gate's second column
+  if (rel == ~reg_pattern(K)) {
+    if (bal) {
+      u0.x = -u0.x;
+      u0.y = -u0.y;
+    } else {
+      u0.z = -u0.z;
+      u0.w = -u0.w;
+      u1.z = -u1.z;
+      u1.w = -u1.w;
+    }
+    rel = 0;
+  }
+  if (bal) {
+    if (rel) bgate_k<K, true>(r, u0, rel);
+    else bgate_k<K, false>(r, u0, 0);
+  } else {
+    if (rel) gate_k<K, true>(r, u0, u1, rel);
+    else gate_k<K, false>(r, u0, u1, 0);
+  }
 }
 
-template <int R>
-__device__ __forceinline__ void stage_body(float2* buf, uint32_t tid, uint32_t tile, const DevOp* __restrict__ ops,
-                                           uint32_t nops) {
-  float2 a[32];
-  load_stage<R>(buf, tid, a);
-  const uint32_t fixed = fixed_index<R>(tid);
+// negate the amplitudes j with bit j of neg set (the pending CZ signs)
+__device__ __forceinline__ void flush_neg(Regs& r, uint32_t neg) {
+#pragma unroll
+  for (int j = 0; j < 32; ++j) {
+    const uint32_t sg = sgn(neg, j);
+    r.a[j] = make_float2(flip(r.a[j].x, sg), flip(r.a[j].y, sg));
+  }
+}
+
+// amplitude j *= (bit j of m ? d1 : d0)
+__device__ __forceinline__ void diag_mask(Regs& r, uint32_t m, float2 d0, float2 d1) {
+#pragma unroll
+  for (int j = 0; j < 32; ++j) {
+    const bool b = (m >> j) & 1u;
+    const float dr = b ? d1.x : d0.x, di = b ? d1.y : d0.y;
+    const float2 v = r.a[j];
+    r.a[j] = make_float2(v.x * dr - v.y * di, v.x * di + v.y * dr);
+  }
+}
+
+// The ops of one stage on the registers (shared by the three layouts).  CZ
+// signs stay pending as a mask over the 32 amplitudes until a gate absorbs
+// them: the sign common to both amplitudes of a pair stays pending, the
+// relative one is applied inside the gate; diagonals commute with the mask.
+__device__ __forceinline__ void apply_ops(Regs& r, uint32_t fixed, uint32_t tile, const DevOp* ops, uint32_t nops) {
   uint32_t neg = 0;
   for (uint32_t o = 0; o < nops; ++o) {
     const DevOp* op = ops + o;
-    const uint32_t hdr = __ldg(&op->hdr);
-    const uint32_t code = hdr & 3u, la = (hdr >> 2) & 127u, lb = (hdr >> 9) & 127u;
+    const uint32_t hdr = op->hdr;
+    const uint32_t code = hdr & 7u, la = (hdr >> 3) & 127u, lb = (hdr >> 10) & 127u;
     if (code == OP_CZ) {
       neg ^= loc_mask(la, fixed, tile) & loc_mask(lb, fixed, tile);
       continue;
     }
-    flush_neg(a, neg);
-    neg = 0;
-    const float4 u0 = __ldg(reinterpret_cast<const float4*>(op->v));
-    const float4 u1 = __ldg(reinterpret_cast<const float4*>(op->v) + 1);
-    if (code == OP_GATE) {
-      switch (la & 31u) {
-        case 0: gate_k<0>(a, u0, u1); break;
-        case 1: gate_k<1>(a, u0, u1); break;
-        case 2: gate_k<2>(a, u0, u1); break;
-        case 3: gate_k<3>(a, u0, u1); break;
-        default: gate_k<4>(a, u0, u1); break;
+    const float4 u0 = reinterpret_cast<const float4*>(op->v)[0];
+    const float4 u1 = reinterpret_cast<const float4*>(op->v)[1];
+    if (code == OP_GATE || code == OP_BGATE) {
+      const uint32_t k = la & 31u, sh = 1u << k, lo = ~reg_pattern(k);
+      const uint32_t rel = (neg ^ (neg >> sh)) & lo;
+      const uint32_t common = neg & lo;
+      neg = common | (common << sh);
+      const bool bal = code == OP_BGATE;
+      switch (k) {
+        case 0: any_gate<0>(r, bal, u0, u1, rel); break;
+        case 1: any_gate<1>(r, bal, u0, u1, rel); break;
+        case 2: any_gate<2>(r, bal, u0, u1, rel); break;
+        case 3: any_gate<3>(r, bal, u0, u1, rel); break;
+        default: any_gate<4>(r, bal, u0, u1, rel); break;
       }
     } else if (code == OP_DIAG) {
-      const uint32_t m = loc_mask(la, fixed, tile);
-#pragma unroll
-      for (int j = 0; j < 32; ++j) {
-        const bool b = (m >> j) & 1u;
-        a[j] = cmulf(a[j], make_float2(b ? u0.z : u0.x, b ? u0.w : u0.y));
-      }
+      diag_mask(r, loc_mask(la, fixed, tile), make_float2(u0.x, u0.y), make_float2(u0.z, u0.w));
     } else {
-      const uint32_t m = loc_mask(la, fixed, tile) & loc_mask(lb, fixed, tile);
-#pragma unroll
-      for (int j = 0; j < 32; ++j)
-        if ((m >> j) & 1u) a[j] = cmulf(a[j], make_float2(u0.x, u0.y));
+      diag_mask(r, loc_mask(la, fixed, tile) & loc_mask(lb, fixed, tile), make_float2(1.f, 0.f),
+                make_float2(u0.x, u0.y));
     }
   }
-  flush_neg(a, neg);
-  store_stage<R>(buf, tid, a);
+  if (neg) flush_neg(r, neg);
 }
 
 __device__ __forceinline__ void load_tile(float2* buf, const float2* st, uint32_t base, const uint32_t* off_lo,
@@ -254,6 +316,8 @@ __global__ void __launch_bounds__(THREADS, NBUF == 2 ? 1 : 2) k_batch(const __gr
   extern __shared__ __align__(1024) unsigned char dsm[];
   __shared__ uint32_t off_lo[128], off_hi[64];
   __shared__ DevPass sp;
+  __shared__ DevOp s_ops[MAX_PASS_OPS];
+  __shared__ uint2 s_stage[MAX_PASS_OPS];
   __shared__ double red[THREADS / 32][2];
   __shared__ uint32_t s_job, s_bit;
   float2* bufs = reinterpret_cast<float2*>(dsm);
@@ -293,6 +357,20 @@ __global__ void __launch_bounds__(THREADS, NBUF == 2 ? 1 : 2) k_batch(const __gr
       }
       const bool zero = sp.flags & PASS_ZERO_INIT, accum = sp.flags & PASS_ACCUM,
                  write = !(sp.flags & PASS_NO_WRITE);
+      // the pass's stages and ops (contiguous, at most MAX_PASS_OPS) into shared memory
+      const uint32_t nstage = min(uint32_t(sp.nstage), MAX_PASS_OPS);
+      uint32_t op_first = 0, op_count = 0;
+      if (nstage) {
+        const DevStage first = P.stage[sp.stage0], last = P.stage[sp.stage0 + nstage - 1];
+        op_first = first.op0;
+        op_count = min(last.op0 + (last.info >> 2) - op_first, MAX_PASS_OPS);
+      }
+      for (uint32_t i = tid; i < nstage; i += THREADS) {
+        const DevStage d = P.stage[sp.stage0 + i];
+        s_stage[i] = make_uint2(d.info, d.op0 - op_first);
+      }
+      for (uint32_t i = tid; i < op_count * 3; i += THREADS)
+        reinterpret_cast<uint4*>(s_ops)[i] = reinterpret_cast<const uint4*>(P.op + op_first)[i];
       if (accum) {
 #pragma unroll 4
         for (uint32_t r = 0; r < TILE / 2 / THREADS; ++r) {
@@ -307,8 +385,6 @@ __global__ void __launch_bounds__(THREADS, NBUF == 2 ? 1 : 2) k_batch(const __gr
           if ((k >> i) & 1u) b += 1u << sp.non[i];
         return b;
       };
-      const DevStage* stages = P.stage + sp.stage0;
-      const uint32_t nstage = sp.nstage;
       if (NBUF == 2 && !zero) {
         load_tile(bufs, st, base_of(0), off_lo, off_hi, tid);
         cp_async_commit();
@@ -333,11 +409,18 @@ __global__ void __launch_bounds__(THREADS, NBUF == 2 ? 1 : 2) k_batch(const __gr
         }
         __syncthreads();
         for (uint32_t s = 0; s < nstage; ++s) {
-          const uint32_t info = __ldg(&stages[s].info), op0 = __ldg(&stages[s].op0);
-          const uint32_t r = info & 3u, nops = info >> 2;
-          if (r == 0) stage_body<0>(cur, tid, k, P.op + op0, nops);
-          else if (r == 1) stage_body<1>(cur, tid, k, P.op + op0, nops);
-          else stage_body<2>(cur, tid, k, P.op + op0, nops);
+          const uint2 d = s_stage[s];
+          const uint32_t r = d.x & 3u;
+          const uint32_t nops = min(d.x >> 2, op_count - min(d.y, op_count));
+          Regs regs;
+          if (r == 0) load_stage<0>(cur, tid, regs);
+          else if (r == 1) load_stage<1>(cur, tid, regs);
+          else load_stage<2>(cur, tid, regs);
+          const uint32_t fixed = r == 0 ? fixed_index<0>(tid) : r == 1 ? fixed_index<1>(tid) : fixed_index<2>(tid);
+          apply_ops(regs, fixed, k, s_ops + d.y, nops);
+          if (r == 0) store_stage<0>(cur, tid, regs);
+          else if (r == 1) store_stage<1>(cur, tid, regs);
+          else store_stage<2>(cur, tid, regs);
           __syncthreads();
         }
         if (write || accum) {

@@ -52,11 +52,37 @@ struct Folder {
     pend[q] = mat_mul(g, pend[q]);
     if (!is_zero(g[1]) || !is_zero(g[2])) nondiag[q] = 1;
   }
+  // A balanced unitary (every entry of modulus 1/sqrt2) is diag(l0, l1) B(w)
+  // with B(w) = s [[1, w], [1, -w]]: B goes to the device, the diagonal stays
+  // pending on the qubit (it commutes with the two-qubit diagonals) and is
+  // multiplied into the qubit's next gate.
   void emit_gate(uint32_t q) {
+    const M2 u = pend[q];
+    const double s = 0.70710678118654752440;
+    auto mod = [](Cd c) { return std::sqrt(c.re * c.re + c.im * c.im); };
+    bool balanced = true;
+    for (int i = 0; i < 4; ++i) balanced = balanced && std::fabs(mod(u[i]) - s) < 1e-12;
     QOp o;
-    o.code = OP_GATE;
     o.a = q;
-    for (int i = 0; i < 4; ++i) o.m[i] = pend[q][i];
+    if (balanced) {
+      const Cd l0{u[0].re / s, u[0].im / s}, l1{u[2].re / s, u[2].im / s};
+      // w = u01 / u00 (|u00| = s)
+      const double n0 = u[0].re * u[0].re + u[0].im * u[0].im;
+      const Cd w{(u[1].re * u[0].re + u[1].im * u[0].im) / n0, (u[1].im * u[0].re - u[1].re * u[0].im) / n0};
+      // unitarity makes u11 = -l1 s w; anything else is not this form
+      const Cd u11 = cmul(l1, Cd{-s * w.re, -s * w.im});
+      if (std::fabs(u11.re - u[3].re) < 1e-12 && std::fabs(u11.im - u[3].im) < 1e-12) {
+        o.code = OP_BGATE;
+        o.m[0] = Cd{s * w.re, s * w.im};
+        o.m[1] = Cd{s, 0.0};
+        out.push_back(o);
+        pend[q] = {l0, Cd{0, 0}, Cd{0, 0}, l1};
+        nondiag[q] = 0;
+        return;
+      }
+    }
+    o.code = OP_GATE;
+    for (int i = 0; i < 4; ++i) o.m[i] = u[i];
     out.push_back(o);
     pend[q] = pauli_matrix(0, 0);
     nondiag[q] = 0;
@@ -248,28 +274,59 @@ uint64_t qmask(const QOp& o) {
   return m;
 }
 
-// list scheduling: ops in order, an op that cannot go (ok false, or a qubit
-// held back by an earlier op) holds back its qubits
+bool is_gate(const QOp& o) { return o.code == OP_GATE || o.code == OP_BGATE; }
+
+// List scheduling: ops in order.  A gate that cannot go holds back every later
+// op on its qubit; a diagonal that cannot go holds back only later gates on
+// its qubits (diagonals commute with one another).  Then a taken diagonal
+// that no later taken gate on its qubits follows, while the program still has
+// a gate on one of them (later[i]), is put back: it waits for the stage of
+// that gate, which absorbs its signs.
 template <class Ok>
-void schedule(const std::vector<uint32_t>& pend, const std::vector<QOp>& ops, Ok ok, std::vector<uint32_t>& taken,
-              std::vector<uint32_t>& rest) {
+void schedule(const std::vector<uint32_t>& pend, const std::vector<QOp>& ops, const std::vector<char>& later, Ok ok,
+              std::vector<uint32_t>& taken, std::vector<uint32_t>& rest) {
   taken.clear();
   rest.clear();
-  uint64_t blocked = 0;
+  uint64_t block_all = 0, block_gates = 0;
   for (uint32_t i : pend) {
-    const uint64_t m = qmask(ops[i]);
-    if ((m & blocked) || !ok(ops[i])) {
-      blocked |= m;
+    const QOp& o = ops[i];
+    const uint64_t m = qmask(o);
+    if (is_gate(o)) {
+      if ((m & (block_all | block_gates)) || !ok(o)) {
+        block_all |= m;
+        rest.push_back(i);
+      } else {
+        taken.push_back(i);
+      }
+    } else if ((m & block_all) || !ok(o)) {
+      block_gates |= m;
       rest.push_back(i);
     } else {
       taken.push_back(i);
     }
   }
+  uint64_t gated = 0;
+  bool deferred = false;
+  for (size_t k = taken.size(); k-- > 0;) {
+    const QOp& o = ops[taken[k]];
+    const uint64_t m = qmask(o);
+    if (is_gate(o)) {
+      gated |= m;
+    } else if (!(m & gated) && later[taken[k]]) {
+      rest.push_back(taken[k]);
+      taken[k] = UINT32_MAX;
+      deferred = true;
+    }
+  }
+  if (deferred) {
+    taken.erase(std::remove(taken.begin(), taken.end(), UINT32_MAX), taken.end());
+    std::sort(rest.begin(), rest.end());
+  }
 }
 
 size_t gate_count(const std::vector<uint32_t>& idx, const std::vector<QOp>& ops) {
   size_t c = 0;
-  for (uint32_t i : idx) c += ops[i].code == OP_GATE;
+  for (uint32_t i : idx) c += is_gate(ops[i]);
   return c;
 }
 
@@ -306,6 +363,16 @@ void compile_one(const Trajectory& t, const PlanKnobs& kn, Local& L) {
 
   std::vector<uint32_t> pend(t.ops.size()), taken, rest, staken, srest;
   for (uint32_t i = 0; i < pend.size(); ++i) pend[i] = i;
+  // later[i]: a gate on one of op i's qubits comes after it
+  std::vector<char> later(t.ops.size(), 0);
+  {
+    uint64_t seen = 0;
+    for (size_t i = t.ops.size(); i-- > 0;) {
+      const uint64_t m = qmask(t.ops[i]);
+      later[i] = (seen & m) != 0;
+      if (is_gate(t.ops[i])) seen |= m;
+    }
+  }
   size_t last_window = 0, turn = 0;
   bool any = false;
   while (!pend.empty()) {
@@ -313,7 +380,7 @@ void compile_one(const Trajectory& t, const PlanKnobs& kn, Local& L) {
     std::vector<uint32_t> best_t, best_r;
     for (size_t k = 0; k < ws.size(); ++k) {
       const size_t w = kn.greedy_windows ? k : (turn + k) % ws.size();
-      schedule(pend, t.ops, [&](const QOp& o) { return o.code != OP_GATE || wpos[w][o.a] >= 0; }, taken, rest);
+      schedule(pend, t.ops, later, [&](const QOp& o) { return !is_gate(o) || wpos[w][o.a] >= 0; }, taken, rest);
       if (taken.size() > best_t.size()) {
         best_w = w;
         best_t = taken;
@@ -322,6 +389,12 @@ void compile_one(const Trajectory& t, const PlanKnobs& kn, Local& L) {
       }
     }
     if (best_t.empty()) throw Error(NCSIM_ERR_INVALID, "batch planner: no window takes the next op");
+    if (best_t.size() > MAX_PASS_OPS) {
+      // a prefix of a list schedule is itself one: the rest waits for a later pass
+      best_r.insert(best_r.end(), best_t.begin() + MAX_PASS_OPS, best_t.end());
+      best_t.resize(MAX_PASS_OPS);
+      std::sort(best_r.begin(), best_r.end());
+    }
     turn = best_w + 1;
     const size_t w = best_w;
     DevPass& ps = add_pass(w, any ? 0 : PASS_ZERO_INIT);
@@ -339,8 +412,8 @@ void compile_one(const Trajectory& t, const PlanKnobs& kn, Local& L) {
       for (uint32_t k = 0; k < NSEL; ++k) {
         const uint32_t r = kn.greedy_stages ? k : (cyc + k) % NSEL;
         const int lo = int(RSHIFT[r]), hi = lo + int(REG_BITS);
-        schedule(sp, t.ops,
-                 [&](const QOp& o) { return o.code != OP_GATE || (wpos[w][o.a] >= lo && wpos[w][o.a] < hi); }, staken,
+        schedule(sp, t.ops, later,
+                 [&](const QOp& o) { return !is_gate(o) || (wpos[w][o.a] >= lo && wpos[w][o.a] < hi); }, staken,
                  srest);
         const size_t g = gate_count(staken, t.ops);
         if (bt.empty() || g > bg || (g == bg && staken.size() > bt.size())) {
@@ -370,12 +443,14 @@ void compile_one(const Trajectory& t, const PlanKnobs& kn, Local& L) {
         DevOp d{};
         uint32_t la = loc(o.a), lb = 0;
         if (o.code == OP_CZ || o.code == OP_CPHASE) lb = loc(o.b);
-        d.hdr = o.code | (la << 2) | (lb << 9);
+        d.hdr = o.code | (la << 3) | (lb << 10);
         if (o.code == OP_GATE) {
           for (int k = 0; k < 4; ++k) {
             d.v[2 * k] = f32(o.m[k].re);
             d.v[2 * k + 1] = f32(o.m[k].im);
           }
+        } else if (o.code == OP_BGATE) {
+          d.v[0] = f32(o.m[0].re), d.v[1] = f32(o.m[0].im), d.v[2] = f32(o.m[1].re);
         } else if (o.code == OP_DIAG) {
           d.v[0] = f32(o.m[0].re), d.v[1] = f32(o.m[0].im), d.v[2] = f32(o.m[1].re), d.v[3] = f32(o.m[1].im);
         } else if (o.code == OP_CPHASE) {
@@ -542,13 +617,23 @@ EmuResult emulate(const Program& P, uint32_t ti) {
           };
           for (uint32_t oi = 0; oi < nops; ++oi) {
             const DevOp& d = P.op[sg.op0 + oi];
-            const uint32_t code = d.hdr & 3u, la = (d.hdr >> 2) & 127u, lb = (d.hdr >> 9) & 127u;
+            const uint32_t code = d.hdr & 7u, la = (d.hdr >> 3) & 127u, lb = (d.hdr >> 10) & 127u;
             if (code == OP_CZ) {
               neg ^= loc_mask(la, fixed, k) & loc_mask(lb, fixed, k);
               continue;
             }
             flush();
-            if (code == OP_GATE) {
+            if (code == OP_BGATE) {
+              const uint32_t kb = la & 31u;
+              const Cd w{d.v[0], d.v[1]};
+              const double sc = d.v[2];
+              for (uint32_t j = 0; j < 32; ++j) {
+                if ((j >> kb) & 1u) continue;
+                const Cd x = a[j], y = cmul(w, a[j | (1u << kb)]);
+                a[j] = Cd{sc * x.re + y.re, sc * x.im + y.im};
+                a[j | (1u << kb)] = Cd{sc * x.re - y.re, sc * x.im - y.im};
+              }
+            } else if (code == OP_GATE) {
               const uint32_t kb = la & 31u;
               const Cd u00{d.v[0], d.v[1]}, u01{d.v[2], d.v[3]}, u10{d.v[4], d.v[5]}, u11{d.v[6], d.v[7]};
               for (uint32_t j = 0; j < 32; ++j) {

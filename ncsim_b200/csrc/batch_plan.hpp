@@ -7,11 +7,15 @@
 // measurements M 0, M 1, ..., M m-1 (a draw only when the outcome is
 // uncertain, src/state/mod.rs:113-131).
 //
-// The host folds the circuit, per qubit, into general 2x2 gates and two-qubit
+// The host folds the circuit, per qubit, into 2x2 gates and two-qubit
 // diagonals: noise is sampled in circuit order (its draws do not depend on the
 // state), one-qubit diagonals and sampled Paulis are multiplied into the next
 // non-diagonal one-qubit gate on the qubit, and the m measurement uniforms that
-// follow the noise draws in the stream are drawn ahead for the device.  The
+// follow the noise draws in the stream are drawn ahead for the device.  A
+// gate whose entries all have modulus 1/sqrt2 (H or SQRT_X times phases and
+// Paulis) is split into diag(l0, l1) s [[1, w], [1, -w]]: the device applies
+// the second factor (a complex multiply and four FMAs per pair instead of
+// sixteen FMAs) and the diagonal joins the qubit's next gate.  The
 // folded ops are grouped into passes over a 13-qubit window (a tile of 8192
 // amplitudes in shared memory) and, inside a pass, into stages: each stage
 // holds 32 amplitudes per thread in registers, over five consecutive tile
@@ -33,18 +37,20 @@ constexpr uint32_t THREADS = 256;
 constexpr uint32_t MIN_QUBITS = TILE_BITS;
 constexpr uint32_t MAX_QUBITS = 26;         // 2^(n-13) <= 8192 high amplitudes per measurement gather
 constexpr uint32_t MAX_NON = MAX_QUBITS - TILE_BITS;
+constexpr uint32_t MAX_PASS_OPS = 256;      // a pass's ops and stages fit the kernel's shared copy
 constexpr uint32_t NSEL = 3;                // stage register-bit sets: tile bits [RSHIFT, RSHIFT+5)
 constexpr uint32_t RSHIFT[NSEL] = {0, 5, 8};
 
 // op codes and qubit locators of the device program
-enum : uint32_t { OP_GATE = 0, OP_CZ = 1, OP_CPHASE = 2, OP_DIAG = 3 };
+enum : uint32_t { OP_GATE = 0, OP_CZ = 1, OP_CPHASE = 2, OP_DIAG = 3, OP_BGATE = 4 };
 enum : uint32_t { LOC_REG = 0, LOC_FIXED = 1, LOC_TILE = 2 };
 enum : uint32_t { PASS_ZERO_INIT = 1, PASS_ACCUM = 2, PASS_NO_WRITE = 4 };
 
-// One op of a stage.  hdr = code | locA << 2 | locB << 9 with loc = type << 5 | index:
+// One op of a stage.  hdr = code | locA << 3 | locB << 10 with loc = type << 5 | index:
 // LOC_REG index = register bit (0..4), LOC_FIXED = bit of the thread's tile
 // index, LOC_TILE = bit of the tile number.  v: GATE 2x2 row-major
-// (re, im); DIAG (d0, d1); CPHASE the phase applied where both bits are 1.
+// (re, im); BGATE (s w, s) for s [[1, w], [1, -w]], s = 1/sqrt2, |w| = 1;
+// DIAG (d0, d1); CPHASE the phase applied where both bits are 1.
 struct alignas(16) DevOp {
   float v[8];
   uint32_t hdr;
