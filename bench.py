@@ -1,10 +1,15 @@
-"""Benchmark of the B200 statevector engine on the random-circuit workload at n = 32.
+"""Benchmark of the B200 statevector engine: gates/s on the random-circuit
+workload at n = 32, and trajectories/s of the batching form.
 
 One step = one run of the seeded random layer circuit (n qubits, depth 20:
 per layer one of H/S/T/SQRT_X/RZ on every qubit, then CZ on a random perfect
 matching; n + n/2 gates per layer) on the device state.  The register is 32
 qubits: 64 GiB in complex128 (plain path) or 32 GiB in complex64 (fused
 precision form), far larger than L2, so no flush is needed between steps.
+
+The trajectories/s part: one step = one run of 4096 noisy trajectories of
+13..26-qubit registers (n = 16 + gen_range(0..7), depth 30, DEPOLARIZE2(1e-3)
+after every CZ, M on every qubit) in the batching form's persistent kernel.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
 
@@ -240,8 +245,127 @@ def run_reference(args):
                          "sample": sample["sample"]},
         "e2e": {"value": v, "unit": "gates/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
+    if not args.no_trajectories:
+        tr = cpu_trajectories(30, 1e-3, args.cpu_budget * 2 / 3)
+        line["trajectories"] = {"metric": "trajectories/s", "value": tr["value"], "unit": "trajectories/s",
+                                "cpu_baseline": tr,
+                                "e2e": {"value": tr["value"], "unit": "trajectories/s",
+                                        "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
     return 0
+
+
+def cpu_trajectories(depth: int, p: float, budget_s: float = 10.0):
+    """The oracle's noisy trajectories (FP64, the reference's StateVector
+    semantics, all host threads) on the host cores: seeds 1, 2, ... until
+    about budget_s seconds have passed."""
+    from oracle import oracle as O
+
+    t0 = time.perf_counter()
+    done = 0
+    while time.perf_counter() - t0 < budget_s:
+        O.trajectory(1 + done, 16, 7, depth, p)
+        done += 1
+    dt = time.perf_counter() - t0
+    return {"value": done / dt, "unit": "trajectories/s", "cores": O.lib().oracle_num_threads(), "kind": "port",
+            "sample": f"oracle trajectories seeds 1..{done} (n = 16 + gen_range(0..7), depth {depth}, "
+                      f"DEPOLARIZE2({p}), M on every qubit) in {dt:.1f} s"}
+
+
+def trajectory_bench(nb, args, dist, peak, peak_kind):
+    """The batching form: `count` noisy trajectories (trajectory t draws from
+    StdRng(seed0 + t): n = 16 + gen_range(0..7), the random layer circuit of
+    depth 30 with DEPOLARIZE2(1e-3) after every CZ, M on every qubit) in one
+    persistent kernel.  A step is one run of the whole batch (one CUDA graph
+    launch); states start at |0...0> in the kernel, the programs are resident."""
+    count, depth, p = args.traj_count, 30, 1e-3
+    seed0 = 1 + RANK * count
+    t0 = time.perf_counter()
+    tb = nb.TrajectoryBatch.random_layers(count, seed0, 16, 7, depth, p)
+    build_s = time.perf_counter() - t0
+    info = tb.info()
+    if args.traj_launch:
+        ctas, bufs = (int(v) for v in args.traj_launch.split(","))
+        tb.set_config(ctas_per_sm=ctas, buffers=bufs)
+    tb.run()  # tunes the launch configuration on first use (unless it was given)
+    cfg = tb.config()
+    for _ in range(args.warmup):
+        tb.run()
+    barrier(dist)
+    ms = [tb.run() for _ in range(args.steps)]
+    ms_mean = max_over_ranks(dist, statistics.mean(ms))
+    value = WORLD * count / (ms_mean / 1e3)
+    n_t, rec, z0, norm = tb.results()
+    achieved = info["state_bytes"] / (ms_mean / 1e3) / 1e9
+    out = {
+        "metric": "trajectories/s",
+        "value": value,
+        "unit": "trajectories/s",
+        "ms_per_step": ms_mean,
+        "steps": args.steps,
+        "warmup": args.warmup,
+        "dtype": "f32 amplitudes (complex64), FP64 reductions",
+        "config": {"workload": f"{count} noisy trajectories per GPU, n = 16 + gen_range(0..7), random layers "
+                               f"depth {depth}, DEPOLARIZE2({p}) after every CZ, M on every qubit; "
+                               f"StdRng(seed0 + t), seed0 = {seed0}",
+                   "count": count, "depth": depth, "p": p, "launch": cfg,
+                   "l2": "about 1 TB of state traffic per step (no flush needed)"},
+        "gpu_launches_per_step": 1,
+        "plan": {k: info[k] for k in ("source_gates", "noise_events", "folded_ops", "passes", "tile_passes",
+                                      "tile_stages", "program_bytes")},
+        "roofline": {"bound": "hbm", "kernel": "k_batch", "achieved": round(achieved, 1), "peak": peak,
+                     "unit": "GB/s", "frac": round(achieved / peak, 4), "peak_kind": peak_kind,
+                     "traffic": profiled_traffic("k_batch"),
+                     "algorithmic_bytes_per_launch": info["state_bytes"]},
+        "host_build_s": build_s,
+    }
+    # accuracy: a strided sample against FP64 plain-path runs of the same draws
+    sample = list(range(0, count, max(1, count // max(1, args.traj_check))))[: args.traj_check]
+    errs, z_b, z_r, same = [], [], [], 0
+    for t in sample:
+        rng = nb.StdRng(seed0 + t)
+        n = 16 + rng.gen_range(0, 7)
+        c = nb.Circuit.random_layers_from(rng, n, depth, p, 0, 0)
+        s = nb.GpuStateVector(n, nb.C128)
+        s.run(c, rng)
+        zr = s.expectation(nb.Pauli(n, 0, 1, 0)).real / s.norm_sq().real
+        m = nb.Circuit.parse(f"QUBITS {n}\n" + "".join(f"M {q}\n" for q in range(n)))
+        rr = s.run(m, rng)
+        same += int(rec[t]) == sum(int(v) << k for k, v in enumerate(rr))
+        errs.append(abs(z0[t] - zr))
+        z_b.append(z0[t])
+        z_r.append(zr)
+        del s
+    if sample:
+        out["accuracy"] = {
+            "reference": "plain complex128 path (FP64) on the same draws",
+            "sample": len(sample),
+            "mean_z0_error": abs(statistics.mean(z_b) - statistics.mean(z_r)),
+            "max_z0_error": max(errs),
+            "records_identical": f"{same}/{len(sample)}",
+            "mean_norm_drift": float(abs(norm - 1.0).mean()),
+        }
+    if not args.no_e2e:
+        def e2e_step():
+            b = nb.TrajectoryBatch.random_layers(count, seed0, 16, 7, depth, p)  # host generation in
+            b.set_config(ctas_per_sm=cfg["ctas_per_sm"], buffers=cfg["buffers"], order=cfg["order"])
+            b.run()  # program upload, the graph, result copies
+            return b.results()  # results out
+
+        e2e_step()
+        barrier(dist)
+        t1 = time.perf_counter()
+        e2e_steps = max(1, min(args.steps, 2))
+        for _ in range(e2e_steps):
+            e2e_step()
+        dt = max_over_ranks(dist, time.perf_counter() - t1)
+        out["e2e"] = {"value": WORLD * e2e_steps * count / dt, "unit": "trajectories/s",
+                      "h2d_bytes_per_step": info["program_bytes"], "d2h_bytes_per_step": count * 28,
+                      "note": "per step: generate and compile the trajectories on the host, upload the "
+                              "program, run, copy records, <Z0> and norms back; host wall clock"}
+    if RANK == 0 and WORLD == 1 and not args.no_cpu_baseline:
+        out["cpu_baseline"] = cpu_trajectories(depth, p, args.cpu_budget * 2 / 3)
+    return out
 
 
 def timed_runs(nb, state, circuit, steps: int, warmup: int, fused: bool, dist):
@@ -284,6 +408,13 @@ def main():
     ap.add_argument("--cpu-budget", type=float, default=15.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--traj-count", type=int, default=4096)
+    ap.add_argument("--traj-check", type=int, default=32)
+    ap.add_argument("--no-trajectories", action="store_true")
+    ap.add_argument("--traj-launch", default="",
+                    help="CTAS_PER_SM,BUFFERS: a fixed launch configuration of the batch kernel (default: tuned)")
+    ap.add_argument("--no-headline", action="store_true",
+                    help="only the trajectories/s part (for profiling the batch kernel)")
     args = ap.parse_args()
 
     if args.impl == "reference":
@@ -295,6 +426,17 @@ def main():
     dist = dist_init()
     seed = 1 + RANK
     peak, peak_kind = measured_peaks()
+
+    if args.no_headline:
+        with ClockSampler() as tclk:
+            tr = trajectory_bench(nb, args, dist, peak, peak_kind)
+        tr["clocks"] = tclk.summary()
+        if RANK == 0:
+            print(json.dumps({"metric": METRIC, "n_gpus": WORLD, "trajectories": tr}), flush=True)
+        if dist is not None:
+            dist.barrier()
+            dist.destroy_process_group()
+        return 0
 
     fused_ok = args.path in ("auto", "fused")
     if fused_ok:
@@ -404,6 +546,11 @@ def main():
     cpu = None
     if RANK == 0 and WORLD == 1 and not args.no_cpu_baseline:
         cpu = cpu_baseline(n if path == "plain" else args.n, args.depth, seed, args.cpu_budget)
+
+    if not args.no_trajectories:
+        with ClockSampler() as tclk:
+            result["trajectories"] = trajectory_bench(nb, args, dist, peak, peak_kind)
+        result["trajectories"]["clocks"] = tclk.summary()
 
     clocks = clk.summary() if clk else None
     line = {

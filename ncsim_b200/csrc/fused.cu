@@ -91,14 +91,16 @@ __device__ __forceinline__ void mbar_arrive(uint32_t bar) {
 __device__ __forceinline__ void mbar_expect_tx(uint32_t bar, uint32_t bytes) {
   asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar), "r"(bytes) : "memory");
 }
+// try_wait with a suspend-time hint: the thread sleeps (up to about 1 ms) until
+// the phase completes instead of spinning
 __device__ __forceinline__ bool mbar_try(uint32_t bar, uint32_t parity) {
   uint32_t ok;
   asm volatile(
       "{\n\t.reg .pred p;\n\t"
-      "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+      "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2, %3;\n\t"
       "selp.u32 %0, 1, 0, p;\n\t}"
       : "=r"(ok)
-      : "r"(bar), "r"(parity)
+      : "r"(bar), "r"(parity), "r"(1000000u)
       : "memory");
   return ok != 0;
 }
@@ -181,6 +183,51 @@ __device__ __forceinline__ uint64_t tile_base(uint64_t t, const PassParams& P) {
     v = ((v >> b) << (b + 1)) | (v & ((uint64_t(1) << b) - 1));
   }
   return v;
+}
+
+// The tile's phase tables of a terms op: the low- and high-half phase products
+// (threads 0-63 and 64-127) and the cross-half sign parities (128-191).
+__device__ __forceinline__ void build_tables(const OpDesc& op, uint64_t base, int tid, const PassParams& P,
+                                             float2* tab_lo, float2* tab_hi, uint8_t* tab_cross) {
+  if (tid < 64) {
+    float2 c = make_float2(1.f, 0.f);
+    for (int k = op.t0; k < op.tl; ++k) {
+      const TermDesc tm = P.terms[k];
+      if ((base & tm.cmask) == tm.cmask && (uint32_t(tid) & tm.tmask) == tm.tmask) c = cmulf(c, make_float2(tm.cr, tm.ci));
+    }
+    tab_lo[tid] = c;
+  } else if (tid < 128) {
+    const uint32_t x = uint32_t(tid - 64);
+    float2 c = make_float2(1.f, 0.f);
+    for (int k = op.tl; k < op.th; ++k) {
+      const TermDesc tm = P.terms[k];
+      const uint32_t hm = tm.tmask >> HALF;
+      if ((base & tm.cmask) == tm.cmask && (x & hm) == hm) c = cmulf(c, make_float2(tm.cr, tm.ci));
+    }
+    tab_hi[x] = c;
+  } else if (tid < 192) {
+    const uint32_t x = uint32_t(tid - 128);
+    uint32_t v = 0;
+    for (int k = op.th; k < op.tc; ++k) {
+      const TermDesc tm = P.terms[k];
+      if ((base & tm.cmask) != tm.cmask) continue;
+      if (x & (tm.tmask >> HALF)) v ^= tm.tmask & ((1u << HALF) - 1);
+    }
+    tab_cross[x] = uint8_t(v);
+  }
+}
+
+// the phase of tile element e under a terms op (its tables built)
+__device__ __forceinline__ float2 term_phase(uint32_t e, const OpDesc& op, uint64_t base, const PassParams& P,
+                                             const float2* tab_lo, const float2* tab_hi, const uint8_t* tab_cross) {
+  const uint32_t lo = e & ((1u << HALF) - 1), hi = e >> HALF;
+  float2 c = cmulf(tab_lo[lo], tab_hi[hi]);
+  if (__popc(lo & tab_cross[hi]) & 1) c = make_float2(-c.x, -c.y);
+  for (int k = op.tc; k < op.t1; ++k) {
+    const TermDesc tm = P.terms[k];
+    if ((base & tm.cmask) == tm.cmask && (e & tm.tmask) == tm.tmask) c = cmulf(c, make_float2(tm.cr, tm.ci));
+  }
+  return c;
 }
 
 __global__ void __launch_bounds__(THREADS, 1) k_fused_pass(const __grid_constant__ PassParams P) {
@@ -303,7 +350,8 @@ __global__ void __launch_bounds__(THREADS, 1) k_fused_pass(const __grid_constant
     uint32_t mma_phase = 0;
     for (uint64_t it = 0; it < my_tiles; ++it) {
       const int b = int(it & 1);
-      if (!mbar_wait(bar_full(b), uint32_t((it >> 1) & 1))) fail(1);
+      // one thread waits for the tile; the others block at the named barrier
+      if (tid == 0 && !mbar_wait(bar_full(b), uint32_t((it >> 1) & 1))) fail(1);
       bar_compute();
       if (abort_sh) break;
       const uint64_t t = uint64_t(blockIdx.x) + it * gridDim.x;
@@ -313,45 +361,12 @@ __global__ void __launch_bounds__(THREADS, 1) k_fused_pass(const __grid_constant
         const OpDesc op = P.ops[oi];
         if (op.kind == 1) {
           // ---- diagonal terms: per-tile tables, then one sweep of the tile ----
-          if (tid < 64) {
-            float2 c = make_float2(1.f, 0.f);
-            for (int k = op.t0; k < op.tl; ++k) {
-              const TermDesc tm = P.terms[k];
-              if ((base & tm.cmask) == tm.cmask && (uint32_t(tid) & tm.tmask) == tm.tmask)
-                c = cmulf(c, make_float2(tm.cr, tm.ci));
-            }
-            tab_lo[tid] = c;
-          } else if (tid < 128) {
-            const uint32_t x = uint32_t(tid - 64);
-            float2 c = make_float2(1.f, 0.f);
-            for (int k = op.tl; k < op.th; ++k) {
-              const TermDesc tm = P.terms[k];
-              const uint32_t hm = tm.tmask >> HALF;
-              if ((base & tm.cmask) == tm.cmask && (x & hm) == hm) c = cmulf(c, make_float2(tm.cr, tm.ci));
-            }
-            tab_hi[x] = c;
-          } else if (tid < 192) {
-            const uint32_t x = uint32_t(tid - 128);
-            uint32_t v = 0;
-            for (int k = op.th; k < op.tc; ++k) {
-              const TermDesc tm = P.terms[k];
-              if ((base & tm.cmask) != tm.cmask) continue;
-              if (x & (tm.tmask >> HALF)) v ^= tm.tmask & ((1u << HALF) - 1);
-            }
-            tab_cross[x] = uint8_t(v);
-          }
+          build_tables(op, base, tid, P, tab_lo, tab_hi, tab_cross);
           bar_compute();
 #pragma unroll 4
           for (int i = 0; i < TILE / COMPUTE_THREADS; ++i) {
             const uint32_t e = uint32_t(tid + COMPUTE_THREADS * i);
-            const uint32_t lo = e & ((1u << HALF) - 1), hi = e >> HALF;
-            float2 c = cmulf(tab_lo[lo], tab_hi[hi]);
-            if (__popc(lo & tab_cross[hi]) & 1) c = make_float2(-c.x, -c.y);
-            for (int k = op.tc; k < op.t1; ++k) {
-              const TermDesc tm = P.terms[k];
-              if ((base & tm.cmask) == tm.cmask && (e & tm.tmask) == tm.tmask) c = cmulf(c, make_float2(tm.cr, tm.ci));
-            }
-            T[e] = cmulf(c, T[e]);
+            T[e] = cmulf(term_phase(e, op, base, P, tab_lo, tab_hi, tab_cross), T[e]);
           }
           bar_compute();
           continue;
@@ -403,8 +418,9 @@ __global__ void __launch_bounds__(THREADS, 1) k_fused_pass(const __grid_constant
           for (int s = 0; s < 4; ++s) mma_bf16(tmem, dah + 2 * s, dbl + 2 * s, idesc, 1);
           mma_commit(bar_mma);
         }
-        if (!mbar_wait(bar_mma, mma_phase)) fail(2);
+        if (tid == 0 && !mbar_wait(bar_mma, mma_phase)) fail(2);
         mma_phase ^= 1u;
+        bar_compute();
         tc_fence_after();
         uint32_t re[16], im[16];
         NCSIM_TMEM_LD16(taddr, re);
