@@ -2,25 +2,27 @@
 //
 // A persistent CTA per SM streams tiles of 2^12 complex64 amplitudes (32 KB)
 // through shared memory with the bulk-copy engine (cp.async.bulk, runs of
-// >= 128 contiguous bytes, double-buffered: tile i+1 loads and tile i-1
-// stores while tile i computes).  Eight warps run the pass's program on each
-// tile:
+// >= 128 contiguous bytes, three rotating tile buffers; warp 8).  The CTA
+// takes its tiles in pairs, and two warpgroups run the pass's program, one on
+// each tile of a pair, so that one group splits amplitudes while the other's
+// MMAs and read-back run.  The unitaries' B operands (16 KB each) stream from
+// L2 into three rotating slots (warp 9); both groups' tcgen05.commit free a
+// slot.  Per group and tile:
 //   unitary op: the tile as 32 rows (the unitary's 5 qubits) x 128 columns;
-//     two threads share a column (16 rows each), split its amplitudes into
-//     bf16 hi/lo and write them K-major, 128-byte swizzled (A = X^T,
-//     128 x 64 per half); one thread issues 12 tcgen05.mma (M=128, N=64,
-//     K=16, bf16 in, f32 accumulate in TMEM):
+//     each thread owns a column, splits its 32 amplitudes into bf16 hi/lo
+//     and writes them K-major, 128-byte swizzled (A = X^T, 128 x 64); one
+//     thread issues 12 tcgen05.mma (M=128, N=64, K=16, bf16 in, f32
+//     accumulate in the group's 64 TMEM columns):
 //       D = Xhi.Rhi + Xlo.Rhi + Xhi.Rlo
 //     with R the real form [[Ur, -Ui], [Ui, Ur]] of the fused unitary (bf16
-//     hi/lo images made on the host); each thread reads its half of its D row
-//     back (tcgen05.ld) and writes the 16 new amplitudes into the tile;
+//     hi/lo images made on the host); each thread reads its D row back
+//     (tcgen05.ld) and writes the 32 new amplitudes into the tile;
 //   diagonal op: the tile index splits into two 6-bit halves; per tile, the
 //     active terms are folded into a 64-entry phase table per half and a
 //     parity table for the cross-half sign terms (CZ-like), so an amplitude
 //     costs two table reads and a parity, whatever the number of terms.
-// A ninth warp issues the bulk copies.  Every wait on an mbarrier is bounded
-// in time: on timeout the CTA records an error code, stops, waits for its own
-// copies and frees its TMEM.
+// Every wait on an mbarrier is bounded in time: on timeout the CTA records an
+// error code, stops, waits for its own copies and frees its TMEM.
 #include <cuda_bf16.h>
 
 #include "engine.cuh"
@@ -34,19 +36,25 @@ namespace fused {
 
 namespace {
 
-constexpr int COMPUTE_THREADS = 256;           // warps 0-7: tensor-core program
-constexpr int THREADS = COMPUTE_THREADS + 32;  // warp 8: bulk copies
+constexpr int GROUP_THREADS = 128;                       // one warpgroup runs the program on one tile
+constexpr int GROUPS = 2;                                // two tiles in flight per CTA
+constexpr int COMPUTE_THREADS = GROUPS * GROUP_THREADS;  // warps 0-7
+constexpr int WARP_TILES = COMPUTE_THREADS / 32;         // warps 8-9: tile loads and stores
+constexpr int TILE_THREADS = 64;
+constexpr int WARP_OPS = WARP_TILES + 2;                 // warp 10: B operand images
+constexpr int THREADS = COMPUTE_THREADS + TILE_THREADS + 32;
 constexpr int TILE = 1 << TILE_BITS;
 constexpr uint32_t TILE_BYTES = uint32_t(TILE) * 8u;
-constexpr int OPERAND_BYTES = 16384;
-constexpr int A_BYTES = 16384;
-constexpr int SM_ROPS = 0;
-constexpr int SM_AHI = SM_ROPS + MAX_UNITARIES * OPERAND_BYTES;
-constexpr int SM_ALO = SM_AHI + A_BYTES;
-constexpr int SM_TILE0 = SM_ALO + A_BYTES;
-constexpr int SM_TOTAL = SM_TILE0 + 2 * int(TILE_BYTES);
+constexpr int OPERAND_BYTES = 16384;  // B: bf16 hi (8 KB) + lo (8 KB)
+constexpr int A_BYTES = 16384;        // A: 128 x 64 bf16, hi and lo separately
+constexpr int NTILEBUF = 3;           // tile buffers rotating over the CTA's tiles
+constexpr int NOPSLOT = 3;            // B operand slots rotating over the unitary uses
+constexpr int SM_A = 0;                                      // per group: A hi, A lo
+constexpr int SM_B = SM_A + GROUPS * 2 * A_BYTES;
+constexpr int SM_TILE0 = SM_B + NOPSLOT * OPERAND_BYTES;
+constexpr int SM_TOTAL = SM_TILE0 + NTILEBUF * int(TILE_BYTES);
 constexpr int SM_DYNAMIC = SM_TOTAL + 1008;  // the dynamic base is 16-byte aligned: slack to reach 1024
-constexpr uint32_t TMEM_COLS = 64;
+constexpr uint32_t TMEM_COLS = 128;          // 64 accumulator columns per group
 constexpr long long WAIT_CYCLES = 4000000000ll;  // about 2 s at 1.9 GHz
 constexpr int HALF = TILE_BITS / 2;              // 6-bit halves of the tile index
 
@@ -118,14 +126,29 @@ __device__ __forceinline__ void bulk_load(uint32_t dst, const void* src, uint32_
                "l"(src), "r"(bytes), "r"(bar)
                : "memory");
 }
-__device__ __forceinline__ void bulk_store(void* dst, uint32_t src, uint32_t bytes) {
-  asm volatile("cp.async.bulk.global.shared::cta.bulk_group [%0], [%1], %2;" ::"l"(dst), "r"(src), "r"(bytes) : "memory");
-}
-__device__ __forceinline__ void bulk_commit() { asm volatile("cp.async.bulk.commit_group;" ::: "memory"); }
-__device__ __forceinline__ void bulk_wait_read_all() { asm volatile("cp.async.bulk.wait_group.read 0;" ::: "memory"); }
-__device__ __forceinline__ void bulk_wait_all() { asm volatile("cp.async.bulk.wait_group 0;" ::: "memory"); }
 __device__ __forceinline__ void fence_async_smem() { asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); }
-__device__ __forceinline__ void bar_compute() { asm volatile("bar.sync 1, 256;" ::: "memory"); }
+__device__ __forceinline__ void cp_async16(uint32_t dst, const void* src) {
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(dst), "l"(src) : "memory");
+}
+// arrives on the mbarrier once this thread's earlier cp.async copies have landed
+__device__ __forceinline__ void cp_async_arrive(uint32_t bar) {
+  asm volatile("cp.async.mbarrier.arrive.noinc.shared::cta.b64 [%0];" ::"r"(bar) : "memory");
+}
+__device__ __forceinline__ void bar_tiles() { asm volatile("bar.sync 3, %0;" ::"n"(TILE_THREADS) : "memory"); }
+// A named barrier that also ORs a flag over its threads: every thread gets the
+// same answer, so a stop decided from it is uniform across the barrier's threads.
+__device__ __forceinline__ bool bar_any(int id, int count, bool v) {
+  uint32_t r;
+  asm volatile(
+      "{\n\t.reg .pred p, q;\n\t"
+      "setp.ne.u32 p, %1, 0;\n\t"
+      "bar.red.or.pred q, %2, %3, p;\n\t"
+      "selp.u32 %0, 1, 0, q;\n\t}"
+      : "=r"(r)
+      : "r"(uint32_t(v)), "r"(id), "r"(count)
+      : "memory");
+  return r != 0;
+}
 
 __device__ __forceinline__ void tc_fence_before() { asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory"); }
 __device__ __forceinline__ void tc_fence_after() { asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory"); }
@@ -185,76 +208,88 @@ __device__ __forceinline__ uint64_t tile_base(uint64_t t, const PassParams& P) {
   return v;
 }
 
-// The tile's phase tables of a terms op: the low- and high-half phase products
-// (threads 0-63 and 64-127) and the cross-half sign parities (128-191).
-__device__ __forceinline__ void build_tables(const OpDesc& op, uint64_t base, int tid, const PassParams& P,
+// The tile's phase tables of a terms op, built by one group's 128 threads: the
+// low-half phase products and cross-half sign parities (threads 0-63) and the
+// high-half phase products (64-127).
+__device__ __forceinline__ void build_tables(const OpDesc& op, uint64_t base, int tg, const TermDesc* terms,
                                              float2* tab_lo, float2* tab_hi, uint8_t* tab_cross) {
-  if (tid < 64) {
+  if (tg < 64) {
+    const uint32_t x = uint32_t(tg);
     float2 c = make_float2(1.f, 0.f);
     for (int k = op.t0; k < op.tl; ++k) {
-      const TermDesc tm = P.terms[k];
-      if ((base & tm.cmask) == tm.cmask && (uint32_t(tid) & tm.tmask) == tm.tmask) c = cmulf(c, make_float2(tm.cr, tm.ci));
+      const TermDesc tm = terms[k];
+      if ((base & tm.cmask) == tm.cmask && (x & tm.tmask) == tm.tmask) c = cmulf(c, make_float2(tm.cr, tm.ci));
     }
-    tab_lo[tid] = c;
-  } else if (tid < 128) {
-    const uint32_t x = uint32_t(tid - 64);
-    float2 c = make_float2(1.f, 0.f);
-    for (int k = op.tl; k < op.th; ++k) {
-      const TermDesc tm = P.terms[k];
-      const uint32_t hm = tm.tmask >> HALF;
-      if ((base & tm.cmask) == tm.cmask && (x & hm) == hm) c = cmulf(c, make_float2(tm.cr, tm.ci));
-    }
-    tab_hi[x] = c;
-  } else if (tid < 192) {
-    const uint32_t x = uint32_t(tid - 128);
+    tab_lo[x] = c;
     uint32_t v = 0;
     for (int k = op.th; k < op.tc; ++k) {
-      const TermDesc tm = P.terms[k];
+      const TermDesc tm = terms[k];
       if ((base & tm.cmask) != tm.cmask) continue;
       if (x & (tm.tmask >> HALF)) v ^= tm.tmask & ((1u << HALF) - 1);
     }
     tab_cross[x] = uint8_t(v);
+  } else {
+    const uint32_t x = uint32_t(tg - 64);
+    float2 c = make_float2(1.f, 0.f);
+    for (int k = op.tl; k < op.th; ++k) {
+      const TermDesc tm = terms[k];
+      const uint32_t hm = tm.tmask >> HALF;
+      if ((base & tm.cmask) == tm.cmask && (x & hm) == hm) c = cmulf(c, make_float2(tm.cr, tm.ci));
+    }
+    tab_hi[x] = c;
   }
 }
 
 // the phase of tile element e under a terms op (its tables built)
-__device__ __forceinline__ float2 term_phase(uint32_t e, const OpDesc& op, uint64_t base, const PassParams& P,
+__device__ __forceinline__ float2 term_phase(uint32_t e, const OpDesc& op, uint64_t base, const TermDesc* terms,
                                              const float2* tab_lo, const float2* tab_hi, const uint8_t* tab_cross) {
   const uint32_t lo = e & ((1u << HALF) - 1), hi = e >> HALF;
   float2 c = cmulf(tab_lo[lo], tab_hi[hi]);
   if (__popc(lo & tab_cross[hi]) & 1) c = make_float2(-c.x, -c.y);
   for (int k = op.tc; k < op.t1; ++k) {
-    const TermDesc tm = P.terms[k];
+    const TermDesc tm = terms[k];
     if ((base & tm.cmask) == tm.cmask && (e & tm.tmask) == tm.tmask) c = cmulf(c, make_float2(tm.cr, tm.ci));
   }
   return c;
 }
 
+__device__ __forceinline__ void bar_group(int g) {
+  asm volatile("bar.sync %0, %1;" ::"r"(1 + g), "r"(GROUP_THREADS) : "memory");
+}
+
 __global__ void __launch_bounds__(THREADS, 1) k_fused_pass(const __grid_constant__ PassParams P) {
   extern __shared__ uint8_t smem_raw[];
   uint8_t* smem = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
-  __shared__ __align__(8) uint64_t bars[5];  // full[2], done[2], mma
+  // mbarriers: tile full[3], tile done[3], operand full[3], operand empty[3], mma[2]
+  __shared__ __align__(8) uint64_t bars[4 * 3 + GROUPS];
   __shared__ uint32_t tmem_base_sh;
   __shared__ volatile int abort_sh;
   __shared__ uint8_t nongate[MAX_UNITARIES][TILE_BITS - GROUP_QUBITS];
-  __shared__ float2 tab_lo[1 << HALF], tab_hi[1 << HALF];
-  __shared__ uint8_t tab_cross[1 << HALF];
+  __shared__ float2 tab_lo[GROUPS][1 << HALF], tab_hi[GROUPS][1 << HALF];
+  __shared__ uint8_t tab_cross[GROUPS][1 << HALF];
+  __shared__ uint64_t run_off[TILE >> LOW_BITS];  // index bits of run r of a tile (the window bits above wl)
+  __shared__ TermDesc s_terms[MAX_TERMS];         // the pass's program, read with runtime indices
+  __shared__ OpDesc s_ops[MAX_OPS];
 
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
-  const uint32_t bar_full0 = smem_u32(&bars[0]), bar_done0 = smem_u32(&bars[2]), bar_mma = smem_u32(&bars[4]);
-  auto bar_full = [&](int b) { return bar_full0 + 8u * uint32_t(b); };
-  auto bar_done = [&](int b) { return bar_done0 + 8u * uint32_t(b); };
+  auto bar_tfull = [&](int b) { return smem_u32(&bars[b]); };
+  auto bar_tdone = [&](int b) { return smem_u32(&bars[3 + b]); };
+  auto bar_ofull = [&](int s) { return smem_u32(&bars[6 + s]); };
+  auto bar_oempty = [&](int s) { return smem_u32(&bars[9 + s]); };
+  auto bar_mma = [&](int g) { return smem_u32(&bars[12 + g]); };
   auto fail = [&](int code) {
     abort_sh = 1;
     atomicCAS(P.err, 0, code);
   };
 
   if (tid == 0) {
-    mbar_init(bar_full(0), 1);
-    mbar_init(bar_full(1), 1);
-    mbar_init(bar_done(0), COMPUTE_THREADS);
-    mbar_init(bar_done(1), COMPUTE_THREADS);
-    mbar_init(bar_mma, 1);
+    for (int i = 0; i < 3; ++i) {
+      mbar_init(bar_tfull(i), TILE_THREADS);  // one cp.async arrival per tile thread
+      mbar_init(bar_tdone(i), GROUP_THREADS);
+      mbar_init(bar_ofull(i), 1);
+      mbar_init(bar_oempty(i), GROUPS);  // one commit per group
+    }
+    for (int g = 0; g < GROUPS; ++g) mbar_init(bar_mma(g), 1);
     abort_sh = 0;
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
   }
@@ -263,131 +298,164 @@ __global__ void __launch_bounds__(THREADS, 1) k_fused_pass(const __grid_constant
                  "r"(TMEM_COLS));
     asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
   }
-  // operand images and the per-unitary column bits
+  for (uint32_t r = uint32_t(tid); r < (uint32_t(TILE) >> P.wl); r += THREADS) run_off[r] = global_index(0, r << P.wl, P);
+  for (int i = tid; i < P.nops; i += THREADS) s_ops[i] = P.ops[i];
   {
-    uint4* dst = reinterpret_cast<uint4*>(smem + SM_ROPS);
-    const int n16 = P.nu * (OPERAND_BYTES / 16);
-    for (int i = tid; i < n16; i += THREADS) dst[i] = P.rops[i];
-    for (int u = tid; u < P.nu; u += THREADS) {
-      uint32_t gm = 0;
-      for (int j = 0; j < GROUP_QUBITS; ++j) gm |= 1u << P.pos[u][j];
-      int m = 0;
-      for (int b = 0; b < TILE_BITS; ++b)
-        if (!((gm >> b) & 1)) nongate[u][m++] = uint8_t(b);
-    }
+    int nterms = 0;
+    for (int i = 0; i < P.nops; ++i) nterms = max(nterms, int(P.ops[i].t1));
+    for (int i = tid; i < nterms; i += THREADS) s_terms[i] = P.terms[i];
   }
-  fence_async_smem();
+  for (int u = tid; u < P.nu; u += THREADS) {  // the non-gate tile bits of each unitary
+    uint32_t gm = 0;
+    for (int j = 0; j < GROUP_QUBITS; ++j) gm |= 1u << P.pos[u][j];
+    int m = 0;
+    for (int b = 0; b < TILE_BITS; ++b)
+      if (!((gm >> b) & 1)) nongate[u][m++] = uint8_t(b);
+  }
   tc_fence_before();
   __syncthreads();
   tc_fence_after();
   const uint32_t tmem = tmem_base_sh;
-  const uint64_t my_tiles = P.ntiles > blockIdx.x ? (P.ntiles - 1 - blockIdx.x) / gridDim.x + 1 : 0;
+  // tiles go in pairs, one per group: this CTA's it-th tile is tile_of(it), in buffer it % 3
+  const uint64_t npairs = (P.ntiles + 1) / 2;
+  const uint64_t my_pairs = npairs > blockIdx.x ? (npairs - 1 - blockIdx.x) / gridDim.x + 1 : 0;
+  const uint64_t my_tiles = 2 * my_pairs;
+  auto tile_of = [&](uint64_t it) { return 2 * (uint64_t(blockIdx.x) + (it >> 1) * gridDim.x) + (it & 1); };
+  // only a one-tile register leaves a pair half empty, always in the CTA's last pair
+  auto have = [&](uint64_t it) { return tile_of(it) < P.ntiles; };
   float2* tiles = reinterpret_cast<float2*>(smem + SM_TILE0);
 
-  if (warp == COMPUTE_THREADS / 32) {
-    // ---------------- bulk-copy producer ----------------
-    const uint32_t run_bytes = (1u << P.wl) * 8u, nruns = uint32_t(TILE) >> P.wl;
-    auto copy_tile = [&](uint64_t it, int b, bool load) {
-      const uint64_t t = uint64_t(blockIdx.x) + it * gridDim.x;
-      const uint64_t base = tile_base(t, P);
-      float2* buf = tiles + size_t(b) * TILE;
-      for (uint32_t r = lane; r < nruns; r += 32) {
-        const uint32_t e = r << P.wl;
-        float2* g = P.amp + global_index(base, e, P);
-        if (load) bulk_load(smem_u32(buf + e), g, run_bytes, bar_full(b));
-        else bulk_store(g, smem_u32(buf + e), run_bytes);
-      }
+  if (warp == WARP_TILES || warp == WARP_TILES + 1) {
+    // ---------------- tile loads (cp.async) and stores: 64 threads, 16-byte chunks ----------------
+    const int pt = tid - COMPUTE_THREADS;
+    const uint32_t cshift = uint32_t(P.wl) - 1u;  // chunks of 2 amplitudes per run: 2^(wl-1)
+    auto chunk_addr = [&](uint64_t base, uint32_t c) {
+      return P.amp + (base | run_off[c >> cshift]) + 2u * (c & ((1u << cshift) - 1u));
+    };
+    auto store_tile = [&](uint64_t j) {  // smem reads are synchronous: the buffer is free afterwards
+      const uint64_t base = tile_base(tile_of(j), P);
+      const float4* buf = reinterpret_cast<const float4*>(tiles + size_t(j % NTILEBUF) * TILE);
+#pragma unroll 4
+      for (uint32_t c = uint32_t(pt); c < uint32_t(TILE) / 2; c += TILE_THREADS)
+        *reinterpret_cast<float4*>(chunk_addr(base, c)) = buf[c];
+    };
+    auto load_tile = [&](uint64_t it) {
+      const int b = int(it % NTILEBUF);
+      const uint64_t base = tile_base(tile_of(it), P);
+      const uint32_t dst = smem_u32(tiles + size_t(b) * TILE);
+#pragma unroll 4
+      for (uint32_t c = uint32_t(pt); c < uint32_t(TILE) / 2; c += TILE_THREADS) cp_async16(dst + 16u * c, chunk_addr(base, c));
+      cp_async_arrive(bar_tfull(b));
+    };
+    // wait (one thread) until the group is done with tile j; false (for all 64 threads alike) to stop
+    auto wait_done = [&](uint64_t j) -> bool {
+      if (pt == 0 && have(j) && !mbar_wait(bar_tdone(int(j % NTILEBUF)), uint32_t((j / NTILEBUF) & 1))) fail(3);
+      return !bar_any(3, TILE_THREADS, abort_sh);
     };
     uint64_t it = 0;
     for (; it < my_tiles; ++it) {
-      const int b = int(it & 1);
-      if (it >= 2) {
-        bool ok = true;
-        if (lane == 0) ok = mbar_wait(bar_done(b), uint32_t(((it - 2) >> 1) & 1));
-        ok = __shfl_sync(0xffffffffu, ok, 0);
-        if (!ok || abort_sh) {
-          if (lane == 0 && !ok) fail(3);
-          break;
-        }
-        copy_tile(it - 2, b, false);
-        bulk_commit();
-        bulk_wait_read_all();
-        __syncwarp();
+      if (it >= NTILEBUF) {
+        if (!wait_done(it - NTILEBUF)) break;
+        if (have(it - NTILEBUF)) store_tile(it - NTILEBUF);
+        bar_tiles();  // every thread has read the buffer before anyone refills it
       }
-      if (lane == 0) mbar_expect_tx(bar_full(b), TILE_BYTES);
+      if (have(it)) load_tile(it);
+    }
+    if (it == my_tiles) {
+      for (uint64_t j = my_tiles >= NTILEBUF ? my_tiles - NTILEBUF : 0; j < my_tiles; ++j) {
+        if (!wait_done(j)) break;
+        if (have(j)) store_tile(j);
+      }
+    }
+    // copies of this thread still in flight land before the CTA exits
+    asm volatile("cp.async.wait_all;" ::: "memory");
+  } else if (warp == WARP_OPS) {
+    // ---------------- B operand images: use k = pair * nu + u, slot k % 3 ----------------
+    const uint64_t nk = my_pairs * uint64_t(P.nu);
+    uint64_t k = 0;
+    for (; k < nk; ++k) {
+      const int sl = int(k % NOPSLOT);
+      if (k >= NOPSLOT) {
+        bool go = true;
+        if (lane == 0) {
+          go = mbar_wait(bar_oempty(sl), uint32_t(((k - NOPSLOT) / NOPSLOT) & 1));
+          if (!go) fail(4);
+          go = go && !abort_sh;
+        }
+        if (!__shfl_sync(0xffffffffu, go, 0)) break;  // lane 0 decides for the warp
+      }
+      if (lane == 0) {
+        mbar_expect_tx(bar_ofull(sl), OPERAND_BYTES);
+        bulk_load(smem_u32(smem + SM_B + sl * OPERAND_BYTES), P.rops + (k % uint64_t(P.nu)) * (OPERAND_BYTES / 16),
+                  OPERAND_BYTES, bar_ofull(sl));
+      }
       __syncwarp();
-      copy_tile(it, b, true);
     }
-    if (!abort_sh) {
-      // the last (up to two) tiles
-      for (uint64_t j = my_tiles >= 2 ? my_tiles - 2 : 0; j < my_tiles; ++j) {
-        const int b = int(j & 1);
-        bool ok = true;
-        if (lane == 0) ok = mbar_wait(bar_done(b), uint32_t((j >> 1) & 1));
-        ok = __shfl_sync(0xffffffffu, ok, 0);
-        if (!ok) {
-          if (lane == 0) fail(3);
-          break;
-        }
-        copy_tile(j, b, false);
-        bulk_commit();
-      }
-    } else if (it > 0) {
-      // an abort: let the loads already issued land before the CTA exits
-      for (uint64_t j = it >= 2 ? it - 2 : 0; j < it; ++j)
-        if (lane == 0) mbar_wait(bar_full(int(j & 1)), uint32_t((j >> 1) & 1));
-    }
-    bulk_wait_all();
+    if (k < nk)  // an abort: let the loads already issued land
+      for (uint64_t j = k >= NOPSLOT ? k - NOPSLOT : 0; j < k; ++j)
+        if (lane == 0) mbar_wait(bar_ofull(int(j % NOPSLOT)), uint32_t((j / NOPSLOT) & 1));
   } else {
-    // ---------------- tensor-core program (256 threads) ----------------
+    // ---------------- tensor-core program: group g on its tile of each pair ----------------
+    const int g = warp / 4, tg = tid & (GROUP_THREADS - 1);
     const uint32_t idesc = (1u << 4) | (1u << 7) | (1u << 10) | ((64u >> 3) << 17) | ((128u >> 4) << 24);
-    const uint32_t a_hi = smem_u32(smem + SM_AHI), a_lo = smem_u32(smem + SM_ALO);
-    const int col = tid & 127, half = tid >> 7;  // A row / TMEM lane, and which 16 of the 32 rows
-    const uint32_t taddr = tmem + (uint32_t((warp & 3) * 32) << 16) + uint32_t(16 * half);
-    const uint32_t row7 = uint32_t(col) & 7u;
-    uint8_t* ahi_row = smem + SM_AHI + (col >> 3) * 1024 + row7 * 128;
-    uint8_t* alo_row = smem + SM_ALO + (col >> 3) * 1024 + row7 * 128;
+    uint8_t* a_hi_p = smem + SM_A + g * 2 * A_BYTES;
+    const uint32_t a_hi = smem_u32(a_hi_p), a_lo = a_hi + A_BYTES;
+    const uint32_t d_tmem = tmem + uint32_t(64 * g);
+    const uint32_t taddr = d_tmem + (uint32_t((warp & 3) * 32) << 16);
+    const uint32_t row7 = uint32_t(tg) & 7u;
+    uint8_t* ahi_row = a_hi_p + (tg >> 3) * 1024 + row7 * 128;
+    uint8_t* alo_row = ahi_row + A_BYTES;
     uint32_t mma_phase = 0;
-    for (uint64_t it = 0; it < my_tiles; ++it) {
-      const int b = int(it & 1);
-      // one thread waits for the tile; the others block at the named barrier
-      if (tid == 0 && !mbar_wait(bar_full(b), uint32_t((it >> 1) & 1))) fail(1);
-      bar_compute();
-      if (abort_sh) break;
-      const uint64_t t = uint64_t(blockIdx.x) + it * gridDim.x;
-      const uint64_t base = tile_base(t, P);
+    for (uint64_t p = 0; p < my_pairs; ++p) {
+      const uint64_t it = 2 * p + uint64_t(g);
+      const bool mine = have(it);
+      const int b = int(it % NTILEBUF);
+      if (mine && tg == 0 && !mbar_wait(bar_tfull(b), uint32_t((it / NTILEBUF) & 1))) fail(1);
+      if (bar_any(1 + g, GROUP_THREADS, abort_sh)) break;
+      const uint64_t base = mine ? tile_base(tile_of(it), P) : 0;
       float2* T = tiles + size_t(b) * TILE;
       for (int oi = 0; oi < P.nops; ++oi) {
-        const OpDesc op = P.ops[oi];
+        const OpDesc op = s_ops[oi];
         if (op.kind == 1) {
+          if (!mine) continue;
           // ---- diagonal terms: per-tile tables, then one sweep of the tile ----
-          build_tables(op, base, tid, P, tab_lo, tab_hi, tab_cross);
-          bar_compute();
+          build_tables(op, base, tg, s_terms, tab_lo[g], tab_hi[g], tab_cross[g]);
+          bar_group(g);
 #pragma unroll 4
-          for (int i = 0; i < TILE / COMPUTE_THREADS; ++i) {
-            const uint32_t e = uint32_t(tid + COMPUTE_THREADS * i);
-            T[e] = cmulf(term_phase(e, op, base, P, tab_lo, tab_hi, tab_cross), T[e]);
+          for (int i = 0; i < TILE / GROUP_THREADS; ++i) {
+            const uint32_t e = uint32_t(tg + GROUP_THREADS * i);
+            T[e] = cmulf(term_phase(e, op, base, s_terms, tab_lo[g], tab_hi[g], tab_cross[g]), T[e]);
           }
-          bar_compute();
+          bar_group(g);
           continue;
         }
-        // ---- unitary op ----
+        // ---- unitary op: this thread owns column tg (A row / TMEM lane) and its 32 rows ----
         const int u = op.u;
+        const uint64_t k = p * uint64_t(P.nu) + uint64_t(u);
+        const int sl = int(k % NOPSLOT);
+        if (!mine) {
+          // the pair's other half is empty: release the operand slot without using it
+          if (abort_sh) break;
+          if (tg == 0) {
+            if (!mbar_wait(bar_ofull(sl), uint32_t((k / NOPSLOT) & 1))) fail(2);
+            mbar_arrive(bar_oempty(sl));
+          }
+          continue;
+        }
         uint32_t cb = 0;
 #pragma unroll
-        for (int j = 0; j < TILE_BITS - GROUP_QUBITS; ++j) cb |= uint32_t((col >> j) & 1) << nongate[u][j];
+        for (int j = 0; j < TILE_BITS - GROUP_QUBITS; ++j) cb |= uint32_t((tg >> j) & 1) << nongate[u][j];
         const uint32_t p0 = 1u << P.pos[u][0], p1 = 1u << P.pos[u][1], p2 = 1u << P.pos[u][2],
-                       p3 = 1u << P.pos[u][3];
-        const uint32_t rb = cb | (half ? (1u << P.pos[u][4]) : 0u);
-        uint32_t ro[16];  // tile offsets of this thread's rows 16*half + i
+                       p3 = 1u << P.pos[u][3], p4 = 1u << P.pos[u][4];
+        uint32_t lo8[8];  // tile offsets of rows 0..7 (gate bits 0-2)
 #pragma unroll
-        for (int i = 0; i < 16; ++i)
-          ro[i] = rb | ((i & 1) ? p0 : 0u) | ((i & 2) ? p1 : 0u) | ((i & 4) ? p2 : 0u) | ((i & 8) ? p3 : 0u);
+        for (int i = 0; i < 8; ++i) lo8[i] = cb | ((i & 1) ? p0 : 0u) | ((i & 2) ? p1 : 0u) | ((i & 4) ? p2 : 0u);
+        const uint32_t hi4[4] = {0u, p3, p4, p3 | p4};  // rows 8q..8q+7
 #pragma unroll
-        for (int s = 0; s < 2; ++s) {
+        for (int q = 0; q < 4; ++q) {
           float2 x[8];
 #pragma unroll
-          for (int i = 0; i < 8; ++i) x[i] = T[ro[8 * s + i]];
+          for (int i = 0; i < 8; ++i) x[i] = T[lo8[i] | hi4[q]];
           uint32_t hr[4], lr[4], hm[4], lm[4];
 #pragma unroll
           for (int i = 0; i < 4; ++i) {
@@ -397,44 +465,49 @@ __global__ void __launch_bounds__(THREADS, 1) k_fused_pass(const __grid_constant
             lr[i] = pack_bf16(a.x - lo_half(hr[i]), c.x - hi_half(hr[i]));
             lm[i] = pack_bf16(a.y - lo_half(hm[i]), c.y - hi_half(hm[i]));
           }
-          const uint32_t cre = uint32_t(2 * half + s), cim = cre + 4u;  // 16-byte chunks of rows 16h+8s..+7
+          const uint32_t cre = uint32_t(q), cim = cre + 4u;  // 16-byte chunks of rows 8q..8q+7
           *reinterpret_cast<uint4*>(ahi_row + ((cre ^ row7) << 4)) = make_uint4(hr[0], hr[1], hr[2], hr[3]);
           *reinterpret_cast<uint4*>(alo_row + ((cre ^ row7) << 4)) = make_uint4(lr[0], lr[1], lr[2], lr[3]);
           *reinterpret_cast<uint4*>(ahi_row + ((cim ^ row7) << 4)) = make_uint4(hm[0], hm[1], hm[2], hm[3]);
           *reinterpret_cast<uint4*>(alo_row + ((cim ^ row7) << 4)) = make_uint4(lm[0], lm[1], lm[2], lm[3]);
         }
         fence_async_smem();
-        bar_compute();
-        if (tid == 0) {
+        if (bar_any(1 + g, GROUP_THREADS, abort_sh)) break;
+        if (tg == 0) {
+          if (!mbar_wait(bar_ofull(sl), uint32_t((k / NOPSLOT) & 1))) fail(2);
           tc_fence_after();
-          const uint32_t b_hi = smem_u32(smem + SM_ROPS + u * OPERAND_BYTES);
+          const uint32_t b_hi = smem_u32(smem + SM_B + sl * OPERAND_BYTES);
           const uint32_t b_lo = b_hi + OPERAND_BYTES / 2;
           const uint64_t dah = sw128_desc(a_hi), dal = sw128_desc(a_lo), dbh = sw128_desc(b_hi), dbl = sw128_desc(b_lo);
 #pragma unroll
-          for (int s = 0; s < 4; ++s) mma_bf16(tmem, dah + 2 * s, dbh + 2 * s, idesc, s > 0);
+          for (int s = 0; s < 4; ++s) mma_bf16(d_tmem, dah + 2 * s, dbh + 2 * s, idesc, s > 0);
 #pragma unroll
-          for (int s = 0; s < 4; ++s) mma_bf16(tmem, dal + 2 * s, dbh + 2 * s, idesc, 1);
+          for (int s = 0; s < 4; ++s) mma_bf16(d_tmem, dal + 2 * s, dbh + 2 * s, idesc, 1);
 #pragma unroll
-          for (int s = 0; s < 4; ++s) mma_bf16(tmem, dah + 2 * s, dbl + 2 * s, idesc, 1);
-          mma_commit(bar_mma);
+          for (int s = 0; s < 4; ++s) mma_bf16(d_tmem, dah + 2 * s, dbl + 2 * s, idesc, 1);
+          mma_commit(bar_mma(g));
+          mma_commit(bar_oempty(sl));  // the slot is free once these MMAs have read it
+          if (!mbar_wait(bar_mma(g), mma_phase)) fail(2);
         }
-        if (tid == 0 && !mbar_wait(bar_mma, mma_phase)) fail(2);
         mma_phase ^= 1u;
-        bar_compute();
+        const bool stop = bar_any(1 + g, GROUP_THREADS, abort_sh);
         tc_fence_after();
-        uint32_t re[16], im[16];
-        NCSIM_TMEM_LD16(taddr, re);
-        NCSIM_TMEM_LD16(taddr + 32u, im);
-        asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+        if (stop) break;
 #pragma unroll
-        for (int i = 0; i < 16; ++i) T[ro[i]] = make_float2(__uint_as_float(re[i]), __uint_as_float(im[i]));
+        for (int h = 0; h < 2; ++h) {
+          uint32_t re[16], im[16];
+          NCSIM_TMEM_LD16(taddr + uint32_t(16 * h), re);
+          NCSIM_TMEM_LD16(taddr + uint32_t(32 + 16 * h), im);
+          asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+#pragma unroll
+          for (int i = 0; i < 16; ++i)
+            T[lo8[i & 7] | hi4[2 * h + (i >> 3)]] = make_float2(__uint_as_float(re[i]), __uint_as_float(im[i]));
+        }
         tc_fence_before();
-        bar_compute();
-        if (abort_sh) break;
+        bar_group(g);
       }
-      fence_async_smem();
-      mbar_arrive(bar_done(b));
-      if (abort_sh) break;
+      if (bar_any(1 + g, GROUP_THREADS, abort_sh)) break;
+      if (mine) mbar_arrive(bar_tdone(b));
     }
   }
   tc_fence_before();
@@ -592,7 +665,8 @@ extern "C" ncsim_status ncsim_sv_run_fused(ncsim_state* s, const ncsim_circuit* 
     NCSIM_CUDA(cudaMallocAsync(&d_err, sizeof(int), s->stream));
     NCSIM_CUDA(cudaMemsetAsync(d_err, 0, sizeof(int), s->stream));
     NCSIM_CUDA(cudaFuncSetAttribute(fused::k_fused_pass, cudaFuncAttributeMaxDynamicSharedMemorySize, fused::SM_DYNAMIC));
-    const unsigned grid = unsigned(std::min<uint64_t>(uint64_t(sm_count()), s->len >> fused::TILE_BITS));
+    const uint64_t pairs = ((s->len >> fused::TILE_BITS) + 1) / 2;  // each CTA takes tiles two at a time
+    const unsigned grid = unsigned(std::min<uint64_t>(uint64_t(sm_count()), pairs));
     size_t m = 0, pi = 0;
     uint64_t gemm = 0;
     for (const fused::Segment& seg : dp->plan.segments) {
