@@ -421,10 +421,27 @@ __global__ void __launch_bounds__(THREADS, 1) k_fused_pass(const __grid_constant
           // ---- diagonal terms: per-tile tables, then one sweep of the tile ----
           build_tables(op, base, tg, s_terms, tab_lo[g], tab_hi[g], tab_cross[g]);
           bar_group(g);
+          {
+            // element e = tg + 128 i: its low 6 bits are the thread's, so the low-half
+            // phase is one read; the high-half entries are the same across a warp
+            const uint32_t lo = uint32_t(tg) & ((1u << HALF) - 1);
+            const float2 L = tab_lo[g][lo];
+            if (op.tc == op.t1) {
+#pragma unroll 8
+              for (int i = 0; i < TILE / GROUP_THREADS; ++i) {
+                const uint32_t e = uint32_t(tg + GROUP_THREADS * i), hi = e >> HALF;
+                float2 c = cmulf(L, tab_hi[g][hi]);
+                const uint32_t sg = uint32_t(__popc(lo & tab_cross[g][hi]) & 1) << 31;
+                c = make_float2(__uint_as_float(__float_as_uint(c.x) ^ sg), __uint_as_float(__float_as_uint(c.y) ^ sg));
+                T[e] = cmulf(c, T[e]);
+              }
+            } else {
 #pragma unroll 4
-          for (int i = 0; i < TILE / GROUP_THREADS; ++i) {
-            const uint32_t e = uint32_t(tg + GROUP_THREADS * i);
-            T[e] = cmulf(term_phase(e, op, base, s_terms, tab_lo[g], tab_hi[g], tab_cross[g]), T[e]);
+              for (int i = 0; i < TILE / GROUP_THREADS; ++i) {
+                const uint32_t e = uint32_t(tg + GROUP_THREADS * i);
+                T[e] = cmulf(term_phase(e, op, base, s_terms, tab_lo[g], tab_hi[g], tab_cross[g]), T[e]);
+              }
+            }
           }
           bar_group(g);
           continue;
