@@ -427,13 +427,28 @@ __global__ void __launch_bounds__(THREADS, 1) k_fused_pass(const __grid_constant
             const uint32_t lo = uint32_t(tg) & ((1u << HALF) - 1);
             const float2 L = tab_lo[g][lo];
             if (op.tc == op.t1) {
-#pragma unroll 8
-              for (int i = 0; i < TILE / GROUP_THREADS; ++i) {
-                const uint32_t e = uint32_t(tg + GROUP_THREADS * i), hi = e >> HALF;
-                float2 c = cmulf(L, tab_hi[g][hi]);
-                const uint32_t sg = uint32_t(__popc(lo & tab_cross[g][hi]) & 1) << 31;
-                c = make_float2(__uint_as_float(__float_as_uint(c.x) ^ sg), __uint_as_float(__float_as_uint(c.y) ^ sg));
-                T[e] = cmulf(c, T[e]);
+              // blocks of 8: every load before any store (the tile and the tables may alias as far
+              // as the compiler knows, so a store would hold back the next loads)
+              const float2* __restrict__ th = tab_hi[g];
+              const uint8_t* __restrict__ tx = tab_cross[g];
+#pragma unroll 1
+              for (int i0 = 0; i0 < TILE / GROUP_THREADS; i0 += 8) {
+                float2 v[8], h[8];
+                uint32_t x[8];
+#pragma unroll
+                for (int j = 0; j < 8; ++j) {
+                  const uint32_t e = uint32_t(tg + GROUP_THREADS * (i0 + j)), hi = e >> HALF;
+                  v[j] = T[e];
+                  h[j] = th[hi];
+                  x[j] = tx[hi];
+                }
+#pragma unroll
+                for (int j = 0; j < 8; ++j) {
+                  float2 c = cmulf(L, h[j]);
+                  const uint32_t sg = uint32_t(__popc(lo & x[j]) & 1) << 31;
+                  c = make_float2(__uint_as_float(__float_as_uint(c.x) ^ sg), __uint_as_float(__float_as_uint(c.y) ^ sg));
+                  T[uint32_t(tg + GROUP_THREADS * (i0 + j))] = cmulf(c, v[j]);
+                }
               }
             } else {
 #pragma unroll 4
@@ -469,10 +484,14 @@ __global__ void __launch_bounds__(THREADS, 1) k_fused_pass(const __grid_constant
         for (int i = 0; i < 8; ++i) lo8[i] = cb | ((i & 1) ? p0 : 0u) | ((i & 2) ? p1 : 0u) | ((i & 4) ? p2 : 0u);
         const uint32_t hi4[4] = {0u, p3, p4, p3 | p4};  // rows 8q..8q+7
 #pragma unroll
-        for (int q = 0; q < 4; ++q) {
-          float2 x[8];
+        for (int q0 = 0; q0 < 4; q0 += 2) {
+          float2 xx[16];  // rows of two chunks, loaded before any store to A
 #pragma unroll
-          for (int i = 0; i < 8; ++i) x[i] = T[lo8[i] | hi4[q]];
+          for (int i = 0; i < 16; ++i) xx[i] = T[lo8[i & 7] | hi4[q0 + (i >> 3)]];
+#pragma unroll
+          for (int qq = 0; qq < 2; ++qq) {
+          const int q = q0 + qq;
+          const float2* x = xx + 8 * qq;
           uint32_t hr[4], lr[4], hm[4], lm[4];
 #pragma unroll
           for (int i = 0; i < 4; ++i) {
@@ -487,6 +506,7 @@ __global__ void __launch_bounds__(THREADS, 1) k_fused_pass(const __grid_constant
           *reinterpret_cast<uint4*>(alo_row + ((cre ^ row7) << 4)) = make_uint4(lr[0], lr[1], lr[2], lr[3]);
           *reinterpret_cast<uint4*>(ahi_row + ((cim ^ row7) << 4)) = make_uint4(hm[0], hm[1], hm[2], hm[3]);
           *reinterpret_cast<uint4*>(alo_row + ((cim ^ row7) << 4)) = make_uint4(lm[0], lm[1], lm[2], lm[3]);
+          }
         }
         fence_async_smem();
         if (bar_any(1 + g, GROUP_THREADS, abort_sh)) break;
