@@ -402,7 +402,7 @@ def main():
     ap.add_argument("--steps", type=int, default=3)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--n", type=int, default=32)
+    ap.add_argument("--n", "--qubits", type=int, default=32, dest="n")  # --qubits passes through torchrun
     ap.add_argument("--depth", type=int, default=20)
     ap.add_argument("--path", default="auto", choices=["auto", "plain", "fused"])
     ap.add_argument("--cpu-budget", type=float, default=15.0)

@@ -2,6 +2,7 @@
 // function validates its arguments on the host (the reference's checks in
 // src/error.rs:69-82 and src/state/vector.rs), enqueues kernels on the state's
 // stream, and waits only when it returns a value.
+#include <atomic>
 #include "engine.cuh"
 #include "host_math.hpp"
 
@@ -98,7 +99,9 @@ ncsim_state* state_new(uint32_t n, int32_t precision) {
   if (precision != NCSIM_C128 && precision != NCSIM_C64) throw Error(NCSIM_ERR_INVALID, "precision must be C128 or C64");
   const uint32_t cap = precision == NCSIM_C128 ? 33 : 34;
   if (n > cap) throw Error(NCSIM_ERR_INVALID, "state vector of " + std::to_string(n) + " qubits exceeds " + std::to_string(cap));
+  static std::atomic<uint64_t> next_uid{1};
   auto* s = new ncsim_state();
+  s->uid = next_uid.fetch_add(1);
   s->n = n;
   s->precision = precision;
   s->len = uint64_t(1) << n;

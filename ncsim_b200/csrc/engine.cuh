@@ -96,6 +96,7 @@ struct ncsim_state {
   mutable std::vector<ncsim::ProfRecord> prof_recs;
   mutable std::vector<cudaEvent_t> prof_pool;
   cudaEvent_t timer0 = nullptr, timer1 = nullptr;
+  uint64_t uid = 0;  // unique over the process: keys the circuits' captured gate graphs
 
   size_t elem_bytes() const { return precision == NCSIM_C128 ? 16 : 8; }
   size_t bytes() const { return size_t(len) * elem_bytes(); }

@@ -116,6 +116,8 @@ struct ncsim_circuit {
   mutable std::shared_ptr<void> fused_plan;
   mutable uint32_t fused_plan_fuse = 0;
   mutable int fused_plan_device = -1;
+  // runs of gates captured as CUDA graphs for one state (built on first use)
+  mutable std::shared_ptr<void> gate_graphs;
   uint64_t num_gates() const;
   uint64_t num_measurements() const;
   std::string text() const;

@@ -2,7 +2,10 @@
 // and the C ABI of the host layer: RNG, circuits, gates, run/measure/sample.
 #include <algorithm>
 #include <cmath>
+#include <cstdlib>
 #include <cstring>
+#include <memory>
+#include <mutex>
 
 #include "ir.hpp"
 
@@ -310,6 +313,97 @@ ncsim_status ncsim_sv_measure(ncsim_state* s, uint64_t x, uint64_t z, uint32_t p
   });
 }
 
+}  // extern "C"
+
+namespace {
+
+// Runs of at least MIN_GRAPH_GATES consecutive gates (annotations between them
+// allowed) are captured once per state as CUDA graphs and replayed by later
+// runs of the same circuit on the same state: one graph launch instead of a
+// host lowering step and a kernel launch per gate.  Measurements, resets and
+// noise stay outside the graphs (their draws and decisions are made on the
+// host).  Not used while the launch profiler records per-launch events, nor
+// when the environment sets NCSIM_NO_GATE_GRAPHS (kernel-by-kernel launches).
+constexpr size_t MIN_GRAPH_GATES = 16;
+
+struct GateGraphs {
+  uint64_t state_uid = 0;
+  int device = -1;
+  std::vector<std::pair<size_t, size_t>> runs;  // [first op, end op) of each run
+  std::vector<cudaGraphExec_t> exec;            // null until captured
+  std::vector<char> failed;                     // capture did not succeed: launch directly
+  ~GateGraphs() {
+    for (auto e : exec)
+      if (e) cudaGraphExecDestroy(e);
+  }
+};
+
+std::mutex g_graph_mu;
+
+bool annotation(OpKind k) { return k == OpKind::Tick || k == OpKind::Detector || k == OpKind::Observable; }
+
+std::shared_ptr<GateGraphs> gate_graphs_for(const ncsim_circuit* c, const ncsim_state* s) {
+  std::lock_guard<std::mutex> lk(g_graph_mu);
+  auto g = std::static_pointer_cast<GateGraphs>(c->gate_graphs);
+  if (g && g->state_uid == s->uid && g->device == s->device) return g;
+  g = std::make_shared<GateGraphs>();
+  g->state_uid = s->uid;
+  g->device = s->device;
+  for (size_t i = 0; i < c->ops.size();) {
+    if (c->ops[i].kind != OpKind::Gate) {
+      ++i;
+      continue;
+    }
+    size_t j = i, gates = 0;
+    while (j < c->ops.size() && (c->ops[j].kind == OpKind::Gate || annotation(c->ops[j].kind))) {
+      gates += c->ops[j].kind == OpKind::Gate;
+      ++j;
+    }
+    if (gates >= MIN_GRAPH_GATES) g->runs.push_back({i, j});
+    i = j;
+  }
+  g->exec.assign(g->runs.size(), nullptr);
+  g->failed.assign(g->runs.size(), 0);
+  c->gate_graphs = g;
+  return g;
+}
+
+// Launches the gates of ops[first, end) on the state's stream, as a graph when it can.
+void run_gates(ncsim_state* s, const ncsim_circuit* c, GateGraphs& g, size_t k) {
+  const auto [first, end] = g.runs[k];
+  if (!g.exec[k] && !g.failed[k]) {
+    cudaGraph_t graph = nullptr;
+    bool ok = cudaStreamBeginCapture(s->stream, cudaStreamCaptureModeThreadLocal) == cudaSuccess;
+    if (ok) {
+      try {
+        for (size_t i = first; i < end; ++i)
+          if (c->ops[i].kind == OpKind::Gate) apply_lowered(s, c->ops[i].lowered);
+      } catch (...) {
+        ok = false;
+      }
+      ok = cudaStreamEndCapture(s->stream, &graph) == cudaSuccess && ok;
+      cudaGraphExec_t e = nullptr;
+      if (ok) ok = cudaGraphInstantiate(&e, graph, 0) == cudaSuccess;
+      if (graph) cudaGraphDestroy(graph);
+      if (ok) g.exec[k] = e;
+    }
+    if (!ok) {
+      cudaGetLastError();  // a failed capture leaves only its own error behind
+      g.failed[k] = 1;
+    }
+  }
+  if (g.exec[k]) {
+    NCSIM_CUDA(cudaGraphLaunch(g.exec[k], s->stream));
+  } else {
+    for (size_t i = first; i < end; ++i)
+      if (c->ops[i].kind == OpKind::Gate) apply_lowered(s, c->ops[i].lowered);
+  }
+}
+
+}  // namespace
+
+extern "C" {
+
 ncsim_status ncsim_sv_run(ncsim_state* s, const ncsim_circuit* c, ncsim_rng* rng, uint8_t* rec, size_t cap, size_t* len) {
   return guarded([&] {
     need(s, "state");
@@ -320,10 +414,19 @@ ncsim_status ncsim_sv_run(ncsim_state* s, const ncsim_circuit* c, ncsim_rng* rng
     if (c->num_measurements() > cap) throw Error(NCSIM_ERR_INVALID, "record buffer too small");
     if (c->num_measurements()) need(rec, "record");
     std::lock_guard<std::recursive_mutex> lk(s->mu);
-    size_t m = 0;
-    for (auto& op : c->ops) {
-      int r = apply_op(s, op, *rng);
+    static const bool graphs_off = std::getenv("NCSIM_NO_GATE_GRAPHS") != nullptr;
+    std::shared_ptr<GateGraphs> g;
+    if (!s->prof && !graphs_off) g = gate_graphs_for(c, s);
+    size_t m = 0, k = 0;
+    for (size_t i = 0; i < c->ops.size();) {
+      if (g && k < g->runs.size() && g->runs[k].first == i) {
+        run_gates(s, c, *g, k);
+        i = g->runs[k++].second;
+        continue;
+      }
+      int r = apply_op(s, c->ops[i], *rng);
       if (r >= 0) rec[m++] = uint8_t(r);
+      ++i;
     }
     NCSIM_CUDA(cudaStreamSynchronize(s->stream));
     if (len) *len = m;

@@ -248,6 +248,29 @@ def test_random_layers_with_measurements(nb, oracle):
     assert maxerr(g, o) < TOL
 
 
+def test_gate_runs_replayed_as_graphs(nb, oracle):
+    """Runs of gates are captured as CUDA graphs on the first run of a circuit on
+    a state and replayed by later runs; measurements in between stay direct.  The
+    register after each run, and the records, match the oracle; a run with the
+    launch profiler on (direct launches) gives the same register."""
+    n = 14
+    text = oracle.random_circuit_text(n, 6, 9) + "M 3\n" + oracle.random_circuit_text(n, 4, 10).split("\n", 1)[1]
+    g = nb.GpuStateVector(n)
+    o = oracle.StateVector(n)
+    rg, ro = nb.StdRng(5), oracle.StdRng(5)
+    c, oc = nb.Circuit.parse(text), oracle.Circuit(text)
+    for _ in range(3):
+        assert g.run(c, rg) == o.run(oc, ro)
+        assert maxerr(g, o) < TOL
+    p = nb.GpuStateVector(n)
+    p.profile(True)
+    p.run(c, nb.StdRng(5))
+    q = nb.GpuStateVector(n)
+    q.run(c, nb.StdRng(5))
+    assert np.abs(p.to_vector() - q.to_vector()).max() < TOL
+    assert p.profile_read()  # the profiled run launched kernel by kernel
+
+
 def test_noisy_trajectories_match_oracle(nb, oracle):
     """The batched family's per-trajectory semantics on the plain path (complex128)."""
     for t in range(3):
