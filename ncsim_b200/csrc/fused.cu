@@ -61,17 +61,20 @@ constexpr int HALF = TILE_BITS / 2;              // 6-bit halves of the tile ind
 enum TermClass : uint8_t { T_LOW = 0, T_HIGH = 1, T_CROSS_SIGN = 2, T_GENERIC = 3 };
 
 struct OpDesc {
-  uint8_t kind;  // 0 unitary, 1 terms
+  uint8_t kind;  // 0 unitary, 1 terms, 2 terms applied by the next unitary's split, 3 by the previous one's read-back
   uint8_t u;     // unitary index (operand slot)
   // terms [t0, t1) sorted by class: low half [t0,tl), high half [tl,th),
   // cross-half signs [th,tc), the rest [tc,t1)
   uint16_t t0, tl, th, tc, t1;
+  uint16_t p0, p1;  // unitary: the preceding terms op's terms, applied while splitting
+  uint16_t q0, q1;  // unitary: the following terms op's terms, applied while reading back
 };
 
 struct TermDesc {
   uint64_t cmask;  // bits outside the window (constant over a tile)
-  uint32_t tmask;  // tile-local bits
+  uint32_t tmask;  // tile-local bits (for a split-applied term: the unitary's non-gate bits)
   float cr, ci;
+  uint32_t rowpat;  // split-applied sign term: the rows (gate index) whose sign flips; 0: a phase on the column
 };
 
 struct PassParams {
@@ -253,6 +256,23 @@ __device__ __forceinline__ float2 term_phase(uint32_t e, const OpDesc& op, uint6
   return c;
 }
 
+// The terms [k0, k1) of a diagonal op applied by a unitary's split or read-back,
+// for the column whose non-gate tile bits are cb: sign terms on one gate qubit
+// flip rows (rowpat), the others multiply the whole column.
+__device__ __forceinline__ void column_terms(const TermDesc* terms, int k0, int k1, uint64_t base, uint32_t cb,
+                                             uint32_t& smask, float2& cth, bool& scal) {
+  for (int k = k0; k < k1; ++k) {
+    const TermDesc tm = terms[k];
+    if ((base & tm.cmask) != tm.cmask || (cb & tm.tmask) != tm.tmask) continue;
+    if (tm.rowpat) {
+      smask ^= tm.rowpat;
+    } else {
+      cth = cmulf(cth, make_float2(tm.cr, tm.ci));
+      scal = true;
+    }
+  }
+}
+
 __device__ __forceinline__ void bar_group(int g) {
   asm volatile("bar.sync %0, %1;" ::"r"(1 + g), "r"(GROUP_THREADS) : "memory");
 }
@@ -416,6 +436,7 @@ __global__ void __launch_bounds__(THREADS, 1) k_fused_pass(const __grid_constant
       float2* T = tiles + size_t(b) * TILE;
       for (int oi = 0; oi < P.nops; ++oi) {
         const OpDesc op = s_ops[oi];
+        if (op.kind >= 2) continue;  // applied by a neighbouring unitary's split or read-back
         if (op.kind == 1) {
           if (!mine) continue;
           // ---- diagonal terms: per-tile tables, then one sweep of the tile ----
@@ -483,11 +504,28 @@ __global__ void __launch_bounds__(THREADS, 1) k_fused_pass(const __grid_constant
 #pragma unroll
         for (int i = 0; i < 8; ++i) lo8[i] = cb | ((i & 1) ? p0 : 0u) | ((i & 2) ? p1 : 0u) | ((i & 4) ? p2 : 0u);
         const uint32_t hi4[4] = {0u, p3, p4, p3 | p4};  // rows 8q..8q+7
+        // a preceding diagonal op, reduced to this column: a phase and a sign mask over the 32 rows
+        uint32_t smask = 0;
+        float2 cth = make_float2(1.f, 0.f);
+        bool scal = false;
+        column_terms(s_terms, op.p0, op.p1, base, cb, smask, cth, scal);
 #pragma unroll
         for (int q0 = 0; q0 < 4; q0 += 2) {
           float2 xx[16];  // rows of two chunks, loaded before any store to A
 #pragma unroll
           for (int i = 0; i < 16; ++i) xx[i] = T[lo8[i & 7] | hi4[q0 + (i >> 3)]];
+          if (scal) {
+#pragma unroll
+            for (int i = 0; i < 16; ++i) xx[i] = cmulf(cth, xx[i]);
+          }
+          if (smask) {
+#pragma unroll
+            for (int i = 0; i < 16; ++i) {
+              const uint32_t sg = (smask << (31 - (8 * q0 + i))) & 0x80000000u;
+              xx[i] = make_float2(__uint_as_float(__float_as_uint(xx[i].x) ^ sg),
+                                  __uint_as_float(__float_as_uint(xx[i].y) ^ sg));
+            }
+          }
 #pragma unroll
           for (int qq = 0; qq < 2; ++qq) {
           const int q = q0 + qq;
@@ -527,6 +565,11 @@ __global__ void __launch_bounds__(THREADS, 1) k_fused_pass(const __grid_constant
           if (!mbar_wait(bar_mma(g), mma_phase)) fail(2);
         }
         mma_phase ^= 1u;
+        // a following diagonal op, reduced to this column (computed while the MMAs run)
+        uint32_t smask2 = 0;
+        float2 cth2 = make_float2(1.f, 0.f);
+        bool scal2 = false;
+        column_terms(s_terms, op.q0, op.q1, base, cb, smask2, cth2, scal2);
         const bool stop = bar_any(1 + g, GROUP_THREADS, abort_sh);
         tc_fence_after();
         if (stop) break;
@@ -537,8 +580,13 @@ __global__ void __launch_bounds__(THREADS, 1) k_fused_pass(const __grid_constant
           NCSIM_TMEM_LD16(taddr + uint32_t(32 + 16 * h), im);
           asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
 #pragma unroll
-          for (int i = 0; i < 16; ++i)
-            T[lo8[i & 7] | hi4[2 * h + (i >> 3)]] = make_float2(__uint_as_float(re[i]), __uint_as_float(im[i]));
+          for (int i = 0; i < 16; ++i) {
+            float2 v = make_float2(__uint_as_float(re[i]), __uint_as_float(im[i]));
+            if (scal2) v = cmulf(cth2, v);
+            const uint32_t sg = (smask2 << (31 - (16 * h + i))) & 0x80000000u;
+            T[lo8[i & 7] | hi4[2 * h + (i >> 3)]] =
+                make_float2(__uint_as_float(__float_as_uint(v.x) ^ sg), __uint_as_float(__float_as_uint(v.y) ^ sg));
+          }
         }
         tc_fence_before();
         bar_group(g);
@@ -644,6 +692,61 @@ std::unique_ptr<DevicePlan> build_device_plan(const ncsim_circuit& c, uint32_t m
       }
       P.nops = no;
       P.nu = nu;
+      // A terms op right before a unitary whose terms are, relative to that unitary's five
+      // qubits, phases of the other bits or signs on one of its qubits is applied while the
+      // unitary splits the tile: a phase and a 32-row sign mask per column.
+      static const uint32_t rowpat[GROUP_QUBITS] = {0xAAAAAAAAu, 0xCCCCCCCCu, 0xF0F0F0F0u, 0xFF00FF00u, 0xFFFF0000u};
+      for (int i = 0; i + 1 < no; ++i) {
+        OpDesc& t = P.ops[i];
+        OpDesc& un = P.ops[i + 1];
+        if (t.kind != 1 || un.kind != 0) continue;
+        uint32_t gm = 0;
+        for (int j = 0; j < GROUP_QUBITS; ++j) gm |= 1u << P.pos[un.u][j];
+        bool ok = true;
+        for (int k = t.t0; k < t.t1 && ok; ++k) {
+          const TermDesc& td = P.terms[k];
+          const uint32_t gpart = td.tmask & gm;
+          ok = gpart == 0 || (__builtin_popcount(gpart) == 1 && td.cr == -1.0f && td.ci == 0.0f);
+        }
+        if (!ok) continue;
+        for (int k = t.t0; k < t.t1; ++k) {
+          TermDesc& td = P.terms[k];
+          const uint32_t gpart = td.tmask & gm;
+          td.rowpat = 0;
+          for (int j = 0; j < GROUP_QUBITS; ++j)
+            if (gpart == (1u << P.pos[un.u][j])) td.rowpat = rowpat[j];
+          td.tmask &= ~gm;
+        }
+        t.kind = 2;
+        un.p0 = t.t0;
+        un.p1 = t.t1;
+      }
+      // the same for a terms op left after a unitary, applied by its read-back
+      for (int i = 1; i < no; ++i) {
+        OpDesc& t = P.ops[i];
+        OpDesc& un = P.ops[i - 1];
+        if (t.kind != 1 || un.kind != 0) continue;
+        uint32_t gm = 0;
+        for (int j = 0; j < GROUP_QUBITS; ++j) gm |= 1u << P.pos[un.u][j];
+        bool ok = true;
+        for (int k = t.t0; k < t.t1 && ok; ++k) {
+          const TermDesc& td = P.terms[k];
+          const uint32_t gpart = td.tmask & gm;
+          ok = gpart == 0 || (__builtin_popcount(gpart) == 1 && td.cr == -1.0f && td.ci == 0.0f);
+        }
+        if (!ok) continue;
+        for (int k = t.t0; k < t.t1; ++k) {
+          TermDesc& td = P.terms[k];
+          const uint32_t gpart = td.tmask & gm;
+          td.rowpat = 0;
+          for (int j = 0; j < GROUP_QUBITS; ++j)
+            if (gpart == (1u << P.pos[un.u][j])) td.rowpat = rowpat[j];
+          td.tmask &= ~gm;
+        }
+        t.kind = 3;
+        un.q0 = t.t0;
+        un.q1 = t.t1;
+      }
       // the pass's first operand: an offset for now, a device pointer below
       P.rops = reinterpret_cast<const uint4*>(uintptr_t(nu ? offsets[offsets.size() - nu] : 0));
       dp->params.push_back(P);
