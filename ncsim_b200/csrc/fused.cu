@@ -10,9 +10,9 @@
 // slot.  Per group and tile:
 //   unitary op: the tile as 32 rows (the unitary's 5 qubits) x 128 columns;
 //     each thread owns a column, splits its 32 amplitudes into bf16 hi/lo
-//     and writes them K-major, 128-byte swizzled (A = X^T, 128 x 64); one
-//     thread issues 12 tcgen05.mma (M=128, N=64, K=16, bf16 in, f32
-//     accumulate in the group's 64 TMEM columns):
+//     and writes them into its own TMEM lane (A = X^T, 128 x 64, K-major,
+//     tcgen05.st); one thread issues 12 tcgen05.mma with A in TMEM (M=128,
+//     N=64, K=16, bf16 in, f32 accumulate in the group's 64 TMEM columns):
 //       D = Xhi.Rhi + Xlo.Rhi + Xhi.Rlo
 //     with R the real form [[Ur, -Ui], [Ui, Ur]] of the fused unitary (bf16
 //     hi/lo images made on the host); each thread reads its D row back
@@ -46,15 +46,14 @@ constexpr int THREADS = COMPUTE_THREADS + TILE_THREADS + 32;
 constexpr int TILE = 1 << TILE_BITS;
 constexpr uint32_t TILE_BYTES = uint32_t(TILE) * 8u;
 constexpr int OPERAND_BYTES = 16384;  // B: bf16 hi (8 KB) + lo (8 KB)
-constexpr int A_BYTES = 16384;        // A: 128 x 64 bf16, hi and lo separately
 constexpr int NTILEBUF = 3;           // tile buffers rotating over the CTA's tiles
 constexpr int NOPSLOT = 3;            // B operand slots rotating over the unitary uses
-constexpr int SM_A = 0;                                      // per group: A hi, A lo
-constexpr int SM_B = SM_A + GROUPS * 2 * A_BYTES;
+constexpr int SM_B = 0;
 constexpr int SM_TILE0 = SM_B + NOPSLOT * OPERAND_BYTES;
 constexpr int SM_TOTAL = SM_TILE0 + NTILEBUF * int(TILE_BYTES);
 constexpr int SM_DYNAMIC = SM_TOTAL + 1008;  // the dynamic base is 16-byte aligned: slack to reach 1024
-constexpr uint32_t TMEM_COLS = 128;          // 64 accumulator columns per group
+// per group 128 columns: the accumulator D (64), the A operand's bf16 hi (32) and lo (32)
+constexpr uint32_t TMEM_COLS = 256;
 constexpr long long WAIT_CYCLES = 4000000000ll;  // about 2 s at 1.9 GHz
 constexpr int HALF = TILE_BITS / 2;              // 6-bit halves of the tile index
 
@@ -129,7 +128,6 @@ __device__ __forceinline__ void bulk_load(uint32_t dst, const void* src, uint32_
                "l"(src), "r"(bytes), "r"(bar)
                : "memory");
 }
-__device__ __forceinline__ void fence_async_smem() { asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); }
 __device__ __forceinline__ void cp_async16(uint32_t dst, const void* src) {
   asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(dst), "l"(src) : "memory");
 }
@@ -166,12 +164,19 @@ __device__ __forceinline__ uint64_t sw128_desc(uint32_t saddr) {
   return d;
 }
 
-__device__ __forceinline__ void mma_bf16(uint32_t tmem_d, uint64_t a, uint64_t b, uint32_t idesc, uint32_t acc) {
+// D (TMEM) += A (TMEM, K-major rows = lanes) x B (shared memory descriptor)
+__device__ __forceinline__ void mma_bf16_ta(uint32_t tmem_d, uint32_t tmem_a, uint64_t b, uint32_t idesc, uint32_t acc) {
   asm volatile(
       "{\n\t.reg .pred p;\n\t"
       "setp.ne.b32 p, %4, 0;\n\t"
-      "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, {%5, %6, %7, %8}, p;\n\t}"
-      ::"r"(tmem_d), "l"(a), "l"(b), "r"(idesc), "r"(acc), "r"(0), "r"(0), "r"(0), "r"(0));
+      "tcgen05.mma.cta_group::1.kind::f16 [%0], [%1], %2, %3, {%5, %6, %7, %8}, p;\n\t}"
+      ::"r"(tmem_d), "r"(tmem_a), "l"(b), "r"(idesc), "r"(acc), "r"(0), "r"(0), "r"(0), "r"(0));
+}
+// eight 32-bit columns of this thread's TMEM lane
+__device__ __forceinline__ void tmem_st8(uint32_t taddr, const uint32_t (&v)[8]) {
+  asm volatile("tcgen05.st.sync.aligned.32x32b.x8.b32 [%0], {%1, %2, %3, %4, %5, %6, %7, %8};" ::"r"(taddr), "r"(v[0]),
+               "r"(v[1]), "r"(v[2]), "r"(v[3]), "r"(v[4]), "r"(v[5]), "r"(v[6]), "r"(v[7])
+               : "memory");
 }
 __device__ __forceinline__ void mma_commit(uint32_t bar) {
   asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(bar) : "memory");
@@ -418,13 +423,11 @@ __global__ void __launch_bounds__(THREADS, 1) k_fused_pass(const __grid_constant
     // ---------------- tensor-core program: group g on its tile of each pair ----------------
     const int g = warp / 4, tg = tid & (GROUP_THREADS - 1);
     const uint32_t idesc = (1u << 4) | (1u << 7) | (1u << 10) | ((64u >> 3) << 17) | ((128u >> 4) << 24);
-    uint8_t* a_hi_p = smem + SM_A + g * 2 * A_BYTES;
-    const uint32_t a_hi = smem_u32(a_hi_p), a_lo = a_hi + A_BYTES;
-    const uint32_t d_tmem = tmem + uint32_t(64 * g);
-    const uint32_t taddr = d_tmem + (uint32_t((warp & 3) * 32) << 16);
-    const uint32_t row7 = uint32_t(tg) & 7u;
-    uint8_t* ahi_row = a_hi_p + (tg >> 3) * 1024 + row7 * 128;
-    uint8_t* alo_row = ahi_row + A_BYTES;
+    const uint32_t d_tmem = tmem + uint32_t(128 * g);  // columns: D [0,64), A hi [64,96), A lo [96,128)
+    const uint32_t a_tmem = d_tmem + 64u;
+    const uint32_t lane_base = uint32_t((warp & 3) * 32) << 16;
+    const uint32_t taddr = d_tmem + lane_base;          // this warp's lanes of D
+    const uint32_t taddr_a = a_tmem + lane_base;        // and of A
     uint32_t mma_phase = 0;
     for (uint64_t p = 0; p < my_pairs; ++p) {
       const uint64_t it = 2 * p + uint64_t(g);
@@ -526,40 +529,38 @@ __global__ void __launch_bounds__(THREADS, 1) k_fused_pass(const __grid_constant
                                   __uint_as_float(__float_as_uint(xx[i].y) ^ sg));
             }
           }
+          // A row (this lane): K = row (real parts) and 32 + row (imaginary parts), two bf16 per
+          // column, so rows 8*q0 .. 8*q0+15 are columns 4*q0 .. 4*q0+7 (re) and 16 + the same (im)
+          uint32_t hr[8], lr[8], hm[8], lm[8];
 #pragma unroll
-          for (int qq = 0; qq < 2; ++qq) {
-          const int q = q0 + qq;
-          const float2* x = xx + 8 * qq;
-          uint32_t hr[4], lr[4], hm[4], lm[4];
-#pragma unroll
-          for (int i = 0; i < 4; ++i) {
-            const float2 a = x[2 * i], c = x[2 * i + 1];
+          for (int i = 0; i < 8; ++i) {
+            const float2 a = xx[2 * i], c = xx[2 * i + 1];
             hr[i] = pack_bf16(a.x, c.x);
             hm[i] = pack_bf16(a.y, c.y);
             lr[i] = pack_bf16(a.x - lo_half(hr[i]), c.x - hi_half(hr[i]));
             lm[i] = pack_bf16(a.y - lo_half(hm[i]), c.y - hi_half(hm[i]));
           }
-          const uint32_t cre = uint32_t(q), cim = cre + 4u;  // 16-byte chunks of rows 8q..8q+7
-          *reinterpret_cast<uint4*>(ahi_row + ((cre ^ row7) << 4)) = make_uint4(hr[0], hr[1], hr[2], hr[3]);
-          *reinterpret_cast<uint4*>(alo_row + ((cre ^ row7) << 4)) = make_uint4(lr[0], lr[1], lr[2], lr[3]);
-          *reinterpret_cast<uint4*>(ahi_row + ((cim ^ row7) << 4)) = make_uint4(hm[0], hm[1], hm[2], hm[3]);
-          *reinterpret_cast<uint4*>(alo_row + ((cim ^ row7) << 4)) = make_uint4(lm[0], lm[1], lm[2], lm[3]);
-          }
+          tmem_st8(taddr_a + uint32_t(4 * q0), hr);
+          tmem_st8(taddr_a + uint32_t(16 + 4 * q0), hm);
+          tmem_st8(taddr_a + uint32_t(32 + 4 * q0), lr);
+          tmem_st8(taddr_a + uint32_t(48 + 4 * q0), lm);
         }
-        fence_async_smem();
+        asm volatile("tcgen05.wait::st.sync.aligned;" ::: "memory");
+        tc_fence_before();
         if (bar_any(1 + g, GROUP_THREADS, abort_sh)) break;
         if (tg == 0) {
           if (!mbar_wait(bar_ofull(sl), uint32_t((k / NOPSLOT) & 1))) fail(2);
           tc_fence_after();
           const uint32_t b_hi = smem_u32(smem + SM_B + sl * OPERAND_BYTES);
           const uint32_t b_lo = b_hi + OPERAND_BYTES / 2;
-          const uint64_t dah = sw128_desc(a_hi), dal = sw128_desc(a_lo), dbh = sw128_desc(b_hi), dbl = sw128_desc(b_lo);
+          const uint64_t dbh = sw128_desc(b_hi), dbl = sw128_desc(b_lo);
+          // K = 16 per MMA: eight A columns, two 16-byte steps of B
 #pragma unroll
-          for (int s = 0; s < 4; ++s) mma_bf16(d_tmem, dah + 2 * s, dbh + 2 * s, idesc, s > 0);
+          for (int s = 0; s < 4; ++s) mma_bf16_ta(d_tmem, a_tmem + 8u * s, dbh + 2 * s, idesc, s > 0);
 #pragma unroll
-          for (int s = 0; s < 4; ++s) mma_bf16(d_tmem, dal + 2 * s, dbh + 2 * s, idesc, 1);
+          for (int s = 0; s < 4; ++s) mma_bf16_ta(d_tmem, a_tmem + 32u + 8u * s, dbh + 2 * s, idesc, 1);
 #pragma unroll
-          for (int s = 0; s < 4; ++s) mma_bf16(d_tmem, dah + 2 * s, dbl + 2 * s, idesc, 1);
+          for (int s = 0; s < 4; ++s) mma_bf16_ta(d_tmem, a_tmem + 8u * s, dbl + 2 * s, idesc, 1);
           mma_commit(bar_mma(g));
           mma_commit(bar_oempty(sl));  // the slot is free once these MMAs have read it
           if (!mbar_wait(bar_mma(g), mma_phase)) fail(2);
