@@ -3,9 +3,9 @@
 // A persistent CTA per SM streams tiles of 2^12 complex64 amplitudes (32 KB)
 // through shared memory with the bulk-copy engine (cp.async.bulk, runs of
 // >= 128 contiguous bytes, three rotating tile buffers; warp 8).  The CTA
-// takes its tiles in pairs, and two warpgroups run the pass's program, one on
-// each tile of a pair, so that one group splits amplitudes while the other's
-// MMAs and read-back run.  The unitaries' B operands (16 KB each) stream from
+// takes its tiles in sets of three, and three warpgroups run the pass's
+// program, one on each tile of a set, so that a group splits amplitudes while
+// the others' MMAs and read-backs run.  The unitaries' B operands (16 KB each) stream from
 // L2 into three rotating slots (warp 9); both groups' tcgen05.commit free a
 // slot.  Per group and tile:
 //   unitary op: the tile as 32 rows (the unitary's 5 qubits) x 128 columns;
@@ -37,8 +37,8 @@ namespace fused {
 namespace {
 
 constexpr int GROUP_THREADS = 128;                       // one warpgroup runs the program on one tile
-constexpr int GROUPS = 2;                                // two tiles in flight per CTA
-constexpr int COMPUTE_THREADS = GROUPS * GROUP_THREADS;  // warps 0-7
+constexpr int GROUPS = 3;                                // three tiles in flight per CTA
+constexpr int COMPUTE_THREADS = GROUPS * GROUP_THREADS;  // warps 0-11
 constexpr int WARP_TILES = COMPUTE_THREADS / 32;         // warps 8-9: tile loads and stores
 constexpr int TILE_THREADS = 64;
 constexpr int WARP_OPS = WARP_TILES + 2;                 // warp 10: B operand images
@@ -46,14 +46,14 @@ constexpr int THREADS = COMPUTE_THREADS + TILE_THREADS + 32;
 constexpr int TILE = 1 << TILE_BITS;
 constexpr uint32_t TILE_BYTES = uint32_t(TILE) * 8u;
 constexpr int OPERAND_BYTES = 16384;  // B: bf16 hi (8 KB) + lo (8 KB)
-constexpr int NTILEBUF = 3;           // tile buffers rotating over the CTA's tiles
+constexpr int NTILEBUF = GROUPS + 2;  // tile buffers rotating over the CTA's tiles
 constexpr int NOPSLOT = 3;            // B operand slots rotating over the unitary uses
 constexpr int SM_B = 0;
 constexpr int SM_TILE0 = SM_B + NOPSLOT * OPERAND_BYTES;
 constexpr int SM_TOTAL = SM_TILE0 + NTILEBUF * int(TILE_BYTES);
 constexpr int SM_DYNAMIC = SM_TOTAL + 1008;  // the dynamic base is 16-byte aligned: slack to reach 1024
 // per group 128 columns: the accumulator D (64), the A operand's bf16 hi (32) and lo (32)
-constexpr uint32_t TMEM_COLS = 256;
+constexpr uint32_t TMEM_COLS = 512;  // 128 per group, rounded up to a power of two
 constexpr long long WAIT_CYCLES = 4000000000ll;  // about 2 s at 1.9 GHz
 constexpr int HALF = TILE_BITS / 2;              // 6-bit halves of the tile index
 
@@ -135,7 +135,8 @@ __device__ __forceinline__ void cp_async16(uint32_t dst, const void* src) {
 __device__ __forceinline__ void cp_async_arrive(uint32_t bar) {
   asm volatile("cp.async.mbarrier.arrive.noinc.shared::cta.b64 [%0];" ::"r"(bar) : "memory");
 }
-__device__ __forceinline__ void bar_tiles() { asm volatile("bar.sync 3, %0;" ::"n"(TILE_THREADS) : "memory"); }
+constexpr int BAR_TILES = 1 + GROUPS;  // named barriers: 1..GROUPS the groups, then the tile threads
+__device__ __forceinline__ void bar_tiles() { asm volatile("bar.sync %0, %1;" ::"n"(BAR_TILES), "n"(TILE_THREADS) : "memory"); }
 // A named barrier that also ORs a flag over its threads: every thread gets the
 // same answer, so a stop decided from it is uniform across the barrier's threads.
 __device__ __forceinline__ bool bar_any(int id, int count, bool v) {
@@ -172,10 +173,10 @@ __device__ __forceinline__ void mma_bf16_ta(uint32_t tmem_d, uint32_t tmem_a, ui
       "tcgen05.mma.cta_group::1.kind::f16 [%0], [%1], %2, %3, {%5, %6, %7, %8}, p;\n\t}"
       ::"r"(tmem_d), "r"(tmem_a), "l"(b), "r"(idesc), "r"(acc), "r"(0), "r"(0), "r"(0), "r"(0));
 }
-// eight 32-bit columns of this thread's TMEM lane
-__device__ __forceinline__ void tmem_st8(uint32_t taddr, const uint32_t (&v)[8]) {
-  asm volatile("tcgen05.st.sync.aligned.32x32b.x8.b32 [%0], {%1, %2, %3, %4, %5, %6, %7, %8};" ::"r"(taddr), "r"(v[0]),
-               "r"(v[1]), "r"(v[2]), "r"(v[3]), "r"(v[4]), "r"(v[5]), "r"(v[6]), "r"(v[7])
+// four 32-bit columns of this thread's TMEM lane
+__device__ __forceinline__ void tmem_st4(uint32_t taddr, const uint32_t (&v)[4]) {
+  asm volatile("tcgen05.st.sync.aligned.32x32b.x4.b32 [%0], {%1, %2, %3, %4};" ::"r"(taddr), "r"(v[0]), "r"(v[1]),
+               "r"(v[2]), "r"(v[3])
                : "memory");
 }
 __device__ __forceinline__ void mma_commit(uint32_t bar) {
@@ -286,7 +287,7 @@ __global__ void __launch_bounds__(THREADS, 1) k_fused_pass(const __grid_constant
   extern __shared__ uint8_t smem_raw[];
   uint8_t* smem = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
   // mbarriers: tile full[3], tile done[3], operand full[3], operand empty[3], mma[2]
-  __shared__ __align__(8) uint64_t bars[4 * 3 + GROUPS];
+  __shared__ __align__(8) uint64_t bars[2 * NTILEBUF + 2 * NOPSLOT + GROUPS];
   __shared__ uint32_t tmem_base_sh;
   __shared__ volatile int abort_sh;
   __shared__ uint8_t nongate[MAX_UNITARIES][TILE_BITS - GROUP_QUBITS];
@@ -298,21 +299,23 @@ __global__ void __launch_bounds__(THREADS, 1) k_fused_pass(const __grid_constant
 
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
   auto bar_tfull = [&](int b) { return smem_u32(&bars[b]); };
-  auto bar_tdone = [&](int b) { return smem_u32(&bars[3 + b]); };
-  auto bar_ofull = [&](int s) { return smem_u32(&bars[6 + s]); };
-  auto bar_oempty = [&](int s) { return smem_u32(&bars[9 + s]); };
-  auto bar_mma = [&](int g) { return smem_u32(&bars[12 + g]); };
+  auto bar_tdone = [&](int b) { return smem_u32(&bars[NTILEBUF + b]); };
+  auto bar_ofull = [&](int s) { return smem_u32(&bars[2 * NTILEBUF + s]); };
+  auto bar_oempty = [&](int s) { return smem_u32(&bars[2 * NTILEBUF + NOPSLOT + s]); };
+  auto bar_mma = [&](int g) { return smem_u32(&bars[2 * NTILEBUF + 2 * NOPSLOT + g]); };
   auto fail = [&](int code) {
     abort_sh = 1;
     atomicCAS(P.err, 0, code);
   };
 
   if (tid == 0) {
-    for (int i = 0; i < 3; ++i) {
+    for (int i = 0; i < NTILEBUF; ++i) {
       mbar_init(bar_tfull(i), TILE_THREADS);  // one cp.async arrival per tile thread
       mbar_init(bar_tdone(i), GROUP_THREADS);
+    }
+    for (int i = 0; i < NOPSLOT; ++i) {
       mbar_init(bar_ofull(i), 1);
-      mbar_init(bar_oempty(i), GROUPS);  // one commit per group
+      mbar_init(bar_oempty(i), GROUPS);  // one commit (or release) per group
     }
     for (int g = 0; g < GROUPS; ++g) mbar_init(bar_mma(g), 1);
     abort_sh = 0;
@@ -341,12 +344,15 @@ __global__ void __launch_bounds__(THREADS, 1) k_fused_pass(const __grid_constant
   __syncthreads();
   tc_fence_after();
   const uint32_t tmem = tmem_base_sh;
-  // tiles go in pairs, one per group: this CTA's it-th tile is tile_of(it), in buffer it % 3
-  const uint64_t npairs = (P.ntiles + 1) / 2;
-  const uint64_t my_pairs = npairs > blockIdx.x ? (npairs - 1 - blockIdx.x) / gridDim.x + 1 : 0;
-  const uint64_t my_tiles = 2 * my_pairs;
-  auto tile_of = [&](uint64_t it) { return 2 * (uint64_t(blockIdx.x) + (it >> 1) * gridDim.x) + (it & 1); };
-  // only a one-tile register leaves a pair half empty, always in the CTA's last pair
+  // tiles go in groups of GROUPS, one per warpgroup: this CTA's it-th tile is tile_of(it),
+  // in buffer it % NTILEBUF; only the register's last group of tiles can be short, and it
+  // is the last one of the CTA that takes it
+  const uint64_t nsets = (P.ntiles + GROUPS - 1) / GROUPS;
+  const uint64_t my_sets = nsets > blockIdx.x ? (nsets - 1 - blockIdx.x) / gridDim.x + 1 : 0;
+  const uint64_t my_tiles = uint64_t(GROUPS) * my_sets;
+  auto tile_of = [&](uint64_t it) {
+    return uint64_t(GROUPS) * (uint64_t(blockIdx.x) + (it / GROUPS) * gridDim.x) + (it % GROUPS);
+  };
   auto have = [&](uint64_t it) { return tile_of(it) < P.ntiles; };
   float2* tiles = reinterpret_cast<float2*>(smem + SM_TILE0);
 
@@ -375,7 +381,7 @@ __global__ void __launch_bounds__(THREADS, 1) k_fused_pass(const __grid_constant
     // wait (one thread) until the group is done with tile j; false (for all 64 threads alike) to stop
     auto wait_done = [&](uint64_t j) -> bool {
       if (pt == 0 && have(j) && !mbar_wait(bar_tdone(int(j % NTILEBUF)), uint32_t((j / NTILEBUF) & 1))) fail(3);
-      return !bar_any(3, TILE_THREADS, abort_sh);
+      return !bar_any(BAR_TILES, TILE_THREADS, abort_sh);
     };
     uint64_t it = 0;
     for (; it < my_tiles; ++it) {
@@ -395,8 +401,8 @@ __global__ void __launch_bounds__(THREADS, 1) k_fused_pass(const __grid_constant
     // copies of this thread still in flight land before the CTA exits
     asm volatile("cp.async.wait_all;" ::: "memory");
   } else if (warp == WARP_OPS) {
-    // ---------------- B operand images: use k = pair * nu + u, slot k % 3 ----------------
-    const uint64_t nk = my_pairs * uint64_t(P.nu);
+    // ---------------- B operand images: use k = set * nu + u, slot k % NOPSLOT ----------------
+    const uint64_t nk = my_sets * uint64_t(P.nu);
     uint64_t k = 0;
     for (; k < nk; ++k) {
       const int sl = int(k % NOPSLOT);
@@ -420,7 +426,7 @@ __global__ void __launch_bounds__(THREADS, 1) k_fused_pass(const __grid_constant
       for (uint64_t j = k >= NOPSLOT ? k - NOPSLOT : 0; j < k; ++j)
         if (lane == 0) mbar_wait(bar_ofull(int(j % NOPSLOT)), uint32_t((j / NOPSLOT) & 1));
   } else {
-    // ---------------- tensor-core program: group g on its tile of each pair ----------------
+    // ---------------- tensor-core program: group g on its tile of each set ----------------
     const int g = warp / 4, tg = tid & (GROUP_THREADS - 1);
     const uint32_t idesc = (1u << 4) | (1u << 7) | (1u << 10) | ((64u >> 3) << 17) | ((128u >> 4) << 24);
     const uint32_t d_tmem = tmem + uint32_t(128 * g);  // columns: D [0,64), A hi [64,96), A lo [96,128)
@@ -429,8 +435,8 @@ __global__ void __launch_bounds__(THREADS, 1) k_fused_pass(const __grid_constant
     const uint32_t taddr = d_tmem + lane_base;          // this warp's lanes of D
     const uint32_t taddr_a = a_tmem + lane_base;        // and of A
     uint32_t mma_phase = 0;
-    for (uint64_t p = 0; p < my_pairs; ++p) {
-      const uint64_t it = 2 * p + uint64_t(g);
+    for (uint64_t p = 0; p < my_sets; ++p) {
+      const uint64_t it = uint64_t(GROUPS) * p + uint64_t(g);
       const bool mine = have(it);
       const int b = int(it % NTILEBUF);
       if (mine && tg == 0 && !mbar_wait(bar_tfull(b), uint32_t((it / NTILEBUF) & 1))) fail(1);
@@ -490,7 +496,7 @@ __global__ void __launch_bounds__(THREADS, 1) k_fused_pass(const __grid_constant
         const uint64_t k = p * uint64_t(P.nu) + uint64_t(u);
         const int sl = int(k % NOPSLOT);
         if (!mine) {
-          // the pair's other half is empty: release the operand slot without using it
+          // this group has no tile in the set: release the operand slot without using it
           if (abort_sh) break;
           if (tg == 0) {
             if (!mbar_wait(bar_ofull(sl), uint32_t((k / NOPSLOT) & 1))) fail(2);
@@ -513,37 +519,37 @@ __global__ void __launch_bounds__(THREADS, 1) k_fused_pass(const __grid_constant
         bool scal = false;
         column_terms(s_terms, op.p0, op.p1, base, cb, smask, cth, scal);
 #pragma unroll
-        for (int q0 = 0; q0 < 4; q0 += 2) {
-          float2 xx[16];  // rows of two chunks, loaded before any store to A
+        for (int q = 0; q < 4; ++q) {
+          float2 xx[8];  // rows 8q..8q+7, loaded before any other work
 #pragma unroll
-          for (int i = 0; i < 16; ++i) xx[i] = T[lo8[i & 7] | hi4[q0 + (i >> 3)]];
+          for (int i = 0; i < 8; ++i) xx[i] = T[lo8[i] | hi4[q]];
           if (scal) {
 #pragma unroll
-            for (int i = 0; i < 16; ++i) xx[i] = cmulf(cth, xx[i]);
+            for (int i = 0; i < 8; ++i) xx[i] = cmulf(cth, xx[i]);
           }
           if (smask) {
 #pragma unroll
-            for (int i = 0; i < 16; ++i) {
-              const uint32_t sg = (smask << (31 - (8 * q0 + i))) & 0x80000000u;
+            for (int i = 0; i < 8; ++i) {
+              const uint32_t sg = (smask << (31 - (8 * q + i))) & 0x80000000u;
               xx[i] = make_float2(__uint_as_float(__float_as_uint(xx[i].x) ^ sg),
                                   __uint_as_float(__float_as_uint(xx[i].y) ^ sg));
             }
           }
           // A row (this lane): K = row (real parts) and 32 + row (imaginary parts), two bf16 per
-          // column, so rows 8*q0 .. 8*q0+15 are columns 4*q0 .. 4*q0+7 (re) and 16 + the same (im)
-          uint32_t hr[8], lr[8], hm[8], lm[8];
+          // column, so rows 8q .. 8q+7 are columns 4q .. 4q+3 (re) and 16 + the same (im)
+          uint32_t hr[4], lr[4], hm[4], lm[4];
 #pragma unroll
-          for (int i = 0; i < 8; ++i) {
+          for (int i = 0; i < 4; ++i) {
             const float2 a = xx[2 * i], c = xx[2 * i + 1];
             hr[i] = pack_bf16(a.x, c.x);
             hm[i] = pack_bf16(a.y, c.y);
             lr[i] = pack_bf16(a.x - lo_half(hr[i]), c.x - hi_half(hr[i]));
             lm[i] = pack_bf16(a.y - lo_half(hm[i]), c.y - hi_half(hm[i]));
           }
-          tmem_st8(taddr_a + uint32_t(4 * q0), hr);
-          tmem_st8(taddr_a + uint32_t(16 + 4 * q0), hm);
-          tmem_st8(taddr_a + uint32_t(32 + 4 * q0), lr);
-          tmem_st8(taddr_a + uint32_t(48 + 4 * q0), lm);
+          tmem_st4(taddr_a + uint32_t(4 * q), hr);
+          tmem_st4(taddr_a + uint32_t(16 + 4 * q), hm);
+          tmem_st4(taddr_a + uint32_t(32 + 4 * q), lr);
+          tmem_st4(taddr_a + uint32_t(48 + 4 * q), lm);
         }
         asm volatile("tcgen05.wait::st.sync.aligned;" ::: "memory");
         tc_fence_before();
@@ -806,8 +812,8 @@ extern "C" ncsim_status ncsim_sv_run_fused(ncsim_state* s, const ncsim_circuit* 
     NCSIM_CUDA(cudaMallocAsync(&d_err, sizeof(int), s->stream));
     NCSIM_CUDA(cudaMemsetAsync(d_err, 0, sizeof(int), s->stream));
     NCSIM_CUDA(cudaFuncSetAttribute(fused::k_fused_pass, cudaFuncAttributeMaxDynamicSharedMemorySize, fused::SM_DYNAMIC));
-    const uint64_t pairs = ((s->len >> fused::TILE_BITS) + 1) / 2;  // each CTA takes tiles two at a time
-    const unsigned grid = unsigned(std::min<uint64_t>(uint64_t(sm_count()), pairs));
+    const uint64_t sets = ((s->len >> fused::TILE_BITS) + fused::GROUPS - 1) / fused::GROUPS;  // a tile per warpgroup
+    const unsigned grid = unsigned(std::min<uint64_t>(uint64_t(sm_count()), sets));
     size_t m = 0, pi = 0;
     uint64_t gemm = 0;
     for (const fused::Segment& seg : dp->plan.segments) {

@@ -35,6 +35,22 @@ def test_fused_random_layers_match_fp64(nb, oracle, n, depth, seed):
     assert st.source_gates == depth * (n + n // 2) and st.passes >= 1
 
 
+def test_fused_reuses_tile_buffers(nb):
+    """n = 21: 512 tiles, so CTAs take more than one set of tiles and every
+    rotating tile buffer and operand slot is reused; against the complex128
+    plain path on the same circuit."""
+    n = 21
+    c = nb.Circuit.random_layers(n, 12, 4)
+    f = nb.GpuStateVector(n, nb.C64)
+    rec, st = f.run_fused(c, nb.StdRng(0))
+    ref = nb.GpuStateVector(n, nb.C128)
+    ref.run(c, nb.StdRng(0))
+    cmp = ref.compare(f)
+    assert cmp["infidelity"] < INFIDELITY
+    assert cmp["max_abs_diff"] < AMP_TOL * 2 ** (-(n - 12) / 2)
+    assert st.passes >= 2
+
+
 def test_fused_random_state_every_gate_kind(nb, oracle):
     n = 13
     r = np.random.default_rng(4)
