@@ -1,12 +1,14 @@
 // Precision form, device side: one kernel launch per pass.
 //
 // A persistent CTA per SM streams tiles of 2^12 complex64 amplitudes (32 KB)
-// through shared memory with the bulk-copy engine (cp.async.bulk, runs of
-// >= 128 contiguous bytes, three rotating tile buffers; warp 8).  The CTA
-// takes its tiles in sets of three, and three warpgroups run the pass's
-// program, one on each tile of a set, so that a group splits amplitudes while
-// the others' MMAs and read-backs run.  The unitaries' B operands (16 KB each) stream from
-// L2 into three rotating slots (warp 9); both groups' tcgen05.commit free a
+// through shared memory: two producer warps copy 16-byte chunks with cp.async
+// (completion on the tile's mbarrier through cp.async.mbarrier.arrive) into
+// four rotating tile buffers and write finished tiles back with 16-byte
+// stores.  The CTA takes its tiles in sets of three, and three warpgroups run
+// the pass's program, one on each tile of a set, so that a group splits
+// amplitudes while the others' MMAs and read-backs run.  The unitaries' B
+// operands (16 KB bf16 images each) stream from L2 into four rotating slots
+// (a third producer warp); each group's tcgen05.commit (or release) frees a
 // slot.  Per group and tile:
 //   unitary op: the tile as 32 rows (the unitary's 5 qubits) x 128 columns;
 //     each thread owns a column, splits its 32 amplitudes into bf16 hi/lo
@@ -17,12 +19,14 @@
 //     with R the real form [[Ur, -Ui], [Ui, Ur]] of the fused unitary (bf16
 //     hi/lo images made on the host); each thread reads its D row back
 //     (tcgen05.ld) and writes the 32 new amplitudes into the tile;
-//   diagonal op: the tile index splits into two 6-bit halves; per tile, the
-//     active terms are folded into a 64-entry phase table per half and a
-//     parity table for the cross-half sign terms (CZ-like), so an amplitude
-//     costs two table reads and a parity, whatever the number of terms.
+//   diagonal op: reduced, where it can be, to a phase per column and a sign
+//     mask over the rows of a neighbouring unitary and applied in that
+//     unitary's split or read-back; otherwise the tile index splits into two
+//     6-bit halves, the active terms fold into a 64-entry phase table per half
+//     and a parity table for cross-half signs, and one sweep applies them.
 // Every wait on an mbarrier is bounded in time: on timeout the CTA records an
-// error code, stops, waits for its own copies and frees its TMEM.
+// error code and every role stops at its next uniform decision point, waits
+// for its own copies and frees its TMEM.
 #include <cuda_bf16.h>
 
 #include "engine.cuh"
@@ -46,8 +50,8 @@ constexpr int THREADS = COMPUTE_THREADS + TILE_THREADS + 32;
 constexpr int TILE = 1 << TILE_BITS;
 constexpr uint32_t TILE_BYTES = uint32_t(TILE) * 8u;
 constexpr int OPERAND_BYTES = 16384;  // B: bf16 hi (8 KB) + lo (8 KB)
-constexpr int NTILEBUF = GROUPS + 2;  // tile buffers rotating over the CTA's tiles
-constexpr int NOPSLOT = 3;            // B operand slots rotating over the unitary uses
+constexpr int NTILEBUF = GROUPS + 1;  // tile buffers rotating over the CTA's tiles (one loading ahead)
+constexpr int NOPSLOT = 4;            // B operand slots rotating over the unitary uses
 constexpr int SM_B = 0;
 constexpr int SM_TILE0 = SM_B + NOPSLOT * OPERAND_BYTES;
 constexpr int SM_TOTAL = SM_TILE0 + NTILEBUF * int(TILE_BYTES);
