@@ -368,6 +368,61 @@ def trajectory_bench(nb, args, dist, peak, peak_kind):
     return out
 
 
+def config_rates(nb, peak, peak_kind):
+    """The other sized workloads of the path, plain complex128 kernels, one GPU:
+    C0 (n = 20, depth 40, with its readouts), C1 (n = 30, depth 20, M on the
+    last 4 qubits) and C3 (n = 31: H on qubits 0..15, 2000 permutation and
+    diagonal gates).  Gates/s from CUDA events on the state's stream; %HBM from
+    the launch profiler's algorithmic bytes over a separate profiled run."""
+    out = {}
+
+    def measure(name, n, circuit, runs, extra=None):
+        s = nb.GpuStateVector(n)
+        rng = nb.StdRng(11)
+        if runs:
+            s.run(circuit, rng)  # warm-up (and the gate graphs' capture)
+            s.timer_start()
+            for _ in range(runs):
+                s.run(circuit, rng)
+            ms = s.timer_stop() / runs
+        s.profile(True)
+        if not runs:  # one profiled run only (long circuits: plain kernels of milliseconds each)
+            s.timer_start()
+        s.run(circuit, rng)
+        if not runs:
+            ms = s.timer_stop()
+        prof = s.profile_read()
+        s.profile(False)
+        pbytes = sum(v["bytes"] for v in prof.values())
+        pms = sum(v["ms"] for v in prof.values())
+        gates = circuit.num_gates
+        r = {"n": n, "gates": gates, "ms_per_run": ms, "gates_per_s": gates / (ms / 1e3),
+             "hbm_frac_of_kernel_time": round(pbytes / (pms / 1e3) / 1e9 / peak, 4) if pms else None,
+             "peak_kind": peak_kind,
+             "kernels": {k: {"launches": v["launches"], "ms": round(v["ms"], 2),
+                             "GBps": round(v["bytes"] / max(v["ms"], 1e-9) / 1e6, 1)} for k, v in prof.items()}}
+        if extra:
+            r.update(extra(s))
+        out[name] = r
+        del s
+
+    def c0_readouts(s):
+        n = 20
+        t0 = time.perf_counter()
+        z = s.expectation(nb.Pauli.from_string(n, "Z0*Z1"))
+        x = s.expectation(nb.Pauli.from_string(n, "X0*X5*Y9"))
+        smp = s.sample(nb.StdRng(2), 4096)
+        ridx = nb.StdRng(3)
+        amps = s.amplitudes_at([ridx.gen_range(0, 1 << n) for _ in range(64)])
+        return {"readouts_ms": (time.perf_counter() - t0) * 1e3, "readouts": "<Z0 Z1>, <X0 X5 Y9>, 4096 shots, "
+                "64 amplitudes", "z0z1": z.real, "x0x5y9": x.real, "shots": int(smp.size), "amplitudes": len(amps)}
+
+    measure("C0", 20, nb.Circuit.random_layers(20, 40, 1), 10, c0_readouts)
+    measure("C1", 30, nb.Circuit.random_layers(30, 20, 1, 0.0, 26, 30), 2)
+    measure("C3", 31, nb.Circuit.reversible(31, 2000, 1), 0)
+    return out
+
+
 def timed_runs(nb, state, circuit, steps: int, warmup: int, fused: bool, dist):
     """Each step runs the circuit on the register the previous steps left.
 
@@ -386,11 +441,15 @@ def timed_runs(nb, state, circuit, steps: int, warmup: int, fused: bool, dist):
         step()
     state.synchronize()
     barrier(dist)
-    state.profile(True)
     state.timer_start()
     for _ in range(steps):
         step()
     ms = state.timer_stop()
+    # one more step with the launch profiler on, for the per-kernel times and algorithmic
+    # bytes of the roofline (its event records are kept out of the timed steps)
+    state.profile(True)
+    step()
+    state.synchronize()
     prof = state.profile_read()
     state.profile(False)
     return ms, prof
@@ -413,6 +472,7 @@ def main():
     ap.add_argument("--no-trajectories", action="store_true")
     ap.add_argument("--traj-launch", default="",
                     help="CTAS_PER_SM,BUFFERS: a fixed launch configuration of the batch kernel (default: tuned)")
+    ap.add_argument("--no-configs", action="store_true", help="skip the C0, C1 and C3 plain-path rates")
     ap.add_argument("--no-headline", action="store_true",
                     help="only the trajectories/s part (for profiling the batch kernel)")
     args = ap.parse_args()
@@ -551,6 +611,8 @@ def main():
         with ClockSampler() as tclk:
             result["trajectories"] = trajectory_bench(nb, args, dist, peak, peak_kind)
         result["trajectories"]["clocks"] = tclk.summary()
+    if not args.no_configs and WORLD == 1:
+        result["configs"] = config_rates(nb, peak, peak_kind)
 
     clocks = clk.summary() if clk else None
     line = {
@@ -580,7 +642,8 @@ def main():
         "cpu_baseline": cpu,
         "e2e": e2e,
         "clocks": clocks,
-        "gpu_launches": launches,
+        "gpu_launches": launches * args.steps,  # the profiled step launches what each timed step does
+        "gpu_launches_per_step": launches,
     }
     line.update(result)
     if RANK == 0:

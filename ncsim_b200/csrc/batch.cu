@@ -233,7 +233,11 @@ __device__ __forceinline__ void apply_ops(Regs& r, uint32_t fixed, uint32_t tile
     const uint32_t hdr = op->hdr;
     const uint32_t code = hdr & 7u, la = (hdr >> 3) & 127u, lb = (hdr >> 10) & 127u;
     if (code == OP_CZ) {
-      neg ^= loc_mask(la, fixed, tile) & loc_mask(lb, fixed, tile);
+      // the register operands' patterns come multiplied; a fixed or tile operand's bit masks them
+      uint32_t m = __float_as_uint(op->v[0]);
+      if ((la >> 5) != LOC_REG) m &= 0u - ((((la >> 5) == LOC_FIXED ? fixed : tile) >> (la & 31u)) & 1u);
+      if ((lb >> 5) != LOC_REG) m &= 0u - ((((lb >> 5) == LOC_FIXED ? fixed : tile) >> (lb & 31u)) & 1u);
+      neg ^= m;
       continue;
     }
     const float4 u0 = reinterpret_cast<const float4*>(op->v)[0];

@@ -6,6 +6,7 @@
 #include <array>
 #include <atomic>
 #include <cmath>
+#include <cstring>
 #include <thread>
 
 namespace ncsim::batch {
@@ -444,7 +445,14 @@ void compile_one(const Trajectory& t, const PlanKnobs& kn, Local& L) {
         uint32_t la = loc(o.a), lb = 0;
         if (o.code == OP_CZ || o.code == OP_CPHASE) lb = loc(o.b);
         d.hdr = o.code | (la << 3) | (lb << 10);
-        if (o.code == OP_GATE) {
+        if (o.code == OP_CZ) {
+          // the register operands' patterns, multiplied here; the device masks in the others' bits
+          static const uint32_t pat[REG_BITS] = {0xAAAAAAAAu, 0xCCCCCCCCu, 0xF0F0F0F0u, 0xFF00FF00u, 0xFFFF0000u};
+          uint32_t m = 0xFFFFFFFFu;
+          if ((la >> 5) == LOC_REG) m &= pat[la & 31u];
+          if ((lb >> 5) == LOC_REG) m &= pat[lb & 31u];
+          std::memcpy(&d.v[0], &m, 4);
+        } else if (o.code == OP_GATE) {
           for (int k = 0; k < 4; ++k) {
             d.v[2 * k] = f32(o.m[k].re);
             d.v[2 * k + 1] = f32(o.m[k].im);

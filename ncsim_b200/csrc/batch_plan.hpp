@@ -50,7 +50,8 @@ enum : uint32_t { PASS_ZERO_INIT = 1, PASS_ACCUM = 2, PASS_NO_WRITE = 4 };
 // LOC_REG index = register bit (0..4), LOC_FIXED = bit of the thread's tile
 // index, LOC_TILE = bit of the tile number.  v: GATE 2x2 row-major
 // (re, im); BGATE (s w, s) for s [[1, w], [1, -w]], s = 1/sqrt2, |w| = 1;
-// DIAG (d0, d1); CPHASE the phase applied where both bits are 1.
+// DIAG (d0, d1); CPHASE the phase applied where both bits are 1; CZ: v[0]'s
+// bits are the product of the register operands' 32-amplitude patterns.
 struct alignas(16) DevOp {
   float v[8];
   uint32_t hdr;
