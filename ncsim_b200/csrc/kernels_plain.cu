@@ -151,6 +151,42 @@ __device__ __forceinline__ uint64_t tile_base(uint64_t t, const TileGeom& g) {
   return v;
 }
 
+// Tile staging for the shared-memory tile kernels.  Element e of a tile is
+// threadIdx.x + r*blockDim.x; its global offset and gate pattern are ORs of a
+// per-thread part and a per-round part (the bit deposit sends each bit of e
+// to its own position), computed once per block.  The loads are cp.async
+// copies straight into shared memory, all of a thread's rounds in flight at
+// once (no register staging).
+struct TileRounds {
+  uint64_t toff;   // offset of threadIdx.x
+  uint32_t tx;     // gate pattern of threadIdx.x
+  uint32_t nr;     // rounds
+};
+
+__device__ __forceinline__ TileRounds tile_rounds(const TileGeom& g, uint64_t* roff, uint32_t* rx) {
+  const uint32_t tsz = 1u << g.T;
+  const uint32_t nr = (tsz + blockDim.x - 1) / blockDim.x;
+  if (threadIdx.x < nr) {
+    roff[threadIdx.x] = tile_offset(threadIdx.x * blockDim.x, g);
+    rx[threadIdx.x] = tile_local_x(threadIdx.x * blockDim.x, g);
+  }
+  return TileRounds{tile_offset(threadIdx.x, g), tile_local_x(threadIdx.x, g), nr};
+}
+
+template <class R>
+__device__ __forceinline__ void tile_load_async(V<R>* tile, const V<R>* src, const uint64_t* roff, uint32_t nr, uint32_t tsz) {
+  for (uint32_t r = 0; r < nr; ++r) {
+    const uint32_t e = threadIdx.x + r * blockDim.x;
+    if (e >= tsz) break;
+    const uint32_t d = static_cast<uint32_t>(__cvta_generic_to_shared(tile + e));
+    if constexpr (sizeof(V<R>) == 16)
+      asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(d), "l"(src + roff[r]) : "memory");
+    else
+      asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(d), "l"(src + roff[r]) : "memory");
+  }
+  asm volatile("cp.async.commit_group;\ncp.async.wait_group 0;\n" ::: "memory");
+}
+
 constexpr int MAX_DENSE_K = 5;  // matrices up to 32x32 travel in the kernel parameters
 
 template <class R>
@@ -174,22 +210,27 @@ __global__ void __launch_bounds__(THREADS) k_dense_tile(V<R>* __restrict__ a, ui
     for (int j = 0; j < g.k; ++j) o |= ((uint32_t(b) >> j) & 1u) << g.pos[j];
     pat[b] = o;
   }
+  __shared__ uint64_t roff[32];
+  __shared__ uint32_t rx[32];
+  const TileRounds tr = tile_rounds(g, roff, rx);
   uint32_t gtile = 0;
   for (int j = 0; j < g.k; ++j) gtile |= 1u << g.pos[j];
   for (uint64_t t = blockIdx.x; t < ntiles; t += gridDim.x) {
-    const uint64_t base = tile_base(t, g);
+    V<R>* amp = a + (tile_base(t, g) | tr.toff);
     __syncthreads();
-    for (uint32_t e = threadIdx.x; e < tsz; e += blockDim.x) tile[e] = a[base | tile_offset(e, g)];
+    tile_load_async<R>(tile, amp, roff, tr.nr, tsz);
     __syncthreads();
-    for (uint32_t e = threadIdx.x; e < tsz; e += blockDim.x) {
-      uint32_t row = tile_local_x(e, g);
-      uint32_t r = e & ~gtile;
+    for (uint32_t q = 0; q < tr.nr; ++q) {
+      const uint32_t e = threadIdx.x + q * blockDim.x;
+      if (e >= tsz) break;
+      const uint32_t row = tr.tx | rx[q];
+      const uint32_t r = e & ~gtile;
       const V<R>* mr = mat + row * gd;
       V<R> acc;
       acc.x = 0;
       acc.y = 0;
       for (int b = 0; b < gd; ++b) acc = cfma(mr[b], tile[r | pat[b]], acc);
-      a[base | tile_offset(e, g)] = acc;
+      amp[roff[q]] = acc;
     }
   }
 }
@@ -317,7 +358,7 @@ template <class R>
 __global__ void __launch_bounds__(THREADS) k_perm_tile(V<R>* __restrict__ a, uint64_t ntiles, const __grid_constant__ PermParams<R> PP) {
   const PermParams<R>* P = &PP;
   extern __shared__ __align__(16) unsigned char smem_raw[];
-  const TileGeom g = P->g;
+  const TileGeom& g = P->g;
   const int gd = 1 << g.k;
   const uint32_t tsz = 1u << g.T;
   V<R>* tile = reinterpret_cast<V<R>*>(smem_raw);
@@ -332,21 +373,26 @@ __global__ void __launch_bounds__(THREADS) k_perm_tile(V<R>* __restrict__ a, uin
     ph[y] = P->ph[y];
     unit[y] = P->unit[y];
   }
+  __shared__ uint64_t roff[32];
+  __shared__ uint32_t rx[32];
+  const TileRounds tr = tile_rounds(g, roff, rx);
   uint32_t gtile = 0;
   for (int j = 0; j < g.k; ++j) gtile |= 1u << g.pos[j];
   for (uint64_t t = blockIdx.x; t < ntiles; t += gridDim.x) {
-    const uint64_t base = tile_base(t, g);
+    V<R>* amp = a + (tile_base(t, g) | tr.toff);
     __syncthreads();
-    for (uint32_t e = threadIdx.x; e < tsz; e += blockDim.x) tile[e] = a[base | tile_offset(e, g)];
+    tile_load_async<R>(tile, amp, roff, tr.nr, tsz);
     __syncthreads();
-    for (uint32_t e = threadIdx.x; e < tsz; e += blockDim.x) {
-      uint32_t y = tile_local_x(e, g);
-      V<R> v = tile[(e & ~gtile) | src[y]];
-      a[base | tile_offset(e, g)] = unit[y] ? v : cmul(ph[y], v);
+#pragma unroll 4
+    for (uint32_t q = 0; q < tr.nr; ++q) {
+      const uint32_t e = threadIdx.x + q * blockDim.x;
+      if (e >= tsz) break;
+      const uint32_t y = tr.tx | rx[q];
+      const V<R> v = tile[(e & ~gtile) | src[y]];
+      amp[roff[q]] = unit[y] ? v : cmul(ph[y], v);
     }
   }
 }
-
 // ---------------------------------------------------------------------------
 // Diagonal(PhasePoly) evaluated from the basis index
 // ---------------------------------------------------------------------------
@@ -435,6 +481,95 @@ __global__ void __launch_bounds__(THREADS) k_phasepoly(V<R>* __restrict__ a, uin
       if (!s_one) c = cmul(scalar, c);
     }
     a[i] = cmul(c, v);
+  }
+}
+
+// Bit-sliced form for exponents of at most 8 bits (a phasor table).  A warp
+// owns 1024 consecutive indices; lane l holds the 32 indices chunk|j<<5|l,
+// j = 0..31, and evaluates each parity for all of them at once as a 32-bit
+// mask over j: parity(p & i) = parity(p_rest & (chunk|l)) ^ parity(p_j & j),
+// the second factor a fixed mask per parity.  Terms are ANDs of those masks,
+// and f = constant + sum coeff*term is accumulated mod 2^B in B bit planes
+// (a ripple-carry add of the warp-uniform coefficient under the term mask).
+// The per-amplitude work is then an extraction of B bits, a table lookup and
+// the multiply; the term evaluation costs about 1/32 of the scalar form.
+template <int B>
+__device__ __forceinline__ void sliced_add(uint32_t (&F)[B], uint32_t m, uint32_t c) {
+  uint32_t carry = 0;  // always a subset of m
+#pragma unroll
+  for (int k = 0; k < B; ++k) {
+    const uint32_t f = F[k];
+    if ((c >> k) & 1u) {
+      F[k] = f ^ m ^ carry;
+      carry = m & (f | carry);
+    } else {
+      F[k] = f ^ carry;
+      carry = f & carry;
+    }
+  }
+}
+
+__host__ __device__ __forceinline__ uint32_t sliced_pattern(uint32_t m5) {
+  // bit j of the result = parity(m5 & j), j = 0..31
+  const uint32_t pat[5] = {0xAAAAAAAAu, 0xCCCCCCCCu, 0xF0F0F0F0u, 0xFF00FF00u, 0xFFFF0000u};
+  uint32_t r = 0;
+  for (int b = 0; b < 5; ++b)
+    if ((m5 >> b) & 1u) r ^= pat[b];
+  return r;
+}
+
+template <class R, int B>
+__global__ void __launch_bounds__(THREADS) k_phasepoly_sliced(V<R>* __restrict__ a, uint64_t len, const __grid_constant__ PolyParams<R> PP) {
+  const PolyParams<R>* P = &PP;
+  __shared__ uint64_t prest[MAX_POLY_PARITIES];  // parity mask outside index bits 5..9
+  __shared__ uint32_t pj[MAX_POLY_PARITIES];     // its values over j
+  __shared__ uint16_t start[MAX_POLY_TERMS + 1];
+  __shared__ uint32_t coeff[MAX_POLY_TERMS];
+  __shared__ V<R> table[1 << B];
+  const int nt = P->nterms;
+  for (int i = threadIdx.x; i <= nt; i += blockDim.x) start[i] = P->start[i];
+  for (int i = threadIdx.x; i < nt; i += blockDim.x) coeff[i] = P->coeff[i];
+  const int npar = P->start[nt];
+  for (int i = threadIdx.x; i < npar; i += blockDim.x) {
+    const uint64_t p = P->par[i];
+    prest[i] = p & ~uint64_t(0x3E0);
+    pj[i] = sliced_pattern(uint32_t(p >> 5) & 31u);
+  }
+  for (int i = threadIdx.x; i < (1 << B); i += blockDim.x) table[i] = P->table[i];
+  __syncthreads();
+  const uint64_t constant = P->constant;
+  const uint32_t lane = threadIdx.x & 31;
+  const uint64_t nchunks = len >> 10;
+  const uint64_t nwarps = (uint64_t(gridDim.x) * blockDim.x) >> 5;
+  for (uint64_t ch = (uint64_t(blockIdx.x) * blockDim.x + threadIdx.x) >> 5; ch < nchunks; ch += nwarps) {
+    const uint64_t idx = (ch << 10) | lane;
+    uint32_t F[B];
+#pragma unroll
+    for (int k = 0; k < B; ++k) F[k] = 0u - uint32_t((constant >> k) & 1);
+    for (int t = 0; t < nt; ++t) {
+      uint32_t m = ~0u;
+      const int l1 = start[t + 1];
+      for (int l = start[t]; l < l1; ++l) m &= pj[l] ^ (0u - (uint32_t(__popcll(prest[l] & idx)) & 1u));
+      sliced_add<B>(F, m, coeff[t]);
+    }
+    V<R>* p = a + idx;
+#pragma unroll
+    for (int jb = 0; jb < 32; jb += 8) {
+      V<R> v[8];
+#pragma unroll
+      for (int u = 0; u < 8; ++u) v[u] = p[(jb + u) << 5];
+#pragma unroll
+      for (int u = 0; u < 8; ++u) {
+        const int j = jb + u;
+        uint32_t f = 0;
+#pragma unroll
+        for (int k = 0; k < B; ++k) f |= ((F[k] >> j) & 1u) << k;
+        if (is_zero(v[u])) continue;
+        const V<R> c = table[f];
+        if (c.x == R(1) && c.y == R(0)) continue;
+        p[j << 5] = cmul(c, v[u]);
+      }
+    }
   }
 }
 
@@ -1032,6 +1167,20 @@ void launch_perm_table(ncsim_state* s, const std::vector<uint32_t>& qubits, cons
   });
 }
 
+template <class R>
+void launch_phasepoly_sliced(uint32_t bits, unsigned grid, cudaStream_t st, V<R>* a, uint64_t len, const PolyParams<R>& P) {
+  switch (bits) {
+    case 1: k_phasepoly_sliced<R, 1><<<grid, THREADS, 0, st>>>(a, len, P); break;
+    case 2: k_phasepoly_sliced<R, 2><<<grid, THREADS, 0, st>>>(a, len, P); break;
+    case 3: k_phasepoly_sliced<R, 3><<<grid, THREADS, 0, st>>>(a, len, P); break;
+    case 4: k_phasepoly_sliced<R, 4><<<grid, THREADS, 0, st>>>(a, len, P); break;
+    case 5: k_phasepoly_sliced<R, 5><<<grid, THREADS, 0, st>>>(a, len, P); break;
+    case 6: k_phasepoly_sliced<R, 6><<<grid, THREADS, 0, st>>>(a, len, P); break;
+    case 7: k_phasepoly_sliced<R, 7><<<grid, THREADS, 0, st>>>(a, len, P); break;
+    default: k_phasepoly_sliced<R, 8><<<grid, THREADS, 0, st>>>(a, len, P); break;
+  }
+}
+
 void launch_phasepoly(ncsim_state* s, const PolyTerms& t) {
   const int nt = int(t.coeffs.size());
   if (nt > MAX_POLY_TERMS || t.parities.size() > size_t(MAX_POLY_PARITIES))
@@ -1051,7 +1200,13 @@ void launch_phasepoly(ncsim_state* s, const PolyTerms& t) {
     P->use_table = !t.root_table.empty();
     for (size_t i = 0; i < t.root_table.size() && i < 256; ++i) P->table[i] = cv<R>(t.root_table[i]);
     ProfScope ps(s, K_PHASEPOLY, full_bytes(s));
-    k_phasepoly<R><<<grid_for(s->len, THREADS), THREADS, 0, s->stream>>>(amp_of<R>(s), s->len, *P);
+    const bool sliced = P->use_table && t.bits >= 1 && t.bits <= 8 && s->len >= 1024;
+    if (sliced) {
+      const unsigned grid = grid_for(s->len >> 5, THREADS);
+      launch_phasepoly_sliced<R>(t.bits, grid, s->stream, amp_of<R>(s), s->len, *P);
+    } else {
+      k_phasepoly<R><<<grid_for(s->len, THREADS), THREADS, 0, s->stream>>>(amp_of<R>(s), s->len, *P);
+    }
     delete P;
     NCSIM_LAUNCHED("phasepoly");
   });

@@ -125,11 +125,14 @@ def test_monomial_and_diagonal_gates_from_text(nb, oracle):
     assert np.abs(a - b).max() < TOL
 
 
-@pytest.mark.parametrize("bits,scalar", [(3, (0, 0, 0)), (5, (1, 3, 2)), (12, (0, 0, 0)), (12, (-2, 5, 3))])
-def test_phase_polynomial_from_the_bit_index(nb, oracle, bits, scalar):
+@pytest.mark.parametrize("bits,scalar,precision", [(3, (0, 0, 0), 0), (5, (1, 3, 2), 0), (8, (0, 1, 3), 0), (1, (0, 0, 0), 1),
+                                                   (3, (2, 1, 2), 1), (12, (0, 0, 0), 0), (12, (-2, 5, 3), 0)])
+def test_phase_polynomial_from_the_bit_index(nb, oracle, bits, scalar, precision):
+    """Exponents of at most 8 bits take the bit-sliced kernel (a warp per
+    1024 amplitudes); wider ones the per-amplitude form."""
     n = 12
     rng = np.random.default_rng(bits)
-    g, o = pair(nb, oracle, n, 4)
+    g, o = pair(nb, oracle, n, 4, precision)
     qs = [int(q) for q in rng.permutation(n)]
     terms = []
     for _ in range(25):
@@ -153,7 +156,8 @@ def test_phase_polynomial_from_the_bit_index(nb, oracle, bits, scalar):
     f %= 1 << bits
     s2, sp, sb = scalar
     factor = (math.sqrt(2) ** s2) * np.exp(2j * np.pi * sp / (1 << sb)) * np.exp(2j * np.pi * f / (1 << bits))
-    assert np.abs(g.to_vector() - v * factor).max() < TOL
+    tol = TOL * abs(math.sqrt(2) ** s2) if precision == 0 else TOL_C64 * max(1.0, math.sqrt(2) ** s2)
+    assert np.abs(g.to_vector() - v * factor).max() < tol
 
 
 def test_paulis_readouts_and_projections(nb, oracle):
@@ -296,6 +300,20 @@ def test_reversible_family_dense(nb, oracle):
     a = g.to_vector()
     assert np.array_equal(np.flatnonzero(a), idx.astype(np.int64))
     assert np.abs(a[idx.astype(np.int64)] - amp).max() < TOL
+
+
+@pytest.mark.parametrize("precision", [0, 1])
+def test_reversible_family_on_a_dense_state(nb, oracle, precision):
+    """Every amplitude nonzero: the 40-term diagonals and the 8-qubit
+    monomials of the reversible family act on all 2^n entries (the bit-sliced
+    phase-polynomial kernel and the tiled permutation kernel)."""
+    n = 16
+    text = oracle.reversible_circuit_text(n, 150, 9)
+    g, o = pair(nb, oracle, n, 12, precision)
+    g.run(nb.Circuit.parse(text), nb.StdRng(0))
+    o.run(oracle.Circuit(text), oracle.StdRng(0))
+    tol = TOL if precision == 0 else TOL_C64 * 2 ** (-n / 2) * 16
+    assert maxerr(g, o) < tol
 
 
 def test_complex64_storage_plain_path(nb, oracle):
