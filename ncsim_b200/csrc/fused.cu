@@ -60,6 +60,8 @@ constexpr int SM_DYNAMIC = SM_TOTAL + 1008;  // the dynamic base is 16-byte alig
 constexpr uint32_t TMEM_COLS = 512;  // 128 per group, rounded up to a power of two
 constexpr long long WAIT_CYCLES = 4000000000ll;  // about 2 s at 1.9 GHz
 constexpr int HALF = TILE_BITS / 2;              // 6-bit halves of the tile index
+constexpr int COL_BITS = TILE_BITS - GROUP_QUBITS;  // a unitary's column index: the tile bits outside its qubits
+constexpr int MAX_CHUNKS = 48;                      // column-term chunks per pass
 
 enum TermClass : uint8_t { T_LOW = 0, T_HIGH = 1, T_CROSS_SIGN = 2, T_GENERIC = 3 };
 
@@ -69,8 +71,8 @@ struct OpDesc {
   // terms [t0, t1) sorted by class: low half [t0,tl), high half [tl,th),
   // cross-half signs [th,tc), the rest [tc,t1)
   uint16_t t0, tl, th, tc, t1;
-  uint16_t p0, p1;  // unitary: the preceding terms op's terms, applied while splitting
-  uint16_t q0, q1;  // unitary: the following terms op's terms, applied while reading back
+  uint8_t pc0, pc1;  // unitary: chunks of the preceding terms op, applied while splitting
+  uint8_t qc0, qc1;  // unitary: chunks of the following terms op, applied while reading back
 };
 
 struct TermDesc {
@@ -78,6 +80,21 @@ struct TermDesc {
   uint32_t tmask;  // tile-local bits (for a split-applied term: the unitary's non-gate bits)
   float cr, ci;
   uint32_t rowpat;  // split-applied sign term: the rows (gate index) whose sign flips; 0: a phase on the column
+};
+
+// Up to 32 terms of a diagonal op applied by a unitary's split or read-back,
+// as bit masks over the chunk's terms (bit t = term t0 + t).  A term is active
+// on a column when its bits outside the tile are set in the tile's base (a
+// per-tile ballot) and its column bits are set in the column index; active
+// terms then flip row signs (row[j]: rows with gate bit j set), negate the
+// column (neg) or multiply it by their phase (gen).
+struct ColChunk {
+  uint32_t need[COL_BITS];     // terms whose condition includes column bit j
+  uint32_t row[GROUP_QUBITS];  // sign terms on the rows with gate bit j set
+  uint32_t neg;                // -1 on the whole column
+  uint32_t gen;                // other phases on the whole column
+  uint16_t t0;
+  uint16_t cnt;
 };
 
 struct PassParams {
@@ -89,8 +106,10 @@ struct PassParams {
   uint8_t win[TILE_BITS];      // window qubits, ascending (tile-local bit j = win[j])
   int nops, nu;
   uint8_t pos[MAX_UNITARIES][GROUP_QUBITS];  // tile-local positions of each unitary's qubits
+  int nchunks;
   OpDesc ops[MAX_OPS];
   TermDesc terms[MAX_TERMS];
+  ColChunk chunks[MAX_CHUNKS];
 };
 
 // ---- PTX wrappers ----
@@ -266,18 +285,26 @@ __device__ __forceinline__ float2 term_phase(uint32_t e, const OpDesc& op, uint6
   return c;
 }
 
-// The terms [k0, k1) of a diagonal op applied by a unitary's split or read-back,
-// for the column whose non-gate tile bits are cb: sign terms on one gate qubit
-// flip rows (rowpat), the others multiply the whole column.
-__device__ __forceinline__ void column_terms(const TermDesc* terms, int k0, int k1, uint64_t base, uint32_t cb,
-                                             uint32_t& smask, float2& cth, bool& scal) {
-  for (int k = k0; k < k1; ++k) {
-    const TermDesc tm = terms[k];
-    if ((base & tm.cmask) != tm.cmask || (cb & tm.tmask) != tm.tmask) continue;
-    if (tm.rowpat) {
-      smask ^= tm.rowpat;
-    } else {
-      cth = cmulf(cth, make_float2(tm.cr, tm.ci));
+// The chunks [c0, c1) of a diagonal op applied by a unitary's split or read-back,
+// for column tg of that unitary (act: the chunks' terms active on this tile):
+// a sign mask over the 32 rows and a phase for the whole column.
+__device__ __forceinline__ void column_chunks(const ColChunk* chunks, const uint32_t* act, int c0, int c1, uint32_t tg,
+                                              const TermDesc* terms, uint32_t& smask, float2& cth, bool& scal) {
+  const uint32_t rowpat[GROUP_QUBITS] = {0xAAAAAAAAu, 0xCCCCCCCCu, 0xF0F0F0F0u, 0xFF00FF00u, 0xFFFF0000u};
+  for (int c = c0; c < c1; ++c) {
+    const ColChunk& ch = chunks[c];
+    uint32_t a = act[c];
+#pragma unroll
+    for (int j = 0; j < COL_BITS; ++j) a &= ((tg >> j) & 1u) ? ~0u : ~ch.need[j];
+#pragma unroll
+    for (int j = 0; j < GROUP_QUBITS; ++j) smask ^= rowpat[j] & (0u - (uint32_t(__popc(a & ch.row[j])) & 1u));
+    if (__popc(a & ch.neg) & 1) {
+      cth = make_float2(-cth.x, -cth.y);
+      scal = true;
+    }
+    for (uint32_t gb = a & ch.gen; gb; gb &= gb - 1) {
+      const TermDesc& td = terms[ch.t0 + (__ffs(gb) - 1)];
+      cth = cmulf(cth, make_float2(td.cr, td.ci));
       scal = true;
     }
   }
@@ -289,7 +316,9 @@ __device__ __forceinline__ void bar_group(int g) {
 
 __global__ void __launch_bounds__(THREADS, 1) k_fused_pass(const __grid_constant__ PassParams P) {
   extern __shared__ uint8_t smem_raw[];
-  uint8_t* smem = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
+  // 1024-byte aligned (the swizzled operand images); an offset into the shared array keeps the
+  // pointers in the shared address space (32-bit addressing for every tile access)
+  uint8_t* smem = smem_raw + ((0u - smem_u32(smem_raw)) & 1023u);
   // mbarriers: tile full[3], tile done[3], operand full[3], operand empty[3], mma[2]
   __shared__ __align__(8) uint64_t bars[2 * NTILEBUF + 2 * NOPSLOT + GROUPS];
   __shared__ uint32_t tmem_base_sh;
@@ -300,6 +329,8 @@ __global__ void __launch_bounds__(THREADS, 1) k_fused_pass(const __grid_constant
   __shared__ uint64_t run_off[TILE >> LOW_BITS];  // index bits of run r of a tile (the window bits above wl)
   __shared__ TermDesc s_terms[MAX_TERMS];         // the pass's program, read with runtime indices
   __shared__ OpDesc s_ops[MAX_OPS];
+  __shared__ ColChunk s_chunks[MAX_CHUNKS];
+  __shared__ uint32_t act_sh[GROUPS][MAX_CHUNKS];  // per tile: the chunks' terms active on it
 
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
   auto bar_tfull = [&](int b) { return smem_u32(&bars[b]); };
@@ -332,6 +363,7 @@ __global__ void __launch_bounds__(THREADS, 1) k_fused_pass(const __grid_constant
   }
   for (uint32_t r = uint32_t(tid); r < (uint32_t(TILE) >> P.wl); r += THREADS) run_off[r] = global_index(0, r << P.wl, P);
   for (int i = tid; i < P.nops; i += THREADS) s_ops[i] = P.ops[i];
+  for (int i = tid; i < P.nchunks; i += THREADS) s_chunks[i] = P.chunks[i];
   {
     int nterms = 0;
     for (int i = 0; i < P.nops; ++i) nterms = max(nterms, int(P.ops[i].t1));
@@ -443,9 +475,20 @@ __global__ void __launch_bounds__(THREADS, 1) k_fused_pass(const __grid_constant
       const uint64_t it = uint64_t(GROUPS) * p + uint64_t(g);
       const bool mine = have(it);
       const int b = int(it % NTILEBUF);
+      const uint64_t base = mine ? tile_base(tile_of(it), P) : 0;
+      if (mine && tg < 32) {  // which column terms apply on this tile (their bits outside it)
+        for (int c = 0; c < P.nchunks; ++c) {
+          bool on = false;
+          if (tg < int(s_chunks[c].cnt)) {
+            const uint64_t cm = s_terms[s_chunks[c].t0 + tg].cmask;
+            on = (base & cm) == cm;
+          }
+          const uint32_t m = __ballot_sync(0xffffffffu, on);
+          if (tg == 0) act_sh[g][c] = m;
+        }
+      }
       if (mine && tg == 0 && !mbar_wait(bar_tfull(b), uint32_t((it / NTILEBUF) & 1))) fail(1);
       if (bar_any(1 + g, GROUP_THREADS, abort_sh)) break;
-      const uint64_t base = mine ? tile_base(tile_of(it), P) : 0;
       float2* T = tiles + size_t(b) * TILE;
       for (int oi = 0; oi < P.nops; ++oi) {
         const OpDesc op = s_ops[oi];
@@ -521,7 +564,11 @@ __global__ void __launch_bounds__(THREADS, 1) k_fused_pass(const __grid_constant
         uint32_t smask = 0;
         float2 cth = make_float2(1.f, 0.f);
         bool scal = false;
-        column_terms(s_terms, op.p0, op.p1, base, cb, smask, cth, scal);
+        column_chunks(s_chunks, act_sh[g], op.pc0, op.pc1, uint32_t(tg), s_terms, smask, cth, scal);
+        // warp-uniform decisions (a lane without a phase multiplies by exactly 1, one without
+        // signs flips nothing), so the unrolled loops carry no divergent branches
+        scal = __any_sync(0xffffffffu, scal);
+        const bool flip = __any_sync(0xffffffffu, smask != 0);
 #pragma unroll
         for (int q = 0; q < 4; ++q) {
           float2 xx[8];  // rows 8q..8q+7, loaded before any other work
@@ -531,7 +578,7 @@ __global__ void __launch_bounds__(THREADS, 1) k_fused_pass(const __grid_constant
 #pragma unroll
             for (int i = 0; i < 8; ++i) xx[i] = cmulf(cth, xx[i]);
           }
-          if (smask) {
+          if (flip) {
 #pragma unroll
             for (int i = 0; i < 8; ++i) {
               const uint32_t sg = (smask << (31 - (8 * q + i))) & 0x80000000u;
@@ -580,7 +627,9 @@ __global__ void __launch_bounds__(THREADS, 1) k_fused_pass(const __grid_constant
         uint32_t smask2 = 0;
         float2 cth2 = make_float2(1.f, 0.f);
         bool scal2 = false;
-        column_terms(s_terms, op.q0, op.q1, base, cb, smask2, cth2, scal2);
+        column_chunks(s_chunks, act_sh[g], op.qc0, op.qc1, uint32_t(tg), s_terms, smask2, cth2, scal2);
+        scal2 = __any_sync(0xffffffffu, scal2);
+        const bool flip2 = __any_sync(0xffffffffu, smask2 != 0);
         const bool stop = bar_any(1 + g, GROUP_THREADS, abort_sh);
         tc_fence_after();
         if (stop) break;
@@ -590,14 +639,25 @@ __global__ void __launch_bounds__(THREADS, 1) k_fused_pass(const __grid_constant
           NCSIM_TMEM_LD16(taddr + uint32_t(16 * h), re);
           NCSIM_TMEM_LD16(taddr + uint32_t(32 + 16 * h), im);
           asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+          if (scal2) {
 #pragma unroll
-          for (int i = 0; i < 16; ++i) {
-            float2 v = make_float2(__uint_as_float(re[i]), __uint_as_float(im[i]));
-            if (scal2) v = cmulf(cth2, v);
-            const uint32_t sg = (smask2 << (31 - (16 * h + i))) & 0x80000000u;
-            T[lo8[i & 7] | hi4[2 * h + (i >> 3)]] =
-                make_float2(__uint_as_float(__float_as_uint(v.x) ^ sg), __uint_as_float(__float_as_uint(v.y) ^ sg));
+            for (int i = 0; i < 16; ++i) {
+              const float2 v = cmulf(cth2, make_float2(__uint_as_float(re[i]), __uint_as_float(im[i])));
+              re[i] = __float_as_uint(v.x);
+              im[i] = __float_as_uint(v.y);
+            }
           }
+          if (flip2) {
+#pragma unroll
+            for (int i = 0; i < 16; ++i) {
+              const uint32_t sg = (smask2 << (31 - (16 * h + i))) & 0x80000000u;
+              re[i] ^= sg;
+              im[i] ^= sg;
+            }
+          }
+#pragma unroll
+          for (int i = 0; i < 16; ++i)
+            T[lo8[i & 7] | hi4[2 * h + (i >> 3)]] = make_float2(__uint_as_float(re[i]), __uint_as_float(im[i]));
         }
         tc_fence_before();
         bar_group(g);
@@ -705,59 +765,54 @@ std::unique_ptr<DevicePlan> build_device_plan(const ncsim_circuit& c, uint32_t m
       P.nu = nu;
       // A terms op right before a unitary whose terms are, relative to that unitary's five
       // qubits, phases of the other bits or signs on one of its qubits is applied while the
-      // unitary splits the tile: a phase and a 32-row sign mask per column.
+      // unitary splits the tile (kind 2); one left after a unitary, by its read-back (kind 3).
+      // Their terms go to the device as chunks of bit masks over 32 terms.
       static const uint32_t rowpat[GROUP_QUBITS] = {0xAAAAAAAAu, 0xCCCCCCCCu, 0xF0F0F0F0u, 0xFF00FF00u, 0xFFFF0000u};
-      for (int i = 0; i + 1 < no; ++i) {
-        OpDesc& t = P.ops[i];
-        OpDesc& un = P.ops[i + 1];
-        if (t.kind != 1 || un.kind != 0) continue;
+      int nch = 0;
+      auto fold = [&](OpDesc& t, OpDesc& un, uint8_t kind) -> bool {
         uint32_t gm = 0;
         for (int j = 0; j < GROUP_QUBITS; ++j) gm |= 1u << P.pos[un.u][j];
-        bool ok = true;
-        for (int k = t.t0; k < t.t1 && ok; ++k) {
+        for (int k = t.t0; k < t.t1; ++k) {
           const TermDesc& td = P.terms[k];
           const uint32_t gpart = td.tmask & gm;
-          ok = gpart == 0 || (__builtin_popcount(gpart) == 1 && td.cr == -1.0f && td.ci == 0.0f);
+          if (!(gpart == 0 || (__builtin_popcount(gpart) == 1 && td.cr == -1.0f && td.ci == 0.0f))) return false;
         }
-        if (!ok) continue;
-        for (int k = t.t0; k < t.t1; ++k) {
-          TermDesc& td = P.terms[k];
-          const uint32_t gpart = td.tmask & gm;
-          td.rowpat = 0;
-          for (int j = 0; j < GROUP_QUBITS; ++j)
-            if (gpart == (1u << P.pos[un.u][j])) td.rowpat = rowpat[j];
-          td.tmask &= ~gm;
+        const int need = (t.t1 - t.t0 + 31) / 32;
+        if (nch + need > MAX_CHUNKS) return false;
+        int colbit[TILE_BITS];  // tile bit -> column bit of this unitary (-1: a gate bit)
+        for (int b = 0, m = 0; b < TILE_BITS; ++b) colbit[b] = ((gm >> b) & 1) ? -1 : m++;
+        const uint8_t c0 = uint8_t(nch);
+        for (int k0 = t.t0; k0 < t.t1; k0 += 32) {
+          ColChunk ch{};
+          ch.t0 = uint16_t(k0);
+          ch.cnt = uint16_t(std::min(32, t.t1 - k0));
+          for (int i = 0; i < ch.cnt; ++i) {
+            TermDesc& td = P.terms[k0 + i];
+            const uint32_t bit = 1u << i;
+            const uint32_t gpart = td.tmask & gm;
+            td.rowpat = 0;
+            for (int j = 0; j < GROUP_QUBITS; ++j)
+              if (gpart == (1u << P.pos[un.u][j])) td.rowpat = rowpat[j], ch.row[j] |= bit;
+            td.tmask &= ~gm;
+            for (int b = 0; b < TILE_BITS; ++b)
+              if ((td.tmask >> b) & 1) ch.need[colbit[b]] |= bit;
+            if (!td.rowpat) {
+              if (td.cr == -1.0f && td.ci == 0.0f) ch.neg |= bit;
+              else ch.gen |= bit;
+            }
+          }
+          P.chunks[nch++] = ch;
         }
-        t.kind = 2;
-        un.p0 = t.t0;
-        un.p1 = t.t1;
-      }
-      // the same for a terms op left after a unitary, applied by its read-back
-      for (int i = 1; i < no; ++i) {
-        OpDesc& t = P.ops[i];
-        OpDesc& un = P.ops[i - 1];
-        if (t.kind != 1 || un.kind != 0) continue;
-        uint32_t gm = 0;
-        for (int j = 0; j < GROUP_QUBITS; ++j) gm |= 1u << P.pos[un.u][j];
-        bool ok = true;
-        for (int k = t.t0; k < t.t1 && ok; ++k) {
-          const TermDesc& td = P.terms[k];
-          const uint32_t gpart = td.tmask & gm;
-          ok = gpart == 0 || (__builtin_popcount(gpart) == 1 && td.cr == -1.0f && td.ci == 0.0f);
-        }
-        if (!ok) continue;
-        for (int k = t.t0; k < t.t1; ++k) {
-          TermDesc& td = P.terms[k];
-          const uint32_t gpart = td.tmask & gm;
-          td.rowpat = 0;
-          for (int j = 0; j < GROUP_QUBITS; ++j)
-            if (gpart == (1u << P.pos[un.u][j])) td.rowpat = rowpat[j];
-          td.tmask &= ~gm;
-        }
-        t.kind = 3;
-        un.q0 = t.t0;
-        un.q1 = t.t1;
-      }
+        t.kind = kind;
+        if (kind == 2) un.pc0 = c0, un.pc1 = uint8_t(nch);
+        else un.qc0 = c0, un.qc1 = uint8_t(nch);
+        return true;
+      };
+      for (int i = 0; i + 1 < no; ++i)
+        if (P.ops[i].kind == 1 && P.ops[i + 1].kind == 0) fold(P.ops[i], P.ops[i + 1], 2);
+      for (int i = 1; i < no; ++i)
+        if (P.ops[i].kind == 1 && P.ops[i - 1].kind == 0) fold(P.ops[i], P.ops[i - 1], 3);
+      P.nchunks = nch;
       // the pass's first operand: an offset for now, a device pointer below
       P.rops = reinterpret_cast<const uint4*>(uintptr_t(nu ? offsets[offsets.size() - nu] : 0));
       dp->params.push_back(P);
