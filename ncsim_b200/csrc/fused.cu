@@ -17,8 +17,9 @@
 //     N=64, K=16, bf16 in, f32 accumulate in the group's 64 TMEM columns):
 //       D = Xhi.Rhi + Xlo.Rhi + Xhi.Rlo
 //     with R the real form [[Ur, -Ui], [Ui, Ur]] of the fused unitary (bf16
-//     hi/lo images made on the host); each thread reads its D row back
-//     (tcgen05.ld) and writes the 32 new amplitudes into the tile;
+//     hi/lo images made on the host, output columns ordered so that each
+//     row's real and imaginary parts are adjacent); each thread reads its D
+//     row back (tcgen05.ld) and writes the 32 new amplitudes into the tile;
 //   diagonal op: reduced, where it can be, to a phase per column and a sign
 //     mask over the rows of a neighbouring unitary and applied in that
 //     unitary's split or read-back; otherwise the tile index splits into two
@@ -655,31 +656,31 @@ __global__ void __launch_bounds__(THREADS, 1) k_fused_pass(const __grid_constant
         const bool stop = bar_any(1 + g, GROUP_THREADS, abort_sh);
         tc_fence_after();
         if (stop) break;
+        // D columns 16h .. 16h+15 hold rows 8h .. 8h+7 as (real, imaginary) pairs
 #pragma unroll
-        for (int h = 0; h < 2; ++h) {
-          uint32_t re[16], im[16];
-          NCSIM_TMEM_LD16(taddr + uint32_t(16 * h), re);
-          NCSIM_TMEM_LD16(taddr + uint32_t(32 + 16 * h), im);
+        for (int h = 0; h < 4; ++h) {
+          uint32_t v[16];
+          NCSIM_TMEM_LD16(taddr + uint32_t(16 * h), v);
           asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
           if (scal2) {
 #pragma unroll
-            for (int i = 0; i < 16; ++i) {
-              const float2 v = cmulf(cth2, make_float2(__uint_as_float(re[i]), __uint_as_float(im[i])));
-              re[i] = __float_as_uint(v.x);
-              im[i] = __float_as_uint(v.y);
+            for (int i = 0; i < 8; ++i) {
+              const float2 c = cmulf(cth2, make_float2(__uint_as_float(v[2 * i]), __uint_as_float(v[2 * i + 1])));
+              v[2 * i] = __float_as_uint(c.x);
+              v[2 * i + 1] = __float_as_uint(c.y);
             }
           }
           if (flip2) {
 #pragma unroll
-            for (int i = 0; i < 16; ++i) {
-              const uint32_t sg = (smask2 << (31 - (16 * h + i))) & 0x80000000u;
-              re[i] ^= sg;
-              im[i] ^= sg;
+            for (int i = 0; i < 8; ++i) {
+              const uint32_t sg = (smask2 << (31 - (8 * h + i))) & 0x80000000u;
+              v[2 * i] ^= sg;
+              v[2 * i + 1] ^= sg;
             }
           }
 #pragma unroll
-          for (int i = 0; i < 16; ++i)
-            T[lo8[i & 7] ^ hi4[2 * h + (i >> 3)]] = make_float2(__uint_as_float(re[i]), __uint_as_float(im[i]));
+          for (int i = 0; i < 8; ++i)
+            T[lo8[i] ^ hi4[h]] = make_float2(__uint_as_float(v[2 * i]), __uint_as_float(v[2 * i + 1]));
         }
         tc_fence_before();
         bar_group(g);

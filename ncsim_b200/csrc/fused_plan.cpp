@@ -429,16 +429,18 @@ float bf16_value(uint16_t b) {
 }
 
 void build_operand_image(const std::vector<CplxD>& u, uint8_t* out) {
-  // R[n][k]: n < 32 real output rows, n >= 32 imaginary; k < 32 real inputs, k >= 32 imaginary
+  // R[n][k]: output n = 2 row + (0 real, 1 imaginary), so the accumulator holds each row's
+  // real and imaginary parts in adjacent columns; k < 32 real inputs, k >= 32 imaginary
   std::memset(out, 0, 16384);
   uint16_t* hi = reinterpret_cast<uint16_t*>(out);
   uint16_t* lo = reinterpret_cast<uint16_t*>(out + 8192);
   for (uint32_t n = 0; n < 64; ++n)
     for (uint32_t k = 0; k < 64; ++k) {
-      const CplxD e = u[(n & 31) * 32 + (k & 31)];
+      const CplxD e = u[(n >> 1) * 32 + (k & 31)];
+      const bool im_out = n & 1;
       double r;
-      if (n < 32 && k < 32) r = e.re;
-      else if (n < 32) r = -e.im;
+      if (!im_out && k < 32) r = e.re;
+      else if (!im_out) r = -e.im;
       else if (k < 32) r = e.im;
       else r = e.re;
       const float rf = float(r);
