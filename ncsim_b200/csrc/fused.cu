@@ -643,9 +643,7 @@ __global__ void __launch_bounds__(THREADS, 1) k_fused_pass(const __grid_constant
           for (int s = 0; s < 4; ++s) mma_bf16_ta(d_tmem, a_tmem + 8u * s, dbl + 2 * s, idesc, 1);
           mma_commit(bar_mma(g));
           mma_commit(bar_oempty(sl));  // the slot is free once these MMAs have read it
-          if (!mbar_wait(bar_mma(g), mma_phase)) fail(2);
         }
-        mma_phase ^= 1u;
         // a following diagonal op, reduced to this column (computed while the MMAs run)
         uint32_t smask2 = 0;
         float2 cth2 = make_float2(1.f, 0.f);
@@ -653,9 +651,13 @@ __global__ void __launch_bounds__(THREADS, 1) k_fused_pass(const __grid_constant
         column_chunks(s_chunks, act_sh[g], op.qc0, op.qc1, uint32_t(tg), s_terms, smask2, cth2, scal2);
         scal2 = __any_sync(0xffffffffu, scal2);
         const bool flip2 = __any_sync(0xffffffffu, smask2 != 0);
-        const bool stop = bar_any(1 + g, GROUP_THREADS, abort_sh);
+        // every thread waits for the accumulator itself (no group barrier: each warp reads its
+        // lanes back as soon as the MMAs land).  A phase cannot be skipped: the next commit
+        // needs every warp past the barrier after this read-back.  On a timeout the read-back
+        // reads stale columns and the barrier below stops the group.
+        if (!mbar_wait(bar_mma(g), mma_phase)) fail(2);
+        mma_phase ^= 1u;
         tc_fence_after();
-        if (stop) break;
         // D columns 16h .. 16h+15 hold rows 8h .. 8h+7 as (real, imaginary) pairs
 #pragma unroll
         for (int h = 0; h < 4; ++h) {
@@ -683,7 +685,7 @@ __global__ void __launch_bounds__(THREADS, 1) k_fused_pass(const __grid_constant
             T[lo8[i] ^ hi4[h]] = make_float2(__uint_as_float(v[2 * i]), __uint_as_float(v[2 * i + 1]));
         }
         tc_fence_before();
-        bar_group(g);
+        if (bar_any(1 + g, GROUP_THREADS, abort_sh)) break;
       }
       if (bar_any(1 + g, GROUP_THREADS, abort_sh)) break;
       if (mine) mbar_arrive(bar_tdone(b));
