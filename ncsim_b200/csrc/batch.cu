@@ -140,6 +140,12 @@ __device__ __forceinline__ uint32_t loc_mask(uint32_t loc, uint32_t fixed, uint3
 __device__ __forceinline__ uint32_t sgn(uint32_t m, int j) { return (m << (31 - j)) & 0x80000000u; }
 __device__ __forceinline__ float flip(float v, uint32_t s) { return __uint_as_float(__float_as_uint(v) ^ s); }
 
+// The gate updates below are written so that every output's last operation
+// consumes the last use of an input it replaces (cross products first, into
+// temporaries): the outputs can take their inputs' registers, and the op
+// loop, whose switch cases must all leave the 32 amplitudes in the same
+// registers, needs no copies back.
+
 // 2x2 gate on register bit K: u0 = (u00, u01), u1 = (u10, u11) as (re, im).
 // REL: the second amplitude of pair j is negated first where bit j of rel is set.
 template <int K, bool REL>
@@ -147,34 +153,53 @@ __device__ __forceinline__ void gate_k(Regs& r, const float4 u0, const float4 u1
 #pragma unroll
   for (int j = 0; j < 32; ++j) {
     if (j & (1 << K)) continue;
-    float2 y = r.a[j + (1 << K)];
+    float xr = r.a[j].x, xi = r.a[j].y, yr = r.a[j + (1 << K)].x, yi = r.a[j + (1 << K)].y;
     if (REL) {
       const uint32_t sg = sgn(rel, j);
-      y = make_float2(flip(y.x, sg), flip(y.y, sg));
+      yr = flip(yr, sg);
+      yi = flip(yi, sg);
     }
-    const float2 x = r.a[j];
-    r.a[j].x = u0.x * x.x - u0.y * x.y + u0.z * y.x - u0.w * y.y;
-    r.a[j].y = u0.x * x.y + u0.y * x.x + u0.z * y.y + u0.w * y.x;
-    r.a[j + (1 << K)].x = u1.x * x.x - u1.y * x.y + u1.z * y.x - u1.w * y.y;
-    r.a[j + (1 << K)].y = u1.x * x.y + u1.y * x.x + u1.z * y.y + u1.w * y.x;
+    // u10 x (kept for the second row), then u00 x in place of x
+    float ar = fmaf(u1.x, xr, -(u1.y * xi)), ai = fmaf(u1.x, xi, u1.y * xr);
+    const float p = u0.y * xi, q = u0.y * xr;
+    xr = fmaf(u0.x, xr, -p);
+    xi = fmaf(u0.x, xi, q);
+    // + u01 y (y still needed below)
+    xr = fmaf(u0.z, yr, fmaf(-u0.w, yi, xr));
+    xi = fmaf(u0.z, yi, fmaf(u0.w, yr, xi));
+    // u10 x + u11 y in place of y
+    ar = fmaf(-u1.w, yi, ar);
+    ai = fmaf(u1.w, yr, ai);
+    yr = fmaf(u1.z, yr, ar);
+    yi = fmaf(u1.z, yi, ai);
+    r.a[j] = make_float2(xr, xi);
+    r.a[j + (1 << K)] = make_float2(yr, yi);
   }
 }
 
 // balanced gate s [[1, w], [1, -w]] on register bit K: c = (s w.re, s w.im, s)
+// (the first output as 2 s x - (s x - s w y): one extra FP32 rounding)
 template <int K, bool REL>
 __device__ __forceinline__ void bgate_k(Regs& r, const float4 c, uint32_t rel) {
+  const float c2 = 2.0f * c.z;
 #pragma unroll
   for (int j = 0; j < 32; ++j) {
     if (j & (1 << K)) continue;
-    const float2 x = r.a[j], y = r.a[j + (1 << K)];
-    float tr = c.x * y.x - c.y * y.y, ti = c.x * y.y + c.y * y.x;
+    float xr = r.a[j].x, xi = r.a[j].y, yr = r.a[j + (1 << K)].x, yi = r.a[j + (1 << K)].y;
+    const float p = c.y * yi, q = c.y * yr;
+    yr = fmaf(c.x, yr, -p);  // s w y, in place of y
+    yi = fmaf(c.x, yi, q);
     if (REL) {
       const uint32_t sg = sgn(rel, j);
-      tr = flip(tr, sg);
-      ti = flip(ti, sg);
+      yr = flip(yr, sg);
+      yi = flip(yi, sg);
     }
-    r.a[j] = make_float2(fmaf(c.z, x.x, tr), fmaf(c.z, x.y, ti));
-    r.a[j + (1 << K)] = make_float2(fmaf(c.z, x.x, -tr), fmaf(c.z, x.y, -ti));
+    yr = fmaf(c.z, xr, -yr);  // s x - s w y
+    yi = fmaf(c.z, xi, -yi);
+    xr = fmaf(c2, xr, -yr);   // s x + s w y
+    xi = fmaf(c2, xi, -yi);
+    r.a[j] = make_float2(xr, xi);
+    r.a[j + (1 << K)] = make_float2(yr, yi);
   }
 }
 
@@ -218,7 +243,8 @@ __device__ __forceinline__ void diag_mask(Regs& r, uint32_t m, float2 d0, float2
     const bool b = (m >> j) & 1u;
     const float dr = b ? d1.x : d0.x, di = b ? d1.y : d0.y;
     const float2 v = r.a[j];
-    r.a[j] = make_float2(v.x * dr - v.y * di, v.x * di + v.y * dr);
+    const float p = v.y * di, q = v.x * di;
+    r.a[j] = make_float2(fmaf(v.x, dr, -p), fmaf(v.y, dr, q));
   }
 }
 
