@@ -350,6 +350,7 @@ __global__ void __launch_bounds__(THREADS, NBUF == 2 ? 1 : 2) k_batch(const __gr
   __shared__ uint2 s_stage[MAX_PASS_OPS];
   __shared__ double red[THREADS / 32][2];
   __shared__ uint32_t s_job, s_bit;
+  __shared__ DevTraj s_tr;  // the job's descriptor, read where needed (frees registers in the stage loop)
   float2* bufs = reinterpret_cast<float2*>(dsm);
   double* T = NBUF == 2 ? reinterpret_cast<double*>(bufs + 2 * TILE) : P.gscratch + size_t(blockIdx.x) * TILE;
   double* G = NBUF == 2 ? T : reinterpret_cast<double*>(bufs);
@@ -363,7 +364,9 @@ __global__ void __launch_bounds__(THREADS, NBUF == 2 ? 1 : 2) k_batch(const __gr
     __syncthreads();
     if (job >= P.count) break;
     const uint32_t t = P.order[job];
-    const DevTraj tr = P.traj[t];
+    if (tid == 0) s_tr = P.traj[t];
+    __syncthreads();
+    const DevTraj& tr = s_tr;
     if (tr.n < MIN_QUBITS || tr.n > P.max_n || tr.nmeas > tr.n) {
       if (tid == 0) atomicOr(P.err, 1u);
       continue;
@@ -453,7 +456,9 @@ __global__ void __launch_bounds__(THREADS, NBUF == 2 ? 1 : 2) k_batch(const __gr
           else store_stage<2>(cur, tid, regs);
           __syncthreads();
         }
-        if (write || accum) {
+        if (!(sp.flags & PASS_NO_WRITE) || (sp.flags & PASS_ACCUM)) {
+          const bool write = !(sp.flags & PASS_NO_WRITE), accum = sp.flags & PASS_ACCUM;
+          const uint32_t base = base_of(k);
 #pragma unroll 4
           for (uint32_t r = 0; r < TILE / 2 / THREADS; ++r) {
             const uint32_t i = 2u * (tid + THREADS * r);
