@@ -347,6 +347,65 @@ ncsim_status ncsim_batch_results(ncsim_batch* b, uint32_t* n, uint64_t* records,
  * the device's pass, tile, stage and op order (n <= 22). */
 ncsim_status ncsim_batch_emulate(const ncsim_batch* b, uint32_t t, uint64_t* record, double* z0, double* norm);
 
+/* ---- sparse form: SparseVector<C64> (src/state/sparse.rs) on the device ----
+ * The nonzero amplitudes of a register of 1..64 qubits as (basis index,
+ * complex128) entries in device memory (at most 2^31 entries).  Operations
+ * that move each entry to one entry (monomial gates, permutations with
+ * phases, Paulis, diagonals) keep the entry order and leave it unsorted when
+ * a key changed; operations that create entries (dense gates, projections)
+ * normalise: entries sorted by index, duplicates summed, exact zeros and
+ * amplitudes under the cutoff dropped (sparse.rs:114-128). */
+typedef struct ncsim_sparse ncsim_sparse;
+/* SparseVector::zero_state (sparse.rs:50-52). */
+ncsim_status ncsim_sparse_create(uint32_t n, ncsim_sparse** out);
+/* SparseVector::from_entries (sparse.rs:54-72): amps are (re, im) pairs; duplicates add. */
+ncsim_status ncsim_sparse_from_entries(uint32_t n, const uint64_t* keys, const double* amps, uint64_t count,
+                                       ncsim_sparse** out);
+ncsim_status ncsim_sparse_destroy(ncsim_sparse* s);
+/* Clone (sparse.rs:27, #[derive(Clone)]). */
+ncsim_status ncsim_sparse_clone(const ncsim_sparse* s, ncsim_sparse** out);
+/* SparseVector::with_cutoff (sparse.rs:74-78): drop |a| < cutoff after each normalisation. */
+ncsim_status ncsim_sparse_set_cutoff(ncsim_sparse* s, double cutoff);
+ncsim_status ncsim_sparse_num_qubits(const ncsim_sparse* s, uint32_t* n);
+/* SparseVector::num_entries (sparse.rs:84-86). */
+ncsim_status ncsim_sparse_num_entries(const ncsim_sparse* s, uint64_t* count);
+/* SparseVector::entries (sparse.rs:88-90), in the current entry order; cap >= num_entries. */
+ncsim_status ncsim_sparse_get_entries(const ncsim_sparse* s, uint64_t* keys, double* amps, uint64_t cap);
+/* SparseVector::sort (sparse.rs:92-97). */
+ncsim_status ncsim_sparse_sort(ncsim_sparse* s);
+/* QuantumState::apply_gate for SparseVector (sparse.rs:266-297): Pauli, monomial, matrix views. */
+ncsim_status ncsim_sparse_apply_gate(ncsim_sparse* s, const ncsim_gate* g, const uint32_t* qubits, uint32_t k);
+/* SparseVector::apply_pauli (sparse.rs:216-231): psi <- i^phase X^x Z^z psi. */
+ncsim_status ncsim_sparse_apply_pauli(ncsim_sparse* s, uint64_t x, uint64_t z, uint32_t phase);
+/* norm_sq (sparse.rs:299-302), FP64 reduction. */
+ncsim_status ncsim_sparse_norm_sq(const ncsim_sparse* s, double* re_im);
+/* amplitude (sparse.rs:304-314): 0 for an index without an entry. */
+ncsim_status ncsim_sparse_amplitude(const ncsim_sparse* s, uint64_t index, double* re_im);
+/* expectation (sparse.rs:316-336) over the sorted view. */
+ncsim_status ncsim_sparse_expectation(const ncsim_sparse* s, uint64_t x, uint64_t z, uint32_t phase, double* re_im);
+/* inner (sparse.rs:338-349): <a|b>. */
+ncsim_status ncsim_sparse_inner(const ncsim_sparse* a, const ncsim_sparse* b, double* re_im);
+/* project (sparse.rs:351-380): psi <- (1 + (-1)^outcome P)/2 psi for Hermitian P; the weight after it. */
+ncsim_status ncsim_sparse_project(ncsim_sparse* s, uint64_t x, uint64_t z, uint32_t phase, int32_t outcome,
+                                  double* weight_re_im);
+/* scale (sparse.rs:382-386). */
+ncsim_status ncsim_sparse_scale(ncsim_sparse* s, double re, double im);
+/* tensor (sparse.rs:388-405): a on the low qubits, b above them (n_a + n_b <= 64). */
+ncsim_status ncsim_sparse_tensor(const ncsim_sparse* a, const ncsim_sparse* b, ncsim_sparse** out);
+/* sample (sparse.rs:407-424): cumulative weights in entry order, one rng.gen::<f64>() per shot. */
+ncsim_status ncsim_sparse_sample(const ncsim_sparse* s, ncsim_rng* rng, uint64_t shots, uint64_t* out);
+/* to_vector (sparse.rs:426-434), n <= 26. */
+ncsim_status ncsim_sparse_to_vector(const ncsim_sparse* s, double* amps, uint64_t len);
+/* QuantumState::measure (mod.rs:113-131) and run (mod.rs:168-183) on the sparse state. */
+ncsim_status ncsim_sparse_measure(ncsim_sparse* s, uint64_t x, uint64_t z, uint32_t phase, ncsim_rng* rng,
+                                  int32_t* outcome);
+ncsim_status ncsim_sparse_run(ncsim_sparse* s, const ncsim_circuit* c, ncsim_rng* rng, uint8_t* rec, size_t cap,
+                              size_t* len);
+/* Waits for the state's queued device work; device-time events on its stream. */
+ncsim_status ncsim_sparse_synchronize(const ncsim_sparse* s);
+ncsim_status ncsim_sparse_timer_start(ncsim_sparse* s);
+ncsim_status ncsim_sparse_timer_stop(ncsim_sparse* s, double* milliseconds);
+
 #ifdef __cplusplus
 }
 #endif

@@ -130,6 +130,31 @@ _SIGNATURES = {
     "ncsim_batch_run": (_i32, [_vp, _P(_dbl)]),
     "ncsim_batch_results": (_i32, [_vp, _P(_u32), _P(_u64), _P(_dbl), _P(_dbl)]),
     "ncsim_batch_emulate": (_i32, [_vp, _u32, _P(_u64), _P(_dbl), _P(_dbl)]),
+    "ncsim_sparse_create": (_i32, [_u32, _P(_vp)]),
+    "ncsim_sparse_from_entries": (_i32, [_u32, _P(_u64), _P(_dbl), _u64, _P(_vp)]),
+    "ncsim_sparse_destroy": (_i32, [_vp]),
+    "ncsim_sparse_clone": (_i32, [_vp, _P(_vp)]),
+    "ncsim_sparse_set_cutoff": (_i32, [_vp, _dbl]),
+    "ncsim_sparse_num_qubits": (_i32, [_vp, _P(_u32)]),
+    "ncsim_sparse_num_entries": (_i32, [_vp, _P(_u64)]),
+    "ncsim_sparse_get_entries": (_i32, [_vp, _P(_u64), _P(_dbl), _u64]),
+    "ncsim_sparse_sort": (_i32, [_vp]),
+    "ncsim_sparse_apply_gate": (_i32, [_vp, _vp, _P(_u32), _u32]),
+    "ncsim_sparse_apply_pauli": (_i32, [_vp, _u64, _u64, _u32]),
+    "ncsim_sparse_norm_sq": (_i32, [_vp, _P(_dbl)]),
+    "ncsim_sparse_amplitude": (_i32, [_vp, _u64, _P(_dbl)]),
+    "ncsim_sparse_expectation": (_i32, [_vp, _u64, _u64, _u32, _P(_dbl)]),
+    "ncsim_sparse_inner": (_i32, [_vp, _vp, _P(_dbl)]),
+    "ncsim_sparse_project": (_i32, [_vp, _u64, _u64, _u32, _i32, _P(_dbl)]),
+    "ncsim_sparse_scale": (_i32, [_vp, _dbl, _dbl]),
+    "ncsim_sparse_tensor": (_i32, [_vp, _vp, _P(_vp)]),
+    "ncsim_sparse_sample": (_i32, [_vp, _vp, _u64, _P(_u64)]),
+    "ncsim_sparse_to_vector": (_i32, [_vp, _P(_dbl), _u64]),
+    "ncsim_sparse_measure": (_i32, [_vp, _u64, _u64, _u32, _vp, _P(_i32)]),
+    "ncsim_sparse_run": (_i32, [_vp, _vp, _vp, _P(C.c_uint8), C.c_size_t, _P(C.c_size_t)]),
+    "ncsim_sparse_synchronize": (_i32, [_vp]),
+    "ncsim_sparse_timer_start": (_i32, [_vp]),
+    "ncsim_sparse_timer_stop": (_i32, [_vp, _P(_dbl)]),
 }
 
 
@@ -724,6 +749,150 @@ class TrajectoryBatch:
         r, z, nn = _u64(), _dbl(), _dbl()
         _check(lib().ncsim_batch_emulate(self._h, t, C.byref(r), C.byref(z), C.byref(nn)))
         return r.value, z.value, nn.value
+
+
+class GpuSparseVector:
+    """The nonzero amplitudes of a register of up to 64 qubits in B200 memory:
+    the drop-in for ``SparseVector<C64>`` (``src/state/sparse.rs``).
+
+    Entries are (basis index, complex128) pairs.  Gates that move each entry to
+    one entry (monomials, permutations with phases, Paulis, diagonals) keep the
+    entry order; dense gates and projections sort, sum duplicates and drop
+    zeros, as the reference does.
+    """
+
+    BACKEND = "GpuSparseVector"
+
+    def __init__(self, n: int, _handle=None):
+        if _handle is None:
+            h = _vp()
+            _check(lib().ncsim_sparse_create(n, C.byref(h)))
+            _handle = h
+        self._h = _handle
+        self.n = n
+
+    @classmethod
+    def zero_state(cls, n: int) -> "GpuSparseVector":
+        return cls(n)
+
+    @classmethod
+    def from_entries(cls, n: int, keys: Sequence[int], amps: Sequence[complex]) -> "GpuSparseVector":
+        """``SparseVector::from_entries`` (sparse.rs:54-72): duplicates are added."""
+        k = np.ascontiguousarray(np.asarray(list(keys), dtype=np.uint64))
+        a = np.ascontiguousarray(np.asarray(list(amps), dtype=np.complex128))
+        h = _vp()
+        _check(lib().ncsim_sparse_from_entries(n, k.ctypes.data_as(_P(_u64)), _dp(a.view(np.float64)), k.size,
+                                               C.byref(h)))
+        return cls(n, h)
+
+    def __del__(self):
+        h = getattr(self, "_h", None)
+        if h and _lib is not None:
+            _lib.ncsim_sparse_destroy(h)
+            self._h = None
+
+    def clone(self) -> "GpuSparseVector":
+        h = _vp()
+        _check(lib().ncsim_sparse_clone(self._h, C.byref(h)))
+        return GpuSparseVector(self.n, h)
+
+    def with_cutoff(self, cutoff: float) -> "GpuSparseVector":
+        _check(lib().ncsim_sparse_set_cutoff(self._h, cutoff))
+        return self
+
+    def num_qubits(self) -> int:
+        return self.n
+
+    def num_entries(self) -> int:
+        m = _u64()
+        _check(lib().ncsim_sparse_num_entries(self._h, C.byref(m)))
+        return m.value
+
+    def entries(self):
+        """(indices, amplitudes) in the current entry order."""
+        m = self.num_entries()
+        k = np.empty(m, dtype=np.uint64)
+        a = np.empty(2 * m, dtype=np.float64)
+        _check(lib().ncsim_sparse_get_entries(self._h, k.ctypes.data_as(_P(_u64)), _dp(a), m))
+        return k, a.view(np.complex128)
+
+    def sort(self) -> None:
+        _check(lib().ncsim_sparse_sort(self._h))
+
+    def apply_gate(self, gate: Gate, qubits: Sequence[int]) -> None:
+        _check(lib().ncsim_sparse_apply_gate(self._h, gate._h, _u32s(qubits), len(qubits)))
+
+    def apply_pauli(self, p: Pauli) -> None:
+        _check(lib().ncsim_sparse_apply_pauli(self._h, p.x, p.z, p.phase))
+
+    def norm_sq(self) -> complex:
+        o = (_dbl * 2)()
+        _check(lib().ncsim_sparse_norm_sq(self._h, o))
+        return _complex(o)
+
+    def amplitude(self, index: int) -> complex:
+        o = (_dbl * 2)()
+        _check(lib().ncsim_sparse_amplitude(self._h, index, o))
+        return _complex(o)
+
+    def expectation(self, p: Pauli) -> complex:
+        if p.n != self.n:
+            raise SimError(8, "expectation: operator on the wrong register")
+        o = (_dbl * 2)()
+        _check(lib().ncsim_sparse_expectation(self._h, p.x, p.z, p.phase, o))
+        return _complex(o)
+
+    def inner(self, other: "GpuSparseVector") -> complex:
+        o = (_dbl * 2)()
+        _check(lib().ncsim_sparse_inner(self._h, other._h, o))
+        return _complex(o)
+
+    def project(self, p: Pauli, outcome: bool) -> complex:
+        o = (_dbl * 2)()
+        _check(lib().ncsim_sparse_project(self._h, p.x, p.z, p.phase, int(bool(outcome)), o))
+        return _complex(o)
+
+    def scale(self, c: complex) -> None:
+        c = complex(c)
+        _check(lib().ncsim_sparse_scale(self._h, c.real, c.imag))
+
+    def tensor(self, other: "GpuSparseVector") -> "GpuSparseVector":
+        h = _vp()
+        _check(lib().ncsim_sparse_tensor(self._h, other._h, C.byref(h)))
+        return GpuSparseVector(self.n + other.n, h)
+
+    def sample(self, rng: StdRng, shots: int) -> np.ndarray:
+        out = np.empty(shots, dtype=np.uint64)
+        _check(lib().ncsim_sparse_sample(self._h, rng._h, shots, out.ctypes.data_as(_P(_u64))))
+        return out
+
+    def to_vector(self) -> np.ndarray:
+        b = np.empty(2 << self.n, dtype=np.float64)
+        _check(lib().ncsim_sparse_to_vector(self._h, _dp(b), 1 << self.n))
+        return b.view(np.complex128)
+
+    def measure(self, p: Pauli, rng: StdRng) -> bool:
+        o = _i32()
+        _check(lib().ncsim_sparse_measure(self._h, p.x, p.z, p.phase, rng._h, C.byref(o)))
+        return bool(o.value)
+
+    def run(self, circuit: Circuit, rng: StdRng) -> list[bool]:
+        m = circuit.num_measurements
+        rec = (C.c_uint8 * max(1, m))()
+        ln = C.c_size_t()
+        _check(lib().ncsim_sparse_run(self._h, circuit._h, rng._h, rec, m, C.byref(ln)))
+        return [bool(rec[i]) for i in range(ln.value)]
+
+    def synchronize(self) -> None:
+        _check(lib().ncsim_sparse_synchronize(self._h))
+
+    def timer_start(self) -> None:
+        _check(lib().ncsim_sparse_timer_start(self._h))
+
+    def timer_stop(self) -> float:
+        ms = _dbl()
+        _check(lib().ncsim_sparse_timer_stop(self._h, C.byref(ms)))
+        return ms.value
 
 
 def device_info() -> dict:

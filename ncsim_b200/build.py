@@ -21,6 +21,7 @@ SOURCES = [
     "csrc/fused_plan.cpp",
     "csrc/batch.cu",
     "csrc/batch_plan.cpp",
+    "csrc/sparse.cu",
     "csrc/host/ir.cpp",
     "csrc/host/runtime.cpp",
 ]
