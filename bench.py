@@ -419,7 +419,27 @@ def config_rates(nb, peak, peak_kind):
 
     measure("C0", 20, nb.Circuit.random_layers(20, 40, 1), 10, c0_readouts)
     measure("C1", 30, nb.Circuit.random_layers(30, 20, 1, 0.0, 26, 30), 2)
-    measure("C3", 31, nb.Circuit.reversible(31, 2000, 1), 0)
+    c3 = nb.Circuit.reversible(31, 2000, 1)
+    measure("C3", 31, c3, 0)
+
+    # the same C3 circuit on the sparse form (SparseVector: 2^16 entries instead of 2^31 amplitudes)
+    sp = nb.GpuSparseVector(31)
+    sp.run(c3, nb.StdRng(11))  # warm-up (stream-ordered pools, CUB temporaries)
+    runs, t0 = 3, time.perf_counter()
+    ms_dev = 0.0
+    for _ in range(runs):
+        sp = nb.GpuSparseVector(31)
+        sp.timer_start()
+        sp.run(c3, nb.StdRng(11))
+        ms_dev += sp.timer_stop()
+    wall = (time.perf_counter() - t0) * 1e3 / runs
+    out["C3_sparse"] = {"n": 31, "gates": c3.num_gates, "entries": sp.num_entries(),
+                        "ms_per_run": ms_dev / runs, "wall_ms_per_run": wall,
+                        "gates_per_s": c3.num_gates / (ms_dev / runs / 1e3),
+                        "speedup_vs_dense": out["C3"]["ms_per_run"] / (ms_dev / runs),
+                        "note": "GpuSparseVector from |0>: device time of the run on its stream (the host waits "
+                                "for entry counts after every normalisation); wall includes state creation"}
+    del sp
     return out
 
 
