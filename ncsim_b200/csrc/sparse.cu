@@ -95,6 +95,25 @@ __global__ void k_sp_monomial(uint64_t* key, double2* amp, uint64_t m, Qubits qs
   }
 }
 
+// the same with the tables in the kernel parameters (no per-gate upload)
+template <int N>
+struct MonoParams {
+  Qubits qs;
+  uint32_t unit[(N + 31) / 32];  // bit x: phase[x] == 1
+  uint16_t image[N];
+  double2 phase[N];
+};
+template <int N>
+__global__ void k_sp_monomial_p(uint64_t* key, double2* amp, uint64_t m, const __grid_constant__ MonoParams<N> P) {
+  for (uint64_t i = uint64_t(blockIdx.x) * blockDim.x + threadIdx.x; i < m; i += uint64_t(gridDim.x) * blockDim.x) {
+    const uint64_t kk = key[i];
+    const uint32_t x = local_of(kk, P.qs);
+    if (!((P.unit[x >> 5] >> (x & 31)) & 1u)) amp[i] = zmul(P.phase[x], amp[i]);
+    const uint32_t y = P.image[x];
+    if (y != x) key[i] = with_local(kk, P.qs, y);
+  }
+}
+
 // i^phase X^x Z^z (sparse.rs:216-231)
 __global__ void k_sp_pauli(uint64_t* key, double2* amp, uint64_t m, uint64_t x, uint64_t z, uint32_t phase) {
   for (uint64_t i = uint64_t(blockIdx.x) * blockDim.x + threadIdx.x; i < m; i += uint64_t(gridDim.x) * blockDim.x) {
@@ -142,28 +161,51 @@ struct SpPoly {
   const uint64_t* coeff;
   const double2* table;
 };
-__global__ void k_sp_phasepoly(const uint64_t* key, double2* amp, uint64_t m, SpPoly P) {
-  const uint64_t mk = P.bits >= 64 ? ~uint64_t(0) : (uint64_t(1) << P.bits) - 1;
-  for (uint64_t i = uint64_t(blockIdx.x) * blockDim.x + threadIdx.x; i < m; i += uint64_t(gridDim.x) * blockDim.x) {
-    const uint64_t kk = key[i];
-    uint64_t f = P.constant;
-    for (uint32_t t = 0; t < P.nterms; ++t) {
-      uint32_t all = 1;
-      for (uint32_t l = P.start[t]; l < P.start[t + 1]; ++l) all &= uint32_t(__popcll(P.par[l] & kk)) & 1u;
-      if (all) f += P.coeff[t];
-    }
-    f &= mk;
-    double2 c;
-    if (P.use_table) {
-      c = P.table[f];
-    } else {
-      if (f == 0 && P.scalar_is_one) continue;
-      c = turn_root(f, P.bits);
-      if (!P.scalar_is_one) c = zmul(P.scalar, c);
-    }
-    if (c.x == 1.0 && c.y == 0.0) continue;
-    amp[i] = zmul(c, amp[i]);
+// amp *= scalar * zeta^f(key), f = constant + sum_t coeff_t prod_l [par_l . key] mod 2^bits
+template <class Start>
+__device__ __forceinline__ void poly_apply(uint64_t kk, double2& amp, uint32_t bits, uint32_t nterms, uint64_t constant,
+                                           bool scalar_is_one, double2 scalar, bool use_table, const Start* start,
+                                           const uint64_t* par, const uint64_t* coeff, const double2* table) {
+  const uint64_t mk = bits >= 64 ? ~uint64_t(0) : (uint64_t(1) << bits) - 1;
+  uint64_t f = constant;
+  for (uint32_t t = 0; t < nterms; ++t) {
+    uint32_t all = 1;
+    for (uint32_t l = start[t]; l < start[t + 1]; ++l) all &= uint32_t(__popcll(par[l] & kk)) & 1u;
+    if (all) f += coeff[t];
   }
+  f &= mk;
+  double2 c;
+  if (use_table) {
+    c = table[f];
+  } else {
+    if (f == 0 && scalar_is_one) return;
+    c = turn_root(f, bits);
+    if (!scalar_is_one) c = zmul(scalar, c);
+  }
+  if (c.x == 1.0 && c.y == 0.0) return;
+  amp = zmul(c, amp);
+}
+__global__ void k_sp_phasepoly(const uint64_t* key, double2* amp, uint64_t m, SpPoly P) {
+  for (uint64_t i = uint64_t(blockIdx.x) * blockDim.x + threadIdx.x; i < m; i += uint64_t(gridDim.x) * blockDim.x)
+    poly_apply(key[i], amp[i], P.bits, P.nterms, P.constant, P.scalar_is_one, P.scalar, P.use_table, P.start, P.par,
+               P.coeff, P.table);
+}
+
+// the same with the terms in the kernel parameters
+constexpr int SP_POLY_TERMS = 128, SP_POLY_PARS = 256;
+struct PolyParamsSp {
+  uint32_t bits, nterms, scalar_is_one, use_table;
+  uint64_t constant;
+  double2 scalar;
+  uint16_t start[SP_POLY_TERMS + 1];
+  uint64_t par[SP_POLY_PARS];
+  uint64_t coeff[SP_POLY_TERMS];
+  double2 table[256];
+};
+__global__ void k_sp_phasepoly_p(const uint64_t* key, double2* amp, uint64_t m, const __grid_constant__ PolyParamsSp P) {
+  for (uint64_t i = uint64_t(blockIdx.x) * blockDim.x + threadIdx.x; i < m; i += uint64_t(gridDim.x) * blockDim.x)
+    poly_apply(key[i], amp[i], P.bits, P.nterms, P.constant, P.scalar_is_one, P.scalar, P.use_table, P.start, P.par,
+               P.coeff, P.table);
 }
 
 __global__ void k_sp_scale(double2* amp, uint64_t m, double2 c) {
@@ -507,7 +549,25 @@ void sp_monomial(ncsim_sparse* s, const std::vector<uint32_t>& qubits, const std
     unit[x] = phase[x].re == 1.0 && phase[x].im == 0.0;
     moves |= image[x] != x;
   }
-  if (s->m) {
+  if (s->m && gd <= 256) {
+    auto launch = [&](auto& P) {
+      P.qs = qs;
+      for (size_t x = 0; x < gd; ++x) {
+        P.image[x] = uint16_t(image[x]);
+        P.phase[x] = ph[x];
+        if (unit[x]) P.unit[x >> 5] |= 1u << (x & 31);
+      }
+      return &P;
+    };
+    if (gd <= 16) {
+      MonoParams<16> P{};
+      k_sp_monomial_p<16><<<sp_grid(s->m), SP_THREADS, 0, s->stream>>>(s->key, s->amp, s->m, *launch(P));
+    } else {
+      MonoParams<256> P{};
+      k_sp_monomial_p<256><<<sp_grid(s->m), SP_THREADS, 0, s->stream>>>(s->key, s->amp, s->m, *launch(P));
+    }
+    NCSIM_LAUNCHED("sparse monomial");
+  } else if (s->m) {
     cudaStream_t st = s->stream;
     uint32_t* di = upload(image, st);
     double2* dp = upload(ph, st);
@@ -603,6 +663,24 @@ void sp_pauli(ncsim_sparse* s, uint64_t x, uint64_t z, uint32_t phase) {
 void sp_phasepoly(ncsim_sparse* s, const PolyTerms& t) {
   if (!s->m) return;
   cudaStream_t st = s->stream;
+  if (t.coeffs.size() <= size_t(SP_POLY_TERMS) && t.parities.size() <= size_t(SP_POLY_PARS) &&
+      t.root_table.size() <= 256) {
+    auto P = std::make_unique<PolyParamsSp>();
+    P->bits = t.bits;
+    P->nterms = uint32_t(t.coeffs.size());
+    P->constant = t.constant;
+    P->scalar = make_double2(t.scalar.re, t.scalar.im);
+    P->scalar_is_one = t.scalar_is_one;
+    P->use_table = !t.root_table.empty();
+    for (size_t i = 0; i < t.term_start.size(); ++i) P->start[i] = uint16_t(t.term_start[i]);
+    if (t.term_start.empty()) P->start[0] = 0;
+    for (size_t i = 0; i < t.parities.size(); ++i) P->par[i] = t.parities[i];
+    for (size_t i = 0; i < t.coeffs.size(); ++i) P->coeff[i] = t.coeffs[i];
+    for (size_t i = 0; i < t.root_table.size(); ++i) P->table[i] = make_double2(t.root_table[i].re, t.root_table[i].im);
+    k_sp_phasepoly_p<<<sp_grid(s->m), SP_THREADS, 0, st>>>(s->key, s->amp, s->m, *P);
+    NCSIM_LAUNCHED("sparse phasepoly");
+    return;
+  }
   SpPoly P{};
   P.bits = t.bits;
   P.nterms = uint32_t(t.coeffs.size());
