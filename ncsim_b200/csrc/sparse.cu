@@ -262,6 +262,62 @@ __global__ void k_sp_tensor(const uint64_t* ka, const double2* va, uint64_t ma, 
   }
 }
 
+// ---- a run of one-to-one ops in one pass ----
+// Monomial gates, diagonals and Paulis map each entry to one entry, so a run of
+// them is applied entry by entry: one thread walks the run's op list with its
+// entry in registers (one launch and one read and write of the entries per run).
+enum : uint32_t { RUN_MONO = 0, RUN_POLY = 1, RUN_PAULI = 2 };
+struct RunOp {
+  uint32_t type;
+  uint32_t k;        // MONO: qubits; POLY: terms
+  uint8_t q[SP_MAX_K];
+  uint16_t pad;
+  uint32_t off;      // MONO: first pattern in image/phase/unit; POLY: first term in start
+  uint32_t bits;     // POLY
+  uint32_t flags;    // POLY: bit 0 scalar is one, bit 1 phasor table; PAULI: the phase
+  uint32_t toff;     // POLY: first entry of its phasor table in RunData::table
+  uint64_t x, z;     // PAULI; POLY: x = constant
+  double2 scalar;    // POLY
+};
+struct RunData {
+  const RunOp* ops;
+  uint32_t nops;
+  const uint16_t* image;  // monomial tables (image, phase, unit share the op's offset)
+  const double2* phase;
+  const uint8_t* unit;
+  const double2* table;   // polynomial phasor tables
+  const uint32_t* start;  // polynomial term starts (absolute indices into par)
+  const uint64_t* par;
+  const uint64_t* coeff;
+};
+__global__ void k_sp_run(uint64_t* key, double2* amp, uint64_t m, RunData d) {
+  for (uint64_t i = uint64_t(blockIdx.x) * blockDim.x + threadIdx.x; i < m; i += uint64_t(gridDim.x) * blockDim.x) {
+    uint64_t kk = key[i];
+    double2 a = amp[i];
+    for (uint32_t o = 0; o < d.nops; ++o) {
+      const RunOp& op = d.ops[o];
+      if (op.type == RUN_MONO) {
+        Qubits qs;
+        qs.k = op.k;
+        for (uint32_t j = 0; j < op.k; ++j) qs.q[j] = op.q[j];
+        const uint32_t x = local_of(kk, qs);
+        if (!d.unit[op.off + x]) a = zmul(d.phase[op.off + x], a);
+        const uint32_t y = d.image[op.off + x];
+        if (y != x) kk = with_local(kk, qs, y);
+      } else if (op.type == RUN_POLY) {
+        poly_apply(kk, a, op.bits, op.k, op.x, op.flags & 1u, op.scalar, (op.flags >> 1) & 1u, d.start + op.off, d.par,
+                   d.coeff + op.off, d.table + op.toff);
+      } else {
+        const uint32_t k = (op.flags + 2u * uint32_t(__popcll(op.z & kk))) & 3u;
+        if (k) a = ipow(a, k);
+        kk ^= op.x;
+      }
+    }
+    key[i] = kk;
+    amp[i] = a;
+  }
+}
+
 // ---- normalisation helpers ----
 struct ZAdd {
   __device__ __forceinline__ double2 operator()(const double2& a, const double2& b) const {
@@ -465,19 +521,23 @@ void sp_normalize(ncsim_sparse* s) {
   sp_normalize_from(s, k, a, s->m);
 }
 
-// a sorted copy of the entries (owned by the caller; stream-ordered)
-void sp_sorted_copy(const ncsim_sparse* s, uint64_t*& k, double2*& a) {
-  cudaStream_t st = s->stream;
-  k = dalloc<uint64_t>(s->m, st);
-  a = dalloc<double2>(s->m, st);
-  if (!s->m) return;
+// a sorted copy of m entries of an n-qubit register, made on stream st (owned by
+// the caller, stream-ordered)
+void sorted_copy(const uint64_t* key, const double2* amp, uint64_t m, uint32_t n, cudaStream_t st, uint64_t*& k,
+                 double2*& a) {
+  k = dalloc<uint64_t>(m, st);
+  a = dalloc<double2>(m, st);
+  if (!m) return;
   size_t tb = 0;
-  const int num = int(s->m);
-  const int end_bit = int(std::max<uint32_t>(1, s->n));
-  NCSIM_CUDA(cub::DeviceRadixSort::SortPairs(nullptr, tb, s->key, k, s->amp, a, num, 0, end_bit, st));
+  const int num = int(m);
+  const int end_bit = int(std::max<uint32_t>(1, n));
+  NCSIM_CUDA(cub::DeviceRadixSort::SortPairs(nullptr, tb, key, k, amp, a, num, 0, end_bit, st));
   void* tmp = dalloc<uint8_t>(tb, st);
-  NCSIM_CUDA(cub::DeviceRadixSort::SortPairs(tmp, tb, s->key, k, s->amp, a, num, 0, end_bit, st));
+  NCSIM_CUDA(cub::DeviceRadixSort::SortPairs(tmp, tb, key, k, amp, a, num, 0, end_bit, st));
   dfree(tmp, st);
+}
+void sp_sorted_copy(const ncsim_sparse* s, uint64_t*& k, double2*& a) {
+  sorted_copy(s->key, s->amp, s->m, s->n, s->stream, k, a);
 }
 
 void sp_sort(ncsim_sparse* s) {
@@ -582,6 +642,27 @@ void sp_monomial(ncsim_sparse* s, const std::vector<uint32_t>& qubits, const std
 }
 
 // a dense matrix (row-major 2^k x 2^k): permutations with phases in place, others by expansion
+// A dense view with one nonzero per column on distinct rows (a permutation with
+// phases, as CCX): every entry moves to one entry (sparse.rs:176-199).
+bool permutation_view(const std::vector<CplxD>& mat, size_t gd, std::vector<uint32_t>& image, std::vector<CplxD>& ph) {
+  image.assign(gd, 0);
+  ph.assign(gd, CplxD{0, 0});
+  std::vector<uint8_t> hit(gd, 0);
+  for (size_t b = 0; b < gd; ++b) {
+    int found = 0;
+    for (size_t a = 0; a < gd; ++a) {
+      const CplxD e = mat[a * gd + b];
+      if (e.re == 0.0 && e.im == 0.0) continue;
+      if (++found > 1 || hit[a]) return false;
+      hit[a] = 1;
+      image[b] = uint32_t(a);
+      ph[b] = e;
+    }
+    if (found != 1) return false;
+  }
+  return true;
+}
+
 void sp_matrix(ncsim_sparse* s, const std::vector<uint32_t>& qubits, const std::vector<CplxD>& mat) {
   const uint32_t k = uint32_t(qubits.size());
   if (k > SP_MAX_K) throw Error(NCSIM_ERR_UNSUPPORTED, "sparse dense gate on more than 10 qubits");
@@ -651,6 +732,92 @@ void sp_matrix(ncsim_sparse* s, const std::vector<uint32_t>& qubits, const std::
   dfree(off, st);
   sp_normalize_from(s, okey, oamp, total);
 }
+
+// the host side of a run: ops and their tables, launched in one kernel
+struct RunBuilder {
+  std::vector<RunOp> ops;
+  std::vector<uint16_t> image;
+  std::vector<double2> phase;
+  std::vector<uint8_t> unit;
+  std::vector<double2> table;
+  std::vector<uint32_t> start;
+  std::vector<uint64_t> par, coeff;
+  bool moves = false;
+
+  bool empty() const { return ops.empty(); }
+  void add_mono(const std::vector<uint32_t>& qubits, const std::vector<uint32_t>& img, const std::vector<CplxD>& ph) {
+    RunOp op{};
+    op.type = RUN_MONO;
+    op.k = uint32_t(qubits.size());
+    for (uint32_t j = 0; j < op.k; ++j) op.q[j] = uint8_t(qubits[j]);
+    op.off = uint32_t(image.size());
+    for (size_t x = 0; x < img.size(); ++x) {
+      image.push_back(uint16_t(img[x]));
+      phase.push_back(make_double2(ph[x].re, ph[x].im));
+      unit.push_back(ph[x].re == 1.0 && ph[x].im == 0.0);
+      moves |= img[x] != x;
+    }
+    ops.push_back(op);
+  }
+  void add_poly(const PolyTerms& t) {
+    RunOp op{};
+    op.type = RUN_POLY;
+    op.k = uint32_t(t.coeffs.size());
+    op.bits = t.bits;
+    op.x = t.constant;
+    op.scalar = make_double2(t.scalar.re, t.scalar.im);
+    op.flags = (t.scalar_is_one ? 1u : 0u) | (t.root_table.empty() ? 0u : 2u);
+    op.off = uint32_t(start.size());
+    const uint32_t pbase = uint32_t(par.size());
+    for (size_t i = 0; i < t.coeffs.size(); ++i) {
+      start.push_back(pbase + (t.term_start.empty() ? 0 : t.term_start[i]));
+      coeff.push_back(t.coeffs[i]);
+    }
+    start.push_back(pbase + (t.term_start.empty() ? 0 : t.term_start[t.coeffs.size()]));
+    // start[] holds nterms + 1 entries per polynomial, coeff[] nterms: keep them aligned
+    coeff.push_back(0);
+    for (uint64_t pm : t.parities) par.push_back(pm);
+    op.toff = uint32_t(table.size());
+    for (const CplxD& c : t.root_table) table.push_back(make_double2(c.re, c.im));
+    ops.push_back(op);
+  }
+  void add_pauli(uint64_t x, uint64_t z, uint32_t ph) {
+    RunOp op{};
+    op.type = RUN_PAULI;
+    op.x = x;
+    op.z = z;
+    op.flags = ph & 3u;
+    moves |= x != 0;
+    ops.push_back(op);
+  }
+  void launch(ncsim_sparse* s) {
+    if (ops.empty()) return;
+    cudaStream_t st = s->stream;
+    if (s->m) {
+      RunOp* d_ops = upload(ops, st);
+      uint16_t* d_img = upload(image, st);
+      double2* d_ph = upload(phase, st);
+      uint8_t* d_unit = upload(unit, st);
+      double2* d_tab = upload(table, st);
+      uint32_t* d_start = upload(start, st);
+      uint64_t* d_par = upload(par, st);
+      uint64_t* d_coeff = upload(coeff, st);
+      RunData d{d_ops, uint32_t(ops.size()), d_img, d_ph, d_unit, d_tab, d_start, d_par, d_coeff};
+      k_sp_run<<<sp_grid(s->m), SP_THREADS, 0, st>>>(s->key, s->amp, s->m, d);
+      NCSIM_LAUNCHED("sparse run");
+      dfree(d_ops, st);
+      dfree(d_img, st);
+      dfree(d_ph, st);
+      dfree(d_unit, st);
+      dfree(d_tab, st);
+      dfree(d_start, st);
+      dfree(d_par, st);
+      dfree(d_coeff, st);
+    }
+    if (moves) s->sorted = false;
+    *this = RunBuilder();
+  }
+};
 
 void sp_pauli(ncsim_sparse* s, uint64_t x, uint64_t z, uint32_t phase) {
   if (s->m) {
@@ -1008,15 +1175,7 @@ ncsim_status ncsim_sparse_inner(const ncsim_sparse* a, const ncsim_sparse* b, do
     uint64_t* kc = nullptr;
     double2* vc = nullptr;
     if (!b->sorted) {  // b's sorted view, made on a's stream
-      ncsim_sparse tmp_view;  // borrows b's arrays for the copy
-      tmp_view.n = b->n;
-      tmp_view.m = b->m;
-      tmp_view.key = b->key;
-      tmp_view.amp = b->amp;
-      tmp_view.stream = a->stream;
-      sp_sorted_copy(&tmp_view, kc, vc);
-      tmp_view.key = nullptr;
-      tmp_view.amp = nullptr;
+      sorted_copy(b->key, b->amp, b->m, b->n, a->stream, kc, vc);
       kb = kc;
       vb = vc;
     }
@@ -1169,10 +1328,52 @@ ncsim_status ncsim_sparse_run(ncsim_sparse* s, const ncsim_circuit* c, ncsim_rng
     if (c->num_measurements()) need(rec, "record");
     Lock lk(s);
     size_t m = 0;
+    // runs of one-to-one ops (gates with a monomial, diagonal or Pauli view, and the
+    // Paulis of sampled noise) go to the device as one pass each; a measurement, a
+    // reset or a gate that creates entries ends a run
+    RunBuilder run;
+    std::vector<uint32_t> img;
+    std::vector<CplxD> ph;
     for (const OpIR& op : c->ops) {
+      if (op.kind == OpKind::Gate) {
+        const LoweredOp& lo = op.lowered;
+        switch (lo.kind) {
+          case LoweredKind::Nothing: continue;
+          case LoweredKind::Monomial:
+            if (lo.qubits.size() <= SP_MAX_K) {
+              run.add_mono(lo.qubits, lo.image, lo.matrix);
+              continue;
+            }
+            break;
+          case LoweredKind::PhasePoly: run.add_poly(lo.poly); continue;
+          case LoweredKind::Pauli: run.add_pauli(lo.x, lo.z, lo.phase); continue;
+          case LoweredKind::Dense:
+            if (lo.qubits.size() <= SP_MAX_K && permutation_view(lo.matrix, size_t(1) << lo.qubits.size(), img, ph)) {
+              run.add_mono(lo.qubits, img, ph);
+              continue;
+            }
+            break;
+        }
+      } else if (op.kind == OpKind::Noise) {
+        // the draws do not depend on the state: a sampled error joins the run
+        const int e = op.noise.sample(*rng);
+        if (e >= 0) {
+          uint64_t x = 0, z = 0;
+          for (size_t j = 0; j < op.qubits.size(); ++j) {
+            x |= uint64_t((e >> j) & 1) << op.qubits[j];
+            z |= uint64_t((e >> (8 + j)) & 1) << op.qubits[j];
+          }
+          run.add_pauli(x, z, 0);
+        }
+        continue;
+      } else if (op.kind != OpKind::Measure && op.kind != OpKind::Reset) {
+        continue;
+      }
+      run.launch(s);
       const int r = sp_apply_op(s, op, *rng);
       if (r >= 0) rec[m++] = uint8_t(r);
     }
+    run.launch(s);
     NCSIM_CUDA(cudaStreamSynchronize(s->stream));
     if (len) *len = m;
   });
