@@ -46,11 +46,11 @@ sys.path.insert(0, ROOT)
 
 
 def measured_peaks():
-    for p in (os.path.join(ROOT, "MEASURED_PEAKS.json"), "/root/repo/MEASURED_PEAKS.json"):
-        if os.path.exists(p):
-            with open(p) as f:
-                d = json.load(f)
-            return float(d["hbm_gbs"]), "measured"
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        with open(p) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
     return FALLBACK_HBM_GBS, "fallback"
 
 

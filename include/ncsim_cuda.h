@@ -15,7 +15,9 @@
  *   2. a C++ host mirror of the trait's provided methods (run, measure,
  *      sample with a seeded StdRng, text circuits, workloads) for hosts that
  *      have no Rust toolchain, and the two GPU-only forms (fused precision
- *      form, batched trajectories).
+ *      form, batched trajectories);
+ *   3. the sparse form: SparseVector<C64> (src/state/sparse.rs) with its
+ *      entries in device memory.
  *
  * Conventions (src/state/vector.rs:14, src/pauli/ops.rs:5):
  *   - qubit q is bit q of a basis index; a k-qubit gate matrix is row-major,
@@ -213,7 +215,7 @@ ncsim_status ncsim_circuit_info(const ncsim_circuit* c, uint32_t* num_qubits, ui
  * without the terminating zero, written only when cap > len. */
 ncsim_status ncsim_circuit_to_text(const ncsim_circuit* c, char* buf, size_t cap, size_t* len);
 
-/* Seeded synthetic workloads (see DESIGN.md for their definitions).
+/* Seeded synthetic workloads (StdRng::seed_from_u64(seed) draws every choice).
  * Random layer family: per layer one of {H, S, T, SQRT_X, RZ(theta)} on every
  * qubit, then CZ on a random perfect matching (optionally followed by
  * DEPOLARIZE2(noise_p)); Z measurements of qubits [m_lo, m_hi) at the end. */
