@@ -545,6 +545,87 @@ constexpr size_t SMEM_NBUF1 = TILE * 8;
 }  // namespace
 
 // ---------------------------------------------------------------------------
+// device buffers of freed batches, kept for the next batch on the same device:
+// a batch's trajectory states take up to tens of GB, and allocating and
+// freeing them cost the driver tens to hundreds of milliseconds per batch.  At
+// most four buffers per device are kept; they are released when an allocation
+// runs out of memory (and the allocation is retried), else at process exit.
+// ---------------------------------------------------------------------------
+namespace {
+struct CachedBuf {
+  int dev;
+  size_t bytes;
+  void* p;
+};
+std::mutex g_buf_mu;
+std::vector<CachedBuf> g_bufs;
+constexpr size_t BUFS_PER_DEVICE = 4;
+
+// a device buffer of at least `bytes` (its capacity in *cap)
+void* buf_alloc(size_t bytes, size_t* cap) {
+  int dev = 0;
+  NCSIM_CUDA(cudaGetDevice(&dev));
+  bytes = std::max<size_t>(bytes, 256);
+  {
+    std::lock_guard<std::mutex> lk(g_buf_mu);
+    size_t best = g_bufs.size();
+    for (size_t i = 0; i < g_bufs.size(); ++i) {
+      const CachedBuf& c = g_bufs[i];
+      if (c.dev != dev || c.bytes < bytes || c.bytes > 2 * bytes + (size_t(64) << 20)) continue;
+      if (best == g_bufs.size() || c.bytes < g_bufs[best].bytes) best = i;
+    }
+    if (best < g_bufs.size()) {
+      void* p = g_bufs[best].p;
+      *cap = g_bufs[best].bytes;
+      g_bufs.erase(g_bufs.begin() + long(best));
+      return p;
+    }
+  }
+  void* p = nullptr;
+  cudaError_t e = cudaMalloc(&p, bytes);
+  if (e == cudaErrorMemoryAllocation) {  // give the kept buffers of this device back and retry
+    cudaGetLastError();
+    std::lock_guard<std::mutex> lk(g_buf_mu);
+    for (size_t i = 0; i < g_bufs.size();) {
+      if (g_bufs[i].dev == dev) {
+        cudaFree(g_bufs[i].p);
+        g_bufs.erase(g_bufs.begin() + long(i));
+      } else {
+        ++i;
+      }
+    }
+    e = cudaMalloc(&p, bytes);
+  }
+  NCSIM_CUDA(e);
+  *cap = bytes;
+  return p;
+}
+
+// returns an idle buffer (its work finished) for reuse on the current device
+void buf_free(void* p, size_t cap) {
+  if (!p) return;
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess) {
+    cudaGetLastError();
+    cudaFree(p);
+    return;
+  }
+  std::lock_guard<std::mutex> lk(g_buf_mu);
+  g_bufs.push_back({dev, cap, p});
+  size_t kept = 0;
+  for (const CachedBuf& c : g_bufs) kept += c.dev == dev;
+  if (kept > BUFS_PER_DEVICE) {  // drop the oldest of this device
+    for (size_t i = 0; i < g_bufs.size(); ++i)
+      if (g_bufs[i].dev == dev) {
+        cudaFree(g_bufs[i].p);
+        g_bufs.erase(g_bufs.begin() + long(i));
+        break;
+      }
+  }
+}
+}  // namespace
+
+// ---------------------------------------------------------------------------
 // the batch object
 // ---------------------------------------------------------------------------
 struct ncsim_batch {
@@ -563,6 +644,7 @@ struct ncsim_batch {
   double* d_norm = nullptr;
   float2* d_slots = nullptr;
   double* d_scratch = nullptr;
+  size_t prog_cap = 0, slots_cap = 0, scratch_cap = 0;  // capacities of the kept-buffer allocations
   uint32_t slot_ctas = 0;
   uint64_t* h_rec = nullptr;
   double* h_z0 = nullptr;
@@ -581,13 +663,16 @@ struct ncsim_batch {
     cudaSetDevice(device);
     if (graph) cudaGraphExecDestroy(graph);
     if (stream) cudaStreamSynchronize(stream);
-    cudaFree(d_prog);
+    buf_free(d_prog, prog_cap);
     cudaFree(d_queue);
     cudaFree(d_rec);
     cudaFree(d_z0);
     cudaFree(d_norm);
-    cudaFree(d_slots);
-    cudaFree(d_scratch);
+    buf_free(d_slots, slots_cap);
+    buf_free(d_scratch, scratch_cap);
+    d_prog = nullptr;
+    d_slots = nullptr;
+    d_scratch = nullptr;
     cudaFreeHost(h_rec);
     cudaFreeHost(h_z0);
     cudaFreeHost(h_norm);
@@ -614,7 +699,10 @@ void ensure_device(ncsim_batch* b) {
   int dev = 0;
   NCSIM_CUDA(cudaGetDevice(&dev));
   if (b->device == dev) return;
-  if (b->device >= 0) b->release();
+  if (b->device >= 0) {
+    b->release();                   // (on its old device)
+    NCSIM_CUDA(cudaSetDevice(dev));  // back to the caller's device
+  }
   b->device = dev;
   NCSIM_CUDA(cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking));
   NCSIM_CUDA(cudaEventCreate(&b->ev0));
@@ -635,7 +723,7 @@ void ensure_device(ncsim_batch* b) {
   b->off_lpt = take(size_t(c) * 4);
   b->off_seq = take(size_t(c) * 4);
   b->off_sample = take(size_t(c) * 4);
-  NCSIM_CUDA(cudaMalloc(&b->d_prog, off));
+  b->d_prog = static_cast<char*>(buf_alloc(off, &b->prog_cap));
   auto up = [&](size_t o, const void* src, size_t bytes) {
     if (bytes) NCSIM_CUDA(cudaMemcpyAsync(b->d_prog + o, src, bytes, cudaMemcpyHostToDevice, b->stream));
   };
@@ -674,14 +762,14 @@ void ensure_slots(ncsim_batch* b, uint32_t ctas) {
     NCSIM_CUDA(cudaGraphExecDestroy(b->graph));
     b->graph = nullptr;
   }
-  cudaFree(b->d_slots);
-  cudaFree(b->d_scratch);
+  buf_free(b->d_slots, b->slots_cap);
+  buf_free(b->d_scratch, b->scratch_cap);
   b->d_slots = nullptr;
   b->d_scratch = nullptr;
   b->slot_ctas = 0;
   const size_t elems = size_t(1) << b->prog.max_n;
-  NCSIM_CUDA(cudaMalloc(&b->d_slots, size_t(ctas) * elems * sizeof(float2)));
-  NCSIM_CUDA(cudaMalloc(&b->d_scratch, size_t(ctas) * TILE * sizeof(double)));
+  b->d_slots = static_cast<float2*>(buf_alloc(size_t(ctas) * elems * sizeof(float2), &b->slots_cap));
+  b->d_scratch = static_cast<double*>(buf_alloc(size_t(ctas) * TILE * sizeof(double), &b->scratch_cap));
   b->slot_ctas = ctas;
 }
 

@@ -28,6 +28,30 @@ int sm_count() {
   return count;
 }
 
+// The library's temporaries (readouts, the sparse form's sort buffers) come from
+// the device's default stream-ordered pool.  Its default release threshold of 0
+// hands freed memory back at every synchronisation, and the next allocation
+// maps it again, which stalled runs by 100 ms and more at times; the pool keeps
+// what it has instead (a per-process allocator setting, set once per device).
+void keep_pool_memory() {
+  static std::mutex mu;
+  static bool done[64] = {};
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) {
+    cudaGetLastError();
+    return;
+  }
+  std::lock_guard<std::mutex> lk(mu);
+  if (done[dev]) return;
+  cudaMemPool_t pool;
+  if (cudaDeviceGetDefaultMemPool(&pool, dev) == cudaSuccess) {
+    uint64_t keep = UINT64_MAX;
+    cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep);
+  }
+  cudaGetLastError();
+  done[dev] = true;
+}
+
 namespace {
 
 void need(const void* p, const char* what) {
@@ -107,13 +131,16 @@ ncsim_state* state_new(uint32_t n, int32_t precision) {
   s->len = uint64_t(1) << n;
   try {
     NCSIM_CUDA(cudaGetDevice(&s->device));
+    keep_pool_memory();
     NCSIM_CUDA(cudaStreamCreateWithFlags(&s->stream, cudaStreamNonBlocking));
     NCSIM_CUDA(cudaMalloc(&s->amp, s->bytes()));
     NCSIM_CUDA(cudaMalloc(&s->partials, sizeof(double) * MAX_REDUCE_BLOCKS * PARTIAL_SLOTS));
     NCSIM_CUDA(cudaMallocHost(&s->host_partials, sizeof(double) * MAX_REDUCE_BLOCKS * PARTIAL_SLOTS));
+    NCSIM_CUDA(cudaMalloc(&s->dev_flag, 256));
   } catch (...) {
     if (s->amp) cudaFree(s->amp);
     if (s->partials) cudaFree(s->partials);
+    if (s->dev_flag) cudaFree(s->dev_flag);
     if (s->host_partials) cudaFreeHost(s->host_partials);
     if (s->stream) cudaStreamDestroy(s->stream);
     delete s;
@@ -131,6 +158,7 @@ void state_free(ncsim_state* s) {
   if (s->timer1) cudaEventDestroy(s->timer1);
   cudaFree(s->amp);
   cudaFree(s->partials);
+  cudaFree(s->dev_flag);
   cudaFreeHost(s->host_partials);
   cudaStreamDestroy(s->stream);
   delete s;

@@ -57,6 +57,8 @@ inline void cuda_check(cudaError_t e, const char* what) {
 // device facts
 // ---------------------------------------------------------------------------
 int sm_count();
+// the current device's default stream-ordered pool keeps freed memory (once per device)
+void keep_pool_memory();
 
 // ---------------------------------------------------------------------------
 // the state handle
@@ -90,6 +92,7 @@ struct ncsim_state {
   int device = 0;
   double* partials = nullptr;       // device scratch: MAX_REDUCE_BLOCKS * PARTIAL_SLOTS
   double* host_partials = nullptr;  // pinned mirror of `partials`
+  int* dev_flag = nullptr;          // device word: a pass kernel's error code (kept for the state's life)
   mutable std::recursive_mutex mu;
   // launch profiler: an event pair per launch while enabled
   mutable bool prof = false;

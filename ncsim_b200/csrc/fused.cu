@@ -892,8 +892,7 @@ extern "C" ncsim_status ncsim_sv_run_fused(ncsim_state* s, const ncsim_circuit* 
     }
     std::lock_guard<std::recursive_mutex> lk(s->mu);
     std::shared_ptr<fused::DevicePlan> dp = device_plan_for(c, max_fuse ? max_fuse : 5);
-    int* d_err = nullptr;
-    NCSIM_CUDA(cudaMallocAsync(&d_err, sizeof(int), s->stream));
+    int* d_err = s->dev_flag;  // the state's own word: no allocation per run
     NCSIM_CUDA(cudaMemsetAsync(d_err, 0, sizeof(int), s->stream));
     NCSIM_CUDA(cudaFuncSetAttribute(fused::k_fused_pass, cudaFuncAttributeMaxDynamicSharedMemorySize, fused::SM_DYNAMIC));
     const uint64_t sets = ((s->len >> fused::TILE_BITS) + fused::GROUPS - 1) / fused::GROUPS;  // a tile per warpgroup
@@ -918,7 +917,6 @@ extern "C" ncsim_status ncsim_sv_run_fused(ncsim_state* s, const ncsim_circuit* 
     }
     int h_err = 0;
     NCSIM_CUDA(cudaMemcpyAsync(&h_err, d_err, sizeof(int), cudaMemcpyDeviceToHost, s->stream));
-    NCSIM_CUDA(cudaFreeAsync(d_err, s->stream));
     NCSIM_CUDA(cudaStreamSynchronize(s->stream));
     if (h_err) throw Error(NCSIM_ERR_DEVICE, "fused pass stopped: a bounded wait timed out (code " + std::to_string(h_err) + ")");
     if (len) *len = m;

@@ -947,6 +947,7 @@ ncsim_sparse* sp_new(uint32_t n) {
   auto s = std::make_unique<ncsim_sparse>();
   s->n = n;
   NCSIM_CUDA(cudaGetDevice(&s->device));
+  keep_pool_memory();
   NCSIM_CUDA(cudaStreamCreateWithFlags(&s->stream, cudaStreamNonBlocking));
   NCSIM_CUDA(cudaMalloc(&s->partials, SP_BLOCKS * 2 * sizeof(double)));
   NCSIM_CUDA(cudaMallocHost(&s->host_partials, SP_BLOCKS * 2 * sizeof(double)));
