@@ -162,15 +162,23 @@ struct SpPoly {
   const double2* table;
 };
 // amp *= scalar * zeta^f(key), f = constant + sum_t coeff_t prod_l [par_l . key] mod 2^bits
+// (and_mask, when given: a term whose parities are all single bits is the AND of
+// those bits, one compare instead of a popcount per parity; 0 for other terms)
 template <class Start>
 __device__ __forceinline__ void poly_apply(uint64_t kk, double2& amp, uint32_t bits, uint32_t nterms, uint64_t constant,
                                            bool scalar_is_one, double2 scalar, bool use_table, const Start* start,
-                                           const uint64_t* par, const uint64_t* coeff, const double2* table) {
+                                           const uint64_t* par, const uint64_t* coeff, const double2* table,
+                                           const uint64_t* and_mask = nullptr) {
   const uint64_t mk = bits >= 64 ? ~uint64_t(0) : (uint64_t(1) << bits) - 1;
   uint64_t f = constant;
   for (uint32_t t = 0; t < nterms; ++t) {
     uint32_t all = 1;
-    for (uint32_t l = start[t]; l < start[t + 1]; ++l) all &= uint32_t(__popcll(par[l] & kk)) & 1u;
+    const uint64_t am = and_mask ? and_mask[t] : 0;
+    if (am) {
+      all = (kk & am) == am;
+    } else {
+      for (uint32_t l = start[t]; l < start[t + 1]; ++l) all &= uint32_t(__popcll(par[l] & kk)) & 1u;
+    }
     if (all) f += coeff[t];
   }
   f &= mk;
@@ -289,6 +297,7 @@ struct RunData {
   const uint32_t* start;  // polynomial term starts (absolute indices into par)
   const uint64_t* par;
   const uint64_t* coeff;
+  const uint64_t* and_mask;  // per term (aligned with coeff): the AND of single-bit parities, or 0
 };
 __global__ void k_sp_run(uint64_t* key, double2* amp, uint64_t m, RunData d) {
   for (uint64_t i = uint64_t(blockIdx.x) * blockDim.x + threadIdx.x; i < m; i += uint64_t(gridDim.x) * blockDim.x) {
@@ -306,7 +315,7 @@ __global__ void k_sp_run(uint64_t* key, double2* amp, uint64_t m, RunData d) {
         if (y != x) kk = with_local(kk, qs, y);
       } else if (op.type == RUN_POLY) {
         poly_apply(kk, a, op.bits, op.k, op.x, op.flags & 1u, op.scalar, (op.flags >> 1) & 1u, d.start + op.off, d.par,
-                   d.coeff + op.off, d.table + op.toff);
+                   d.coeff + op.off, d.table + op.toff, d.and_mask + op.off);
       } else {
         const uint32_t k = (op.flags + 2u * uint32_t(__popcll(op.z & kk))) & 3u;
         if (k) a = ipow(a, k);
@@ -741,7 +750,7 @@ struct RunBuilder {
   std::vector<uint8_t> unit;
   std::vector<double2> table;
   std::vector<uint32_t> start;
-  std::vector<uint64_t> par, coeff;
+  std::vector<uint64_t> par, coeff, and_mask;
   bool moves = false;
 
   bool empty() const { return ops.empty(); }
@@ -772,10 +781,18 @@ struct RunBuilder {
     for (size_t i = 0; i < t.coeffs.size(); ++i) {
       start.push_back(pbase + (t.term_start.empty() ? 0 : t.term_start[i]));
       coeff.push_back(t.coeffs[i]);
+      uint64_t am = 0;
+      bool single = !t.term_start.empty() && t.term_start[i + 1] > t.term_start[i];
+      for (uint32_t l = single ? t.term_start[i] : 0; single && l < t.term_start[i + 1]; ++l) {
+        single = __builtin_popcountll(t.parities[l]) == 1;
+        am |= t.parities[l];
+      }
+      and_mask.push_back(single ? am : 0);
     }
     start.push_back(pbase + (t.term_start.empty() ? 0 : t.term_start[t.coeffs.size()]));
-    // start[] holds nterms + 1 entries per polynomial, coeff[] nterms: keep them aligned
+    // start[] holds nterms + 1 entries per polynomial, coeff[] and and_mask[] nterms: keep them aligned
     coeff.push_back(0);
+    and_mask.push_back(0);
     for (uint64_t pm : t.parities) par.push_back(pm);
     op.toff = uint32_t(table.size());
     for (const CplxD& c : t.root_table) table.push_back(make_double2(c.re, c.im));
@@ -802,7 +819,8 @@ struct RunBuilder {
       uint32_t* d_start = upload(start, st);
       uint64_t* d_par = upload(par, st);
       uint64_t* d_coeff = upload(coeff, st);
-      RunData d{d_ops, uint32_t(ops.size()), d_img, d_ph, d_unit, d_tab, d_start, d_par, d_coeff};
+      uint64_t* d_and = upload(and_mask, st);
+      RunData d{d_ops, uint32_t(ops.size()), d_img, d_ph, d_unit, d_tab, d_start, d_par, d_coeff, d_and};
       k_sp_run<<<sp_grid(s->m), SP_THREADS, 0, st>>>(s->key, s->amp, s->m, d);
       NCSIM_LAUNCHED("sparse run");
       dfree(d_ops, st);
@@ -813,6 +831,7 @@ struct RunBuilder {
       dfree(d_start, st);
       dfree(d_par, st);
       dfree(d_coeff, st);
+      dfree(d_and, st);
     }
     if (moves) s->sorted = false;
     *this = RunBuilder();
