@@ -3,11 +3,11 @@
 // A persistent CTA per SM streams tiles of 2^12 complex64 amplitudes (32 KB)
 // through shared memory: two producer warps copy 16-byte chunks with cp.async
 // (completion on the tile's mbarrier through cp.async.mbarrier.arrive) into
-// four rotating tile buffers and write finished tiles back with 16-byte
-// stores.  The CTA takes its tiles in sets of three, and three warpgroups run
+// five rotating tile buffers and write finished tiles back with 16-byte
+// stores.  The CTA takes its tiles in sets of four, and four warpgroups run
 // the pass's program, one on each tile of a set, so that a group splits
 // amplitudes while the others' MMAs and read-backs run.  The unitaries' B
-// operands (16 KB bf16 images each) stream from L2 into four rotating slots
+// operands (16 KB bf16 images each) stream from L2 into three rotating slots
 // (a third producer warp); each group's tcgen05.commit (or release) frees a
 // slot.  Per group and tile:
 //   unitary op: the tile as 32 rows (the unitary's 5 qubits) x 128 columns;
@@ -42,17 +42,17 @@ namespace fused {
 namespace {
 
 constexpr int GROUP_THREADS = 128;                       // one warpgroup runs the program on one tile
-constexpr int GROUPS = 3;                                // three tiles in flight per CTA
-constexpr int COMPUTE_THREADS = GROUPS * GROUP_THREADS;  // warps 0-11
-constexpr int WARP_TILES = COMPUTE_THREADS / 32;         // warps 8-9: tile loads and stores
+constexpr int GROUPS = 4;                                // four tiles in flight per CTA
+constexpr int COMPUTE_THREADS = GROUPS * GROUP_THREADS;  // warps 0-15
+constexpr int WARP_TILES = COMPUTE_THREADS / 32;         // warps 16-17: tile loads and stores
 constexpr int TILE_THREADS = 64;
-constexpr int WARP_OPS = WARP_TILES + 2;                 // warp 10: B operand images
+constexpr int WARP_OPS = WARP_TILES + 2;                 // warp 18: B operand images
 constexpr int THREADS = COMPUTE_THREADS + TILE_THREADS + 32;
 constexpr int TILE = 1 << TILE_BITS;
 constexpr uint32_t TILE_BYTES = uint32_t(TILE) * 8u;
 constexpr int OPERAND_BYTES = 16384;  // B: bf16 hi (8 KB) + lo (8 KB)
 constexpr int NTILEBUF = GROUPS + 1;  // tile buffers rotating over the CTA's tiles (one loading ahead)
-constexpr int NOPSLOT = 4;            // B operand slots rotating over the unitary uses
+constexpr int NOPSLOT = 3;            // B operand slots rotating over the unitary uses
 constexpr int SM_B = 0;
 constexpr int SM_TILE0 = SM_B + NOPSLOT * OPERAND_BYTES;
 constexpr int SM_TOTAL = SM_TILE0 + NTILEBUF * int(TILE_BYTES);
