@@ -434,6 +434,16 @@ struct Lock {
   std::lock_guard<std::recursive_mutex> g;
   explicit Lock(const ncsim_sparse* s) : g(s->mu) { NCSIM_CUDA(cudaSetDevice(s->device)); }
 };
+// two states locked together without an order between them (no deadlock when
+// other threads lock the same pair the other way round); a's device current
+struct PairLock {
+  std::unique_lock<std::recursive_mutex> la, lb;
+  PairLock(const ncsim_sparse* a, const ncsim_sparse* b) : la(a->mu, std::defer_lock), lb(b->mu, std::defer_lock) {
+    if (a == b) la.lock();
+    else std::lock(la, lb);
+    NCSIM_CUDA(cudaSetDevice(a->device));
+  }
+};
 
 template <class T>
 T* dalloc(size_t count, cudaStream_t st) {
@@ -1186,9 +1196,7 @@ ncsim_status ncsim_sparse_inner(const ncsim_sparse* a, const ncsim_sparse* b, do
     need(b, "b");
     need(re_im, "out");
     if (a->n != b->n) throw Error(NCSIM_ERR_INVALID, "inner: register sizes differ");
-    Lock la(a);
-    std::unique_lock<std::recursive_mutex> lb(b->mu, std::defer_lock);
-    if (a != b) lb.lock();
+    PairLock lk(a, b);
     NCSIM_CUDA(cudaStreamSynchronize(b->stream));
     uint64_t* kb = b->key;
     double2* vb = b->amp;
@@ -1242,9 +1250,7 @@ ncsim_status ncsim_sparse_tensor(const ncsim_sparse* a, const ncsim_sparse* b, n
     need(b, "b");
     need(out, "out");
     if (a->n + b->n > 64) throw Error(NCSIM_ERR_UNSUPPORTED, "sparse tensor product of more than 64 qubits");
-    Lock la(a);
-    std::unique_lock<std::recursive_mutex> lb(b->mu, std::defer_lock);
-    if (a != b) lb.lock();
+    PairLock lk(a, b);
     NCSIM_CUDA(cudaStreamSynchronize(a->stream));
     NCSIM_CUDA(cudaStreamSynchronize(b->stream));
     const uint64_t tot = a->m * b->m;
