@@ -283,13 +283,20 @@ bool is_gate(const QOp& o) { return o.code == OP_GATE || o.code == OP_BGATE; }
 // that no later taken gate on its qubits follows, while the program still has
 // a gate on one of them (later[i]), is put back: it waits for the stage of
 // that gate, which absorbs its signs.
+// Once every qubit of the register (full) is blocked for every op, nothing later
+// can be taken: the rest of the list is copied to `rest` at once.
 template <class Ok>
 void schedule(const std::vector<uint32_t>& pend, const std::vector<QOp>& ops, const std::vector<char>& later, Ok ok,
-              std::vector<uint32_t>& taken, std::vector<uint32_t>& rest) {
+              uint64_t full, std::vector<uint32_t>& taken, std::vector<uint32_t>& rest) {
   taken.clear();
   rest.clear();
   uint64_t block_all = 0, block_gates = 0;
-  for (uint32_t i : pend) {
+  for (size_t pi = 0; pi < pend.size(); ++pi) {
+    if ((block_all & full) == full) {
+      rest.insert(rest.end(), pend.begin() + long(pi), pend.end());
+      break;
+    }
+    const uint32_t i = pend[pi];
     const QOp& o = ops[i];
     const uint64_t m = qmask(o);
     if (is_gate(o)) {
@@ -348,6 +355,7 @@ void compile_one(const Trajectory& t, const PlanKnobs& kn, Local& L) {
   for (size_t w = 0; w < ws.size(); ++w)
     for (uint32_t b = 0; b < TILE_BITS; ++b) wpos[w][ws[w][b]] = int(b);
   const uint64_t ntiles = uint64_t(1) << (n - TILE_BITS);
+  const uint64_t full = n >= 64 ? ~uint64_t(0) : (uint64_t(1) << n) - 1;
 
   auto add_pass = [&](size_t w, uint8_t flags) -> DevPass& {
     DevPass p{};
@@ -381,11 +389,11 @@ void compile_one(const Trajectory& t, const PlanKnobs& kn, Local& L) {
     std::vector<uint32_t> best_t, best_r;
     for (size_t k = 0; k < ws.size(); ++k) {
       const size_t w = kn.greedy_windows ? k : (turn + k) % ws.size();
-      schedule(pend, t.ops, later, [&](const QOp& o) { return !is_gate(o) || wpos[w][o.a] >= 0; }, taken, rest);
+      schedule(pend, t.ops, later, [&](const QOp& o) { return !is_gate(o) || wpos[w][o.a] >= 0; }, full, taken, rest);
       if (taken.size() > best_t.size()) {
         best_w = w;
-        best_t = taken;
-        best_r = rest;
+        best_t.swap(taken);  // (taken and rest are cleared by the next schedule)
+        best_r.swap(rest);
         if (!kn.greedy_windows) break;
       }
     }
@@ -414,13 +422,13 @@ void compile_one(const Trajectory& t, const PlanKnobs& kn, Local& L) {
         const uint32_t r = kn.greedy_stages ? k : (cyc + k) % NSEL;
         const int lo = int(RSHIFT[r]), hi = lo + int(REG_BITS);
         schedule(sp, t.ops, later,
-                 [&](const QOp& o) { return !is_gate(o) || (wpos[w][o.a] >= lo && wpos[w][o.a] < hi); }, staken,
-                 srest);
+                 [&](const QOp& o) { return !is_gate(o) || (wpos[w][o.a] >= lo && wpos[w][o.a] < hi); }, full,
+                 staken, srest);
         const size_t g = gate_count(staken, t.ops);
         if (bt.empty() || g > bg || (g == bg && staken.size() > bt.size())) {
           best_r_sel = r;
-          bt = staken;
-          br = srest;
+          bt.swap(staken);
+          br.swap(srest);
           bg = g;
           if (!kn.greedy_stages && !staken.empty()) break;
         }
@@ -513,39 +521,33 @@ Program compile(const std::vector<Trajectory>& ts, const PlanKnobs& knobs) {
   for (auto& e : errs)
     if (!e.empty()) throw Error(NCSIM_ERR_INVALID, e);
 
+  // the trajectories' places in the program (prefix sums), then their parts copied
+  // in parallel into the sized (uninitialised) arrays
   Program P;
-  size_t np = 0, ns = 0, no = 0, nd = 0;
+  std::vector<size_t> p0(ts.size() + 1, 0), s0(ts.size() + 1, 0), o0(ts.size() + 1, 0), d0(ts.size() + 1, 0);
   for (size_t i = 0; i < ts.size(); ++i) {
-    np += loc[i].pass.size();
-    ns += loc[i].stage.size();
-    no += loc[i].op.size();
-    nd += ts[i].draws.size();
+    p0[i + 1] = p0[i] + loc[i].pass.size();
+    s0[i + 1] = s0[i] + loc[i].stage.size();
+    o0[i + 1] = o0[i] + loc[i].op.size();
+    d0[i + 1] = d0[i] + ts[i].draws.size();
   }
-  P.pass.reserve(np);
-  P.stage.reserve(ns);
-  P.op.reserve(no);
-  P.draws.reserve(nd);
+  if (o0.back() > UINT32_MAX || s0.back() > UINT32_MAX || d0.back() > UINT32_MAX)
+    throw Error(NCSIM_ERR_UNSUPPORTED, "batch program too large (more than 2^32 ops, stages or draws)");
+  P.pass.resize(p0.back());
+  P.stage.resize(s0.back());
+  P.op.resize(o0.back());
+  P.draws.resize(d0.back());
+  P.traj.resize(ts.size());
   for (size_t i = 0; i < ts.size(); ++i) {
     const Trajectory& t = ts[i];
-    Local& L = loc[i];
-    DevTraj d{};
+    const Local& L = loc[i];
+    DevTraj& d = P.traj[i];
+    d = DevTraj{};
     d.n = t.n;
     d.npass = uint32_t(L.pass.size());
-    d.pass0 = uint32_t(P.pass.size());
-    d.draw0 = uint32_t(P.draws.size());
+    d.pass0 = uint32_t(p0[i]);
+    d.draw0 = uint32_t(d0[i]);
     d.nmeas = t.nmeas;
-    const uint32_t s0 = uint32_t(P.stage.size()), o0 = uint32_t(P.op.size());
-    for (auto p : L.pass) {
-      p.stage0 += s0;
-      P.pass.push_back(p);
-    }
-    for (auto s : L.stage) {
-      s.op0 += o0;
-      P.stage.push_back(s);
-    }
-    P.op.insert(P.op.end(), L.op.begin(), L.op.end());
-    P.draws.insert(P.draws.end(), t.draws.begin(), t.draws.end());
-    P.traj.push_back(d);
     P.source_gates += t.source_gates;
     P.noise_events += t.noise_events;
     P.folded_ops += t.ops.size();
@@ -554,6 +556,28 @@ Program compile(const std::vector<Trajectory>& ts, const PlanKnobs& knobs) {
     P.state_bytes += L.bytes;
     P.max_n = std::max(P.max_n, t.n);
   }
+  next = 0;
+  auto copy = [&] {
+    for (size_t i; (i = next.fetch_add(1)) < ts.size();) {
+      const Local& L = loc[i];
+      for (size_t k = 0; k < L.pass.size(); ++k) {
+        DevPass p = L.pass[k];
+        p.stage0 += uint32_t(s0[i]);
+        P.pass[p0[i] + k] = p;
+      }
+      for (size_t k = 0; k < L.stage.size(); ++k) {
+        DevStage s = L.stage[k];
+        s.op0 += uint32_t(o0[i]);
+        P.stage[s0[i] + k] = s;
+      }
+      if (!L.op.empty()) std::memcpy(&P.op[o0[i]], L.op.data(), L.op.size() * sizeof(DevOp));
+      if (!ts[i].draws.empty()) std::memcpy(&P.draws[d0[i]], ts[i].draws.data(), ts[i].draws.size() * sizeof(double));
+    }
+  };
+  th.clear();
+  for (unsigned k = 1; k < nth; ++k) th.emplace_back(copy);
+  copy();
+  for (auto& x : th) x.join();
   return P;
 }
 

@@ -23,6 +23,8 @@
 #pragma once
 
 #include <cstdint>
+#include <memory>
+#include <utility>
 #include <vector>
 
 #include "host/ir.hpp"
@@ -98,12 +100,33 @@ struct PlanKnobs {
   bool greedy_stages = true;   // pick the register set that takes most gates (else cycle)
 };
 
+// an allocator whose resize leaves trivially constructible elements
+// uninitialised (the program's arrays are filled in parallel after sizing)
+template <class T>
+struct UninitAlloc : std::allocator<T> {
+  template <class U>
+  struct rebind {
+    using other = UninitAlloc<U>;
+  };
+  UninitAlloc() = default;
+  template <class U>
+  UninitAlloc(const UninitAlloc<U>&) noexcept {}
+  template <class U>
+  void construct(U*) noexcept {}
+  template <class U, class... A>
+  void construct(U* p, A&&... a) {
+    ::new (static_cast<void*>(p)) U(std::forward<A>(a)...);
+  }
+};
+template <class T>
+using ProgVec = std::vector<T, UninitAlloc<T>>;
+
 struct Program {
   std::vector<DevTraj> traj;
-  std::vector<DevPass> pass;
-  std::vector<DevStage> stage;
-  std::vector<DevOp> op;
-  std::vector<double> draws;
+  ProgVec<DevPass> pass;
+  ProgVec<DevStage> stage;
+  ProgVec<DevOp> op;
+  ProgVec<double> draws;
   uint64_t source_gates = 0, noise_events = 0, folded_ops = 0, tile_passes = 0, tile_stages = 0;
   uint32_t max_n = 0;
   // algorithmic HBM bytes of one run: per pass 2 * 8 * 2^n (one read of 8 * 2^n
