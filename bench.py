@@ -174,40 +174,91 @@ def host_mem_available() -> int:
     return 0
 
 
+def layer_sample_text(n: int, depth: int, seed: int, ones: int) -> str:
+    """A sample of the random layer circuit with its own gate mix: from each
+    layer in turn, its next one-qubit gates and CZ gates in the layer's 2:1
+    ratio (`ones` one-qubit gates and ones // 2 CZ gates in all), in circuit
+    order.  Run from |+>^n, every gate acts on a dense register."""
+    from oracle import oracle as O
+
+    lines = O.random_circuit_text(n, depth, seed).strip().split("\n")
+    per = n + n // 2
+    body = lines[1:]
+    out, want1, want2 = [], ones, ones // 2
+    for L in range(depth):
+        layer = body[L * per:(L + 1) * per]
+        one = [ln for ln in layer if not ln.startswith("CZ ")]
+        two = [ln for ln in layer if ln.startswith("CZ ")]
+        a, b = min(want1, len(one)), min(want2, len(two))
+        out += one[:a] + two[:b]
+        want1 -= a
+        want2 -= b
+        if want1 <= 0 and want2 <= 0:
+            break
+    return lines[0] + "\n" + "\n".join(out) + "\n"
+
+
 def cpu_baseline(n_want: int, depth: int, seed: int, budget_s: float = 15.0):
     """The oracle (C++ restatement of the reference's StateVector, all host
-    threads) on a bounded sample of the same workload: the first G gates of
-    the same circuit from |+>^n, timed; G grows until the sample takes about
-    budget_s seconds."""
+    threads) on a bounded sample of the same workload: one-qubit gates and CZ
+    gates of the same circuit in its 2:1 ratio, applied to a dense register
+    (|+>^n), complex128.  The sample grows until it takes about budget_s."""
     from oracle import oracle as O
 
     avail = host_mem_available()
     n = n_want
     while n > 20 and (16 << n) * 1.3 > avail:
         n -= 1
-    text = O.random_circuit_text(n, depth, seed)
-    circ = O.Circuit(text)
     s = O.StateVector.plus_state(n)
-    done, elapsed, g = 0, 0.0, 1
-    total_gates = circ.num_gates
-    while elapsed < budget_s and done < total_gates:
-        g = min(g, total_gates - done)
-        # each call restarts at the circuit's first gate: the sample is the first g gates
-        dt = s.run_gates_timed(circ, g)
-        elapsed += dt
-        done += g
-        per = dt / g
-        g = max(1, int(min(budget_s - elapsed, budget_s / 3) / max(per, 1e-9)))
+    ones, elapsed, gates = 2, 0.0, 0
+    while True:
+        text = layer_sample_text(n, depth, seed, ones)
+        c = O.Circuit(text)
+        dt = s.run_gates_timed(c, c.num_gates)
+        elapsed, gates = dt, c.num_gates
+        if dt >= budget_s / 3 or ones >= 4 * n:
+            break
+        ones = max(ones + 2, int(ones * min(8.0, budget_s / 3 / max(dt, 1e-3))))
+        ones += ones & 1
+    n1 = sum(1 for ln in text.split("\n")[1:] if ln and not ln.startswith("CZ "))
     return {
-        "value": done / elapsed,
+        "value": gates / elapsed,
         "unit": "gates/s",
         "cores": O.lib().oracle_num_threads(),
         "kind": "port",
-        "sample": f"oracle StateVector<C64> at n={n}: {done} gates of the random layer circuit "
-                  f"(depth {depth}, seed {seed}) from |+>^n in {elapsed:.1f} s"
+        "sample": f"oracle StateVector<C64> (complex128) at n={n}: {gates} gates of the random layer circuit "
+                  f"(depth {depth}, seed {seed}) in its own mix ({n1} one-qubit, {gates - n1} CZ), on a dense "
+                  f"register (|+>^n), in {elapsed:.1f} s"
                   + ("" if n == n_want else f" (n reduced from {n_want} to fit host memory)"),
         "n": n,
     }
+
+
+def published_workload_text(n: int) -> str:
+    """The reference's published StateVector workload (examples/bench.rs:120-137):
+    H on every qubit, then for q in 0..n: T q, CX q (q+1)%n, CCZ q (q+1)%n (q+2)%n,
+    RX(0.3) q."""
+    h = "".join(f"H {q}\n" for q in range(n))
+    layer = "".join(f"T {q}\nCX {q} {(q + 1) % n}\nCCZ {q} {(q + 1) % n} {(q + 2) % n}\nRX(0.3) {q}\n"
+                    for q in range(n))
+    return f"QUBITS {n}\n", h, layer
+
+
+def published_workload_cpu(n: int = 22, reps: int = 3):
+    """The same workload on the oracle (host threads): seconds for the 4n-gate layer
+    and for one expectation of X0*Y3*Z5."""
+    from oracle import oracle as O
+
+    hdr, h, layer = published_workload_text(n)
+    s = O.StateVector(n)
+    s.run(O.Circuit(hdr + h), O.StdRng(0))
+    c = O.Circuit(hdr + layer)
+    t_layer = min(s.run_gates_timed(c, c.num_gates) for _ in range(reps))
+    t0 = time.perf_counter()
+    for _ in range(20):
+        s.expectation("X0*Y3*Z5")
+    t_exp = (time.perf_counter() - t0) / 20
+    return {"layer_s": t_layer, "expectation_s": t_exp, "cores": O.lib().oracle_num_threads(), "kind": "port"}
 
 
 def run_reference(args):
@@ -247,6 +298,7 @@ def run_reference(args):
     }
     if not args.no_trajectories:
         tr = cpu_trajectories(30, 1e-3, args.cpu_budget * 2 / 3)
+        tr.pop("results")
         line["trajectories"] = {"metric": "trajectories/s", "value": tr["value"], "unit": "trajectories/s",
                                 "cpu_baseline": tr,
                                 "e2e": {"value": tr["value"], "unit": "trajectories/s",
@@ -255,21 +307,57 @@ def run_reference(args):
     return 0
 
 
-def cpu_trajectories(depth: int, p: float, budget_s: float = 10.0):
+def cpu_trajectories(depth: int, p: float, budget_s: float = 10.0, seed0: int = 1):
     """The oracle's noisy trajectories (FP64, the reference's StateVector
-    semantics, all host threads) on the host cores: seeds 1, 2, ... until
-    about budget_s seconds have passed."""
+    semantics, all host threads) on the host cores: seeds seed0, seed0+1, ...
+    until about budget_s seconds have passed.  `results` holds each one's
+    (n, <Z0>/norm before the measurements, record)."""
     from oracle import oracle as O
 
     t0 = time.perf_counter()
-    done = 0
+    results = []
     while time.perf_counter() - t0 < budget_s:
-        O.trajectory(1 + done, 16, 7, depth, p)
-        done += 1
+        results.append(O.trajectory(seed0 + len(results), 16, 7, depth, p))
     dt = time.perf_counter() - t0
+    done = len(results)
     return {"value": done / dt, "unit": "trajectories/s", "cores": O.lib().oracle_num_threads(), "kind": "port",
-            "sample": f"oracle trajectories seeds 1..{done} (n = 16 + gen_range(0..7), depth {depth}, "
-                      f"DEPOLARIZE2({p}), M on every qubit) in {dt:.1f} s"}
+            "sample": f"oracle trajectories seeds {seed0}..{seed0 + done - 1} (n = 16 + gen_range(0..7), depth "
+                      f"{depth}, DEPOLARIZE2({p}), M on every qubit) in {dt:.1f} s",
+            "results": results}
+
+
+def trajectory_fp64_reference(nb, count: int, seed0: int, depth: int, p: float, workers: int = 8):
+    """<Z0>/<psi|psi> before the final measurements and the record of
+    trajectories 0..count-1 (StdRng(seed0 + t)) on the plain complex128 path,
+    from `workers` host threads (one register per size and thread, so the
+    small registers' kernels overlap)."""
+    import concurrent.futures as cf
+
+    import numpy as np
+
+    z = np.empty(count)
+    rec = np.empty(count, dtype=np.uint64)
+
+    def work(start):
+        states, meas = {}, {}
+        for t in range(start, count, workers):
+            rng = nb.StdRng(seed0 + t)
+            n = 16 + rng.gen_range(0, 7)
+            c = nb.Circuit.random_layers_from(rng, n, depth, p, 0, 0)
+            s = states.get(n)
+            if s is None:
+                s = states[n] = nb.GpuStateVector(n, nb.C128)
+                meas[n] = nb.Circuit.parse(f"QUBITS {n}\n" + "".join(f"M {q}\n" for q in range(n)))
+            else:
+                s.set_basis(0)
+            s.run(c, rng)
+            z[t] = s.expectation(nb.Pauli(n, 0, 1, 0)).real / s.norm_sq().real
+            r = s.run(meas[n], rng)
+            rec[t] = sum(int(v) << k for k, v in enumerate(r))
+
+    with cf.ThreadPoolExecutor(workers) as ex:
+        list(ex.map(work, range(workers)))
+    return z, rec
 
 
 def trajectory_bench(nb, args, dist, peak, peak_kind):
@@ -319,31 +407,21 @@ def trajectory_bench(nb, args, dist, peak, peak_kind):
                      "algorithmic_bytes_per_launch": info["state_bytes"]},
         "host_build_s": build_s,
     }
-    # accuracy: a strided sample against FP64 plain-path runs of the same draws
-    sample = list(range(0, count, max(1, count // max(1, args.traj_check))))[: args.traj_check]
-    errs, z_b, z_r, same = [], [], [], 0
-    for t in sample:
-        rng = nb.StdRng(seed0 + t)
-        n = 16 + rng.gen_range(0, 7)
-        c = nb.Circuit.random_layers_from(rng, n, depth, p, 0, 0)
-        s = nb.GpuStateVector(n, nb.C128)
-        s.run(c, rng)
-        zr = s.expectation(nb.Pauli(n, 0, 1, 0)).real / s.norm_sq().real
-        m = nb.Circuit.parse(f"QUBITS {n}\n" + "".join(f"M {q}\n" for q in range(n)))
-        rr = s.run(m, rng)
-        same += int(rec[t]) == sum(int(v) << k for k, v in enumerate(rr))
-        errs.append(abs(z0[t] - zr))
-        z_b.append(z0[t])
-        z_r.append(zr)
-        del s
-    if sample:
+    # accuracy: every trajectory against a complex128 run of the same draws on the plain path
+    if args.traj_check:
+        t1 = time.perf_counter()
+        check = min(count, args.traj_check)
+        z_ref, rec_ref = trajectory_fp64_reference(nb, check, seed0, depth, p)
+        zb = z0[:check]
+        same = int((rec[:check] == rec_ref).sum())
         out["accuracy"] = {
-            "reference": "plain complex128 path (FP64) on the same draws",
-            "sample": len(sample),
-            "mean_z0_error": abs(statistics.mean(z_b) - statistics.mean(z_r)),
-            "max_z0_error": max(errs),
-            "records_identical": f"{same}/{len(sample)}",
+            "reference": "plain complex128 path (FP64) per trajectory, same draws (StdRng(seed0 + t))",
+            "trajectories": check,
+            "mean_z0_error": abs(float(zb.mean()) - float(z_ref.mean())),
+            "max_z0_error": float(abs(zb - z_ref).max()),
+            "records_identical": f"{same}/{check}",
             "mean_norm_drift": float(abs(norm - 1.0).mean()),
+            "check_s": round(time.perf_counter() - t1, 1),
         }
     if not args.no_e2e:
         def e2e_step():
@@ -364,7 +442,16 @@ def trajectory_bench(nb, args, dist, peak, peak_kind):
                       "note": "per step: generate and compile the trajectories on the host, upload the "
                               "program, run, copy records, <Z0> and norms back; host wall clock"}
     if RANK == 0 and WORLD == 1 and not args.no_cpu_baseline:
-        out["cpu_baseline"] = cpu_trajectories(depth, p, args.cpu_budget * 2 / 3)
+        cpu = cpu_trajectories(depth, p, args.cpu_budget * 2 / 3, seed0)
+        res = cpu.pop("results")
+        if res:
+            errs = [abs(z0[t] - zo) for t, (_, zo, _) in enumerate(res)]
+            same = sum(int(rec[t]) == sum(int(v) << k for k, v in enumerate(ro)) for t, (_, _, ro) in enumerate(res))
+            out["accuracy_oracle"] = {"reference": "the CPU oracle (FP64 restatement of StateVector) on the same "
+                                                   "draws: the CPU baseline's trajectories",
+                                      "trajectories": len(res), "max_z0_error": max(errs),
+                                      "records_identical": f"{same}/{len(res)}"}
+        out["cpu_baseline"] = cpu
     return out
 
 
@@ -376,8 +463,8 @@ def config_rates(nb, peak, peak_kind):
     the launch profiler's algorithmic bytes over a separate profiled run."""
     out = {}
 
-    def measure(name, n, circuit, runs, extra=None):
-        s = nb.GpuStateVector(n)
+    def measure(name, n, circuit, runs, extra=None, init_plus=False):
+        s = nb.GpuStateVector.plus_state(n) if init_plus else nb.GpuStateVector(n)
         rng = nb.StdRng(11)
         if runs:
             s.run(circuit, rng)  # warm-up (and the gate graphs' capture)
@@ -421,6 +508,52 @@ def config_rates(nb, peak, peak_kind):
     measure("C1", 30, nb.Circuit.random_layers(30, 20, 1, 0.0, 26, 30), 2)
     c3 = nb.Circuit.reversible(31, 2000, 1)
     measure("C3", 31, c3, 0)
+    # From |0...0> the register holds 2^16 nonzero amplitudes of 2^31, and the diagonal
+    # kernels write only nonzero ones, so bytes per second of that run are not a
+    # roofline.  The kernels' roofline is taken on a dense register instead: the same
+    # 2016 gates from |+>^31.
+    c3r = out["C3"]
+    c3r["hbm_frac_of_kernel_time"] = None
+    c3r["note"] = ("sparse register (2^16 of 2^31 amplitudes nonzero): per-kernel GB/s omitted; see "
+                   "C3_dense_register for the kernels' roofline")
+    c3r["kernels"] = {k: {"launches": v["launches"], "ms": v["ms"]} for k, v in c3r["kernels"].items()}
+    measure("C3_dense_register", 31, c3, 0, init_plus=True)
+
+    # the reference's published StateVector workload (examples/bench.rs:120-143; README.md:210-211:
+    # 0.10 s for the 88-gate layer and 1.4 ms per expectation at n = 22 on a 16-thread desktop)
+    n = 22
+    hdr, h, layer = published_workload_text(n)
+    s = nb.GpuStateVector(n)
+    s.run(nb.Circuit.parse(hdr + h), nb.StdRng(0))
+    lc = nb.Circuit.parse(hdr + layer)
+    rng = nb.StdRng(0)
+    s.timer_start()
+    s.run(lc, rng)  # a circuit's first run launches kernel by kernel
+    one_shot = s.timer_stop()
+    s.run(lc, rng)  # the second captures its gate graph
+    reps = 20
+    s.timer_start()
+    for _ in range(reps):
+        s.run(lc, rng)
+    replay = s.timer_stop() / reps
+    pz = nb.Pauli.from_string(n, "X0*Y3*Z5")
+    s.expectation(pz)
+    t0 = time.perf_counter()
+    for _ in range(20):
+        s.expectation(pz)
+    exp_s = (time.perf_counter() - t0) / 20
+    del s
+    pub = {"workload": "n=22 complex128: H on every qubit, then for q in 0..22: T q, CX q q+1, CCZ q q+1 q+2, "
+                       "RX(0.3) q (88 gates); 20 expectations of X0*Y3*Z5",
+           "layer_ms_first_run": one_shot, "layer_ms_replayed": replay, "layer_gates_per_s": 4 * n / (one_shot / 1e3),
+           "expectation_ms": exp_s * 1e3,
+           "published": {"layer_s": 0.10, "expectation_s": 1.4e-3, "hardware": "16-thread desktop (README.md:202)"},
+           "vs_published_layer": 0.10 / (one_shot / 1e3), "vs_published_expectation": 1.4e-3 / exp_s}
+    if RANK == 0 and WORLD == 1:
+        cpu = published_workload_cpu(n)
+        pub["cpu_oracle"] = cpu
+        pub["vs_cpu_oracle_layer"] = cpu["layer_s"] / (one_shot / 1e3)
+    out["published_n22"] = pub
 
     # the same C3 circuit on the sparse form (SparseVector: 2^16 entries instead of 2^31 amplitudes)
     sp = nb.GpuSparseVector(31)
@@ -488,8 +621,10 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--traj-count", type=int, default=4096)
-    ap.add_argument("--traj-check", type=int, default=32)
+    ap.add_argument("--traj-check", type=int, default=4096,
+                    help="trajectories checked against complex128 plain-path runs (0: none)")
     ap.add_argument("--no-trajectories", action="store_true")
+    ap.add_argument("--no-capacity", action="store_true", help="skip the n = 34 complex64 capacity run")
     ap.add_argument("--traj-launch", default="",
                     help="CTAS_PER_SM,BUFFERS: a fixed launch configuration of the batch kernel (default: tuned)")
     ap.add_argument("--no-configs", action="store_true", help="skip the C0, C1 and C3 plain-path rates")
@@ -556,7 +691,7 @@ def main():
     dom_name, dom_v = dom
     achieved = dom_v["bytes"] / (dom_v["ms"] / 1e3) / 1e9
     total_bytes = sum(v["bytes"] for v in prof.values())
-    overall = total_bytes / (ms / 1e3) / 1e9
+    overall = total_bytes / (ms / args.steps / 1e3) / 1e9  # the profiled step's bytes over one step's time
     traffic = profiled_traffic(dom_name)
     roofline = {
         "bound": "hbm",
@@ -574,22 +709,32 @@ def main():
     result["kernels"] = {k: {"launches": v["launches"], "ms": round(v["ms"], 3),
                              "GBps": round(v["bytes"] / max(v["ms"], 1e-9) / 1e6, 1)} for k, v in prof.items()}
 
-    # the FP64 comparison arm and the fidelity of the fused result
+    # The FP64 arm: the same circuit on the plain complex128 path.  Its first run from
+    # |0...0> is also the reference of the fused result's fidelity; its second run, on
+    # the dense register the first left, is timed (the regime of the fused steps).
+    head = {}
     if path == "fused":
         ref = nb.GpuStateVector(n, nb.C128)
-        ms_p, prof_p = timed_runs(nb, ref, circuit, 1, 1, False, None)
-        result["plain_fp64"] = {"gates_per_s": gates / (ms_p / 1e3), "ms_per_circuit": ms_p}
-        del ref
+        ref.run(circuit, nb.StdRng(7))
         fz = nb.GpuStateVector(n, nb.C64)
-        ref64 = nb.GpuStateVector(n, nb.C128)
-        rng_a, rng_b = nb.StdRng(7), nb.StdRng(7)
-        ref64.run(circuit, rng_a)
-        fz.run_fused(circuit, rng_b)
-        cmpd = ref64.compare(fz)
+        fz.run_fused(circuit, nb.StdRng(7))
+        cmpd = ref.compare(fz)
+        del fz
+        ref.synchronize()
+        ref.timer_start()
+        ref.run(circuit, nb.StdRng(7))
+        ms_p = ref.timer_stop()
+        del ref
+        fp64 = gates / (ms_p / 1e3)
+        head = {"fp64_gates_per_s": round(fp64, 2),
+                "speedup_vs_fp64": round(value / WORLD / fp64, 3),
+                "infidelity": cmpd["infidelity"],
+                "max_abs_err": cmpd["max_abs_diff"]}
+        result["plain_fp64"] = {"gates_per_s": fp64, "ms_per_circuit": ms_p,
+                                "note": "plain one-kernel-per-gate path, complex128, same circuit, dense register"}
         result["fidelity"] = {"infidelity": cmpd["infidelity"], "max_abs_diff": cmpd["max_abs_diff"],
-                              "norm_fused": cmpd["norm_b"]}
-        result["speedup_vs_fp64"] = value / WORLD / result["plain_fp64"]["gates_per_s"]
-        del fz, ref64
+                              "norm_fused": cmpd["norm_b"],
+                              "reference": "plain complex128 run of the identical circuit from |0...0>"}
 
     # end to end through the C ABI: host circuit text in, readouts out
     e2e = None
@@ -623,14 +768,26 @@ def main():
                        "64 amplitudes; host wall clock"}
         del e2e_state
 
+    # capacity: the fused form at n = 34 (complex64, 128 GiB), beyond the reference's
+    # n <= 30; its circuit and then the inverse circuit must bring |0...0> back
+    if path == "fused" and not args.no_capacity:
+        result["capacity"] = capacity_run(nb, args.depth)
+        if "gates_per_s" in result["capacity"]:
+            head["capacity_n34_gates_per_s"] = round(result["capacity"]["gates_per_s"], 2)
+
     cpu = None
     if RANK == 0 and WORLD == 1 and not args.no_cpu_baseline:
-        cpu = cpu_baseline(n if path == "plain" else args.n, args.depth, seed, args.cpu_budget)
+        cpu = cpu_baseline(n, args.depth, seed, args.cpu_budget)
+        if "fp64_gates_per_s" in head:
+            head["fp64_vs_cpu"] = round(head["fp64_gates_per_s"] / cpu["value"], 1)
 
     if not args.no_trajectories:
         with ClockSampler() as tclk:
             result["trajectories"] = trajectory_bench(nb, args, dist, peak, peak_kind)
         result["trajectories"]["clocks"] = tclk.summary()
+        acc = result["trajectories"].get("accuracy")
+        if acc:
+            head["traj_mean_z0_error"] = acc["mean_z0_error"]
     if not args.no_configs and WORLD == 1:
         result["configs"] = config_rates(nb, peak, peak_kind)
 
@@ -646,6 +803,9 @@ def main():
         "higher_is_better": True,
         "scaling": "weak",
         "vs_baseline": None,
+    }
+    line.update(head)  # the short comparison keys early in the line
+    line.update({
         "dtype": "f32" if path == "fused" else "f64",
         "data": "synthetic",
         "config": {
@@ -664,7 +824,7 @@ def main():
         "clocks": clocks,
         "gpu_launches": launches * args.steps,  # the profiled step launches what each timed step does
         "gpu_launches_per_step": launches,
-    }
+    })
     line.update(result)
     if RANK == 0:
         print(json.dumps(line), flush=True)
@@ -672,6 +832,42 @@ def main():
         dist.barrier()
         dist.destroy_process_group()
     return 0
+
+
+def inverse_text(text: str) -> str:
+    """The inverse of a random layer circuit: gates in reverse order, each replaced by its inverse."""
+    inv = {"H": "H", "S": "S_DAG", "T": "T_DAG", "SQRT_X": "SQRT_X_DAG", "CZ": "CZ"}
+    lines = text.strip().split("\n")
+    out = [lines[0]]
+    for ln in reversed(lines[1:]):
+        name, rest = ln.split(" ", 1)
+        out.append(f"RZ({-float(name[3:-1])!r}) {rest}" if name.startswith("RZ(") else f"{inv[name]} {rest}")
+    return "\n".join(out) + "\n"
+
+
+def capacity_run(nb, depth: int, n: int = 34):
+    """The fused form at n = 34 (complex64, 128 GiB): the random layer circuit
+    (device time on the state's stream), the norm after it, then the inverse
+    circuit, after which the register should be |0...0> again."""
+    free = nb.device_info()["free_bytes"]
+    if free < (8 << n) + (4 << 30):
+        return {"n": n, "skipped": f"needs {(8 << n) / 2**30:.0f} GiB, {free / 2**30:.0f} GiB free"}
+    c = nb.Circuit.random_layers(n, depth, 1)
+    ci = nb.Circuit.parse(inverse_text(c.to_text()))
+    s = nb.GpuStateVector(n, nb.C64)
+    s.run_fused(c, nb.StdRng(0))  # plans the circuit (host) and warms up
+    s.set_basis(0)
+    s.timer_start()
+    _, st = s.run_fused(c, nb.StdRng(0))
+    ms = s.timer_stop()
+    nn = s.norm_sq().real
+    s.run_fused(ci, nb.StdRng(0))
+    back = 1.0 - abs(s.amplitude(0)) ** 2
+    del s
+    return {"n": n, "precision": "complex64 (128 GiB)", "gates": c.num_gates, "passes": st.passes,
+            "ms_per_circuit": ms, "gates_per_s": c.num_gates / (ms / 1e3), "norm_drift": abs(nn - 1.0),
+            "round_trip_infidelity": back,
+            "note": "from |0...0>: the circuit (timed), <psi|psi>, then its inverse; 1 - |<0|psi>|^2 after both"}
 
 
 if __name__ == "__main__":

@@ -72,6 +72,15 @@ const char* ncsim_last_error(void);
 int32_t ncsim_abi_version(void);
 /* Streaming multiprocessors, free and total device memory of the current device. */
 ncsim_status ncsim_device_info(int32_t* sm_count, uint64_t* free_bytes, uint64_t* total_bytes);
+/* Temporaries (readouts, staging, the sparse form's sort buffers) come from a
+ * stream-ordered pool that the library creates per device and that keeps
+ * freed memory for the next call; the device's default pool is not touched.
+ * This gives the kept memory of every such pool back to the device (call it
+ * when no library work is queued). */
+ncsim_status ncsim_trim_memory(void);
+/* Bytes the current device's library pool holds from the device, and bytes of
+ * it in use by queued or running library calls. */
+ncsim_status ncsim_pool_info(uint64_t* reserved_bytes, uint64_t* used_bytes);
 
 /* ======================================================================
  * 1. State operations (the QuantumState<C64> boundary)
@@ -96,6 +105,9 @@ ncsim_status ncsim_sv_set_plus(ncsim_state* s);
 ncsim_status ncsim_sv_set_amplitudes(ncsim_state* s, const double* amps, uint64_t len);
 /* All 2^n amplitudes to host memory as complex128 (to_vector, vector.rs:542-544). */
 ncsim_status ncsim_sv_get_amplitudes(const ncsim_state* s, double* amps, uint64_t len);
+/* Amplitudes first .. first+count-1 as complex128 (a slice of to_vector, for
+ * registers too large to copy to the host at once). */
+ncsim_status ncsim_sv_get_amplitudes_range(const ncsim_state* s, uint64_t first, uint64_t count, double* amps);
 /* One amplitude <x|psi> (QuantumState::amplitude, vector.rs:408-410). */
 ncsim_status ncsim_sv_get_amplitude(const ncsim_state* s, uint64_t index, double* re_im);
 /* count amplitudes at the given indices (amplitude called in a loop). */
@@ -186,7 +198,11 @@ ncsim_status ncsim_sv_profile_read(ncsim_state* s, ncsim_kernel_stat* out, uint3
  * where an allocation or free could synchronize the device, fragment the pool
  * or exceed the budget.  The reduction scratch is a file-scope device array of
  * 1024 block partials (32 KB); registers of up to 34 qubits are accepted and
- * larger ones are rejected with NCSIM_ERR_INVALID.  The first call on a
+ * larger ones are rejected with NCSIM_ERR_INVALID.  `amps` must be device
+ * (or managed) memory of the current device holding all 2^n amplitudes inside
+ * one allocation, and a non-NULL `stream` must belong to the current device:
+ * a host pointer, a shorter buffer or another device's stream is rejected
+ * with NCSIM_ERR_INVALID before anything is launched.  The first call on a
  * device resolves the array's device address (set-up), so make it before any
  * stream capture.  All calls share the array: calls that overlap on the GPU
  * race and must be serialized by the caller. */
@@ -330,6 +346,11 @@ ncsim_status ncsim_batch_random_layers(uint32_t count, uint64_t seed0, uint32_t 
 ncsim_status ncsim_batch_from_circuits(uint32_t count, const ncsim_circuit* const* circuits, const uint64_t* seeds,
                                        ncsim_batch** out);
 ncsim_status ncsim_batch_free(ncsim_batch* b);
+/* Gives back the batch's device and pinned memory, its stream and its graph
+ * (results of earlier runs are dropped); the batch keeps its program, and the
+ * next run sets everything up again on the device current at that time (so a
+ * batch can move between devices).  The caller's current device is kept. */
+ncsim_status ncsim_batch_release(ncsim_batch* b);
 ncsim_status ncsim_batch_info(const ncsim_batch* b, ncsim_batch_stats* st);
 ncsim_status ncsim_batch_trajectory_qubits(const ncsim_batch* b, uint32_t* n);
 ncsim_status ncsim_batch_set_config(ncsim_batch* b, const ncsim_batch_config* cfg);

@@ -58,6 +58,8 @@ _SIGNATURES = {
     "ncsim_last_error": (C.c_char_p, []),
     "ncsim_abi_version": (_i32, []),
     "ncsim_device_info": (_i32, [_P(_i32), _P(_u64), _P(_u64)]),
+    "ncsim_trim_memory": (_i32, []),
+    "ncsim_pool_info": (_i32, [_P(_u64), _P(_u64)]),
     "ncsim_sv_create": (_i32, [_u32, _i32, _P(_vp)]),
     "ncsim_sv_destroy": (_i32, [_vp]),
     "ncsim_sv_clone": (_i32, [_vp, _P(_vp)]),
@@ -67,6 +69,7 @@ _SIGNATURES = {
     "ncsim_sv_set_plus": (_i32, [_vp]),
     "ncsim_sv_set_amplitudes": (_i32, [_vp, _P(_dbl), _u64]),
     "ncsim_sv_get_amplitudes": (_i32, [_vp, _P(_dbl), _u64]),
+    "ncsim_sv_get_amplitudes_range": (_i32, [_vp, _u64, _u64, _P(_dbl)]),
     "ncsim_sv_get_amplitude": (_i32, [_vp, _u64, _P(_dbl)]),
     "ncsim_sv_gather_amplitudes": (_i32, [_vp, _P(_u64), _u64, _P(_dbl)]),
     "ncsim_sv_apply_matrix": (_i32, [_vp, _P(_u32), _u32, _P(_dbl)]),
@@ -122,6 +125,7 @@ _SIGNATURES = {
     "ncsim_batch_random_layers": (_i32, [_u32, _u64, _u32, _u32, _u32, _dbl, _P(_vp)]),
     "ncsim_batch_from_circuits": (_i32, [_u32, _P(_vp), _P(_u64), _P(_vp)]),
     "ncsim_batch_free": (_i32, [_vp]),
+    "ncsim_batch_release": (_i32, [_vp]),
     "ncsim_batch_info": (_i32, [_vp, _vp]),
     "ncsim_batch_trajectory_qubits": (_i32, [_vp, _P(_u32)]),
     "ncsim_batch_set_config": (_i32, [_vp, _vp]),
@@ -454,11 +458,24 @@ class GpuStateVector:
         b = np.ascontiguousarray(np.asarray(amps, dtype=np.complex128)).view(np.float64)
         _check(lib().ncsim_sv_set_amplitudes(self._h, _dp(b), 1 << self.n))
 
+    def set_basis(self, index: int) -> None:
+        """The register becomes the basis state |index> (in place)."""
+        _check(lib().ncsim_sv_set_basis(self._h, index))
+
     def to_vector(self) -> np.ndarray:
         """All amplitudes as complex128 (``to_vector``, vector.rs:542)."""
         b = np.empty(2 << self.n, dtype=np.float64)
         _check(lib().ncsim_sv_get_amplitudes(self._h, _dp(b), 1 << self.n))
         return b.view(np.complex128)
+
+    def to_vector_range(self, first: int, count: int, out: np.ndarray | None = None) -> np.ndarray:
+        """Amplitudes ``first .. first+count-1`` as complex128 (a slice of ``to_vector``)."""
+        if out is None:
+            out = np.empty(count, dtype=np.complex128)
+        if out.dtype != np.complex128 or out.size < count or not out.flags.c_contiguous:
+            raise ValueError("out must be a contiguous complex128 array of at least count elements")
+        _check(lib().ncsim_sv_get_amplitudes_range(self._h, first, count, _dp(out.view(np.float64))))
+        return out[:count]
 
     def amplitude(self, index: int) -> complex:
         o = (_dbl * 2)()
@@ -701,6 +718,11 @@ class TrajectoryBatch:
         if h and _lib is not None:
             _lib.ncsim_batch_free(h)
 
+    def release(self) -> None:
+        """Gives back the batch's device memory, stream and graph; the next run
+        sets them up again on the then-current device."""
+        _check(lib().ncsim_batch_release(self._h))
+
     def info(self) -> dict:
         st = BatchStats()
         _check(lib().ncsim_batch_info(self._h, C.byref(st)))
@@ -899,3 +921,15 @@ def device_info() -> dict:
     sm, fr, tot = _i32(), _u64(), _u64()
     _check(lib().ncsim_device_info(C.byref(sm), C.byref(fr), C.byref(tot)))
     return {"sm_count": sm.value, "free_bytes": fr.value, "total_bytes": tot.value}
+
+
+def trim_memory() -> None:
+    """Gives the memory kept by the library's per-device pools back to the device."""
+    _check(lib().ncsim_trim_memory())
+
+
+def pool_info() -> dict:
+    """Bytes the current device's library pool holds, and bytes of it in use."""
+    r, u = _u64(), _u64()
+    _check(lib().ncsim_pool_info(C.byref(r), C.byref(u)))
+    return {"reserved_bytes": r.value, "used_bytes": u.value}

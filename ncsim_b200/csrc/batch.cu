@@ -658,8 +658,14 @@ struct ncsim_batch {
   double last_ms = 0.0;
 
   ~ncsim_batch() { release(); }
+  // Frees every device and pinned resource on the batch's device and leaves
+  // the object as if it had never run (all pointers null, all capacities 0),
+  // so the next run sets everything up again on the then-current device.  The
+  // calling thread's current device is restored.
   void release() {
     if (device < 0) return;
+    int caller = -1;
+    if (cudaGetDevice(&caller) != cudaSuccess) caller = -1;
     cudaSetDevice(device);
     if (graph) cudaGraphExecDestroy(graph);
     if (stream) cudaStreamSynchronize(stream);
@@ -671,17 +677,32 @@ struct ncsim_batch {
     buf_free(d_slots, slots_cap);
     buf_free(d_scratch, scratch_cap);
     d_prog = nullptr;
+    d_queue = nullptr;
+    d_rec = nullptr;
+    d_z0 = nullptr;
+    d_norm = nullptr;
     d_slots = nullptr;
     d_scratch = nullptr;
+    prog_cap = slots_cap = scratch_cap = 0;
+    slot_ctas = 0;
     cudaFreeHost(h_rec);
     cudaFreeHost(h_z0);
     cudaFreeHost(h_norm);
     cudaFreeHost(h_err);
+    h_rec = nullptr;
+    h_z0 = nullptr;
+    h_norm = nullptr;
+    h_err = nullptr;
     if (ev0) cudaEventDestroy(ev0);
     if (ev1) cudaEventDestroy(ev1);
     if (stream) cudaStreamDestroy(stream);
+    ev0 = ev1 = nullptr;
+    stream = nullptr;
     graph = nullptr;
+    have_results = false;
     device = -1;
+    cudaGetLastError();
+    if (caller >= 0) cudaSetDevice(caller);
   }
   uint32_t count() const { return uint32_t(prog.traj.size()); }
 };
@@ -699,10 +720,7 @@ void ensure_device(ncsim_batch* b) {
   int dev = 0;
   NCSIM_CUDA(cudaGetDevice(&dev));
   if (b->device == dev) return;
-  if (b->device >= 0) {
-    b->release();                   // (on its old device)
-    NCSIM_CUDA(cudaSetDevice(dev));  // back to the caller's device
-  }
+  if (b->device >= 0) b->release();  // on its old device; the caller's device stays current
   b->device = dev;
   NCSIM_CUDA(cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking));
   NCSIM_CUDA(cudaEventCreate(&b->ev0));
@@ -756,7 +774,7 @@ uint32_t grid_for(const ncsim_batch_config& cfg) {
 }
 
 void ensure_slots(ncsim_batch* b, uint32_t ctas) {
-  if (b->slot_ctas >= ctas) return;
+  if (b->slot_ctas >= ctas && b->d_slots && b->d_scratch) return;
   NCSIM_CUDA(cudaStreamSynchronize(b->stream));
   if (b->graph) {  // the captured launch holds the old slot pointers
     NCSIM_CUDA(cudaGraphExecDestroy(b->graph));
@@ -773,8 +791,16 @@ void ensure_slots(ncsim_batch* b, uint32_t ctas) {
   b->slot_ctas = ctas;
 }
 
+// every device buffer a launch reads or writes must exist (a batch released
+// from its device is set up again by ensure_device/ensure_slots before this)
+void check_launch_buffers(const ncsim_batch* b) {
+  if (!b->d_prog || !b->d_queue || !b->d_rec || !b->d_z0 || !b->d_norm || !b->d_slots || !b->d_scratch || !b->stream)
+    throw Error(NCSIM_ERR_DEVICE, "batch launch without its device buffers (released and not set up again)");
+}
+
 // one launch of the kernel over `count` jobs of the order array at order_off
 void enqueue_kernel(ncsim_batch* b, const ncsim_batch_config& cfg, size_t order_off, uint32_t count) {
+  check_launch_buffers(b);
   KParams k{};
   k.traj = dev_ptr<DevTraj>(b, b->off_traj);
   k.pass = dev_ptr<DevPass>(b, b->off_pass);
@@ -974,6 +1000,14 @@ ncsim_status ncsim_batch_from_circuits(uint32_t count, const ncsim_circuit* cons
 
 ncsim_status ncsim_batch_free(ncsim_batch* b) {
   return guarded([&] { delete b; });
+}
+
+ncsim_status ncsim_batch_release(ncsim_batch* b) {
+  return guarded([&] {
+    if (!b) throw Error(NCSIM_ERR_INVALID, "null batch");
+    std::lock_guard<std::mutex> lk(b->mu);
+    b->release();
+  });
 }
 
 ncsim_status ncsim_batch_info(const ncsim_batch* b, ncsim_batch_stats* st) {

@@ -28,28 +28,44 @@ int sm_count() {
   return count;
 }
 
-// The library's temporaries (readouts, the sparse form's sort buffers) come from
-// the device's default stream-ordered pool.  Its default release threshold of 0
-// hands freed memory back at every synchronisation, and the next allocation
-// maps it again, which stalled runs by 100 ms and more at times; the pool keeps
-// what it has instead (a per-process allocator setting, set once per device).
-void keep_pool_memory() {
-  static std::mutex mu;
-  static bool done[64] = {};
+// The library's temporaries (readouts, staging buffers, the sparse form's
+// sort buffers) come from a stream-ordered pool the library owns, one per
+// device, created on first use.  A pool with the default release threshold of
+// 0 hands freed memory back at every synchronisation, and the next allocation
+// maps it again, which stalled runs by 100 ms and more at times; this pool
+// keeps what it has (threshold UINT64_MAX) until ncsim_trim_memory or process
+// exit.  The device's default pool, which other code in the process may use,
+// is left as it is.
+namespace {
+constexpr int POOL_DEVICES = 64;
+std::mutex g_pool_mu;
+cudaMemPool_t g_pool[POOL_DEVICES] = {};
+}  // namespace
+
+cudaMemPool_t lib_pool() {
   int dev = 0;
-  if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) {
-    cudaGetLastError();
-    return;
-  }
-  std::lock_guard<std::mutex> lk(mu);
-  if (done[dev]) return;
-  cudaMemPool_t pool;
-  if (cudaDeviceGetDefaultMemPool(&pool, dev) == cudaSuccess) {
+  NCSIM_CUDA(cudaGetDevice(&dev));
+  if (dev < 0 || dev >= POOL_DEVICES) throw Error(NCSIM_ERR_DEVICE, "device index out of range");
+  std::lock_guard<std::mutex> lk(g_pool_mu);
+  if (!g_pool[dev]) {
+    cudaMemPoolProps props{};
+    props.allocType = cudaMemAllocationTypePinned;
+    props.handleTypes = cudaMemHandleTypeNone;
+    props.location.type = cudaMemLocationTypeDevice;
+    props.location.id = dev;
+    cudaMemPool_t p = nullptr;
+    NCSIM_CUDA(cudaMemPoolCreate(&p, &props));
     uint64_t keep = UINT64_MAX;
-    cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep);
+    NCSIM_CUDA(cudaMemPoolSetAttribute(p, cudaMemPoolAttrReleaseThreshold, &keep));
+    g_pool[dev] = p;
   }
-  cudaGetLastError();
-  done[dev] = true;
+  return g_pool[dev];
+}
+
+void trim_lib_pools() {
+  std::lock_guard<std::mutex> lk(g_pool_mu);
+  for (int d = 0; d < POOL_DEVICES; ++d)
+    if (g_pool[d]) NCSIM_CUDA(cudaMemPoolTrimTo(g_pool[d], 0));
 }
 
 namespace {
@@ -131,7 +147,6 @@ ncsim_state* state_new(uint32_t n, int32_t precision) {
   s->len = uint64_t(1) << n;
   try {
     NCSIM_CUDA(cudaGetDevice(&s->device));
-    keep_pool_memory();
     NCSIM_CUDA(cudaStreamCreateWithFlags(&s->stream, cudaStreamNonBlocking));
     NCSIM_CUDA(cudaMalloc(&s->amp, s->bytes()));
     NCSIM_CUDA(cudaMalloc(&s->partials, sizeof(double) * MAX_REDUCE_BLOCKS * PARTIAL_SLOTS));
@@ -212,7 +227,7 @@ void state_set_amplitudes(ncsim_state* s, const double* amps, uint64_t len) {
   }
   const uint64_t chunk = std::min<uint64_t>(len, uint64_t(1) << 24);
   double2* stage = nullptr;
-  NCSIM_CUDA(cudaMallocAsync(&stage, chunk * sizeof(double2), s->stream));
+  NCSIM_CUDA(pool_alloc(&stage, chunk * sizeof(double2), s->stream));
   for (uint64_t off = 0; off < len; off += chunk) {
     uint64_t c = std::min(chunk, len - off);
     NCSIM_CUDA(cudaMemcpyAsync(stage, amps + 2 * off, c * sizeof(double2), cudaMemcpyHostToDevice, s->stream));
@@ -222,24 +237,32 @@ void state_set_amplitudes(ncsim_state* s, const double* amps, uint64_t len) {
   NCSIM_CUDA(cudaStreamSynchronize(s->stream));
 }
 
-void state_get_amplitudes(const ncsim_state* s, double* amps, uint64_t len) {
-  if (len != s->len) throw Error(NCSIM_ERR_INVALID, "amplitude buffer length differs from 2^n");
+// amplitudes [first, first + count) as complex128 into host memory
+static void state_get_range(const ncsim_state* s, uint64_t first, uint64_t count, double* amps) {
+  if (first > s->len || count > s->len - first) throw Error(NCSIM_ERR_INVALID, "amplitude range outside the register");
+  if (count == 0) return;
   need(amps, "amplitudes");
   if (s->precision == NCSIM_C128) {
-    NCSIM_CUDA(cudaMemcpyAsync(amps, s->amp, s->bytes(), cudaMemcpyDeviceToHost, s->stream));
+    NCSIM_CUDA(cudaMemcpyAsync(amps, static_cast<const double2*>(s->amp) + first, count * sizeof(double2),
+                               cudaMemcpyDeviceToHost, s->stream));
     NCSIM_CUDA(cudaStreamSynchronize(s->stream));
     return;
   }
-  const uint64_t chunk = std::min<uint64_t>(len, uint64_t(1) << 24);
+  const uint64_t chunk = std::min<uint64_t>(count, uint64_t(1) << 24);
   double2* stage = nullptr;
-  NCSIM_CUDA(cudaMallocAsync(&stage, chunk * sizeof(double2), s->stream));
-  for (uint64_t off = 0; off < len; off += chunk) {
-    uint64_t c = std::min(chunk, len - off);
-    launch_convert_out(s, stage, off, c);
+  NCSIM_CUDA(pool_alloc(&stage, chunk * sizeof(double2), s->stream));
+  for (uint64_t off = 0; off < count; off += chunk) {
+    uint64_t c = std::min(chunk, count - off);
+    launch_convert_out(s, stage, first + off, c);
     NCSIM_CUDA(cudaMemcpyAsync(amps + 2 * off, stage, c * sizeof(double2), cudaMemcpyDeviceToHost, s->stream));
   }
   NCSIM_CUDA(cudaFreeAsync(stage, s->stream));
   NCSIM_CUDA(cudaStreamSynchronize(s->stream));
+}
+
+void state_get_amplitudes(const ncsim_state* s, double* amps, uint64_t len) {
+  if (len != s->len) throw Error(NCSIM_ERR_INVALID, "amplitude buffer length differs from 2^n");
+  state_get_range(s, 0, len, amps);
 }
 
 void state_gather(const ncsim_state* s, const uint64_t* idx, uint64_t count, double* out) {
@@ -248,8 +271,8 @@ void state_gather(const ncsim_state* s, const uint64_t* idx, uint64_t count, dou
   need(out, "output");
   uint64_t* d_idx = nullptr;
   double2* d_out = nullptr;
-  NCSIM_CUDA(cudaMallocAsync(&d_idx, count * sizeof(uint64_t), s->stream));
-  NCSIM_CUDA(cudaMallocAsync(&d_out, count * sizeof(double2), s->stream));
+  NCSIM_CUDA(pool_alloc(&d_idx, count * sizeof(uint64_t), s->stream));
+  NCSIM_CUDA(pool_alloc(&d_out, count * sizeof(double2), s->stream));
   NCSIM_CUDA(cudaMemcpyAsync(d_idx, idx, count * sizeof(uint64_t), cudaMemcpyHostToDevice, s->stream));
   launch_gather(s, d_idx, d_out, count);
   NCSIM_CUDA(cudaMemcpyAsync(out, d_out, count * sizeof(double2), cudaMemcpyDeviceToHost, s->stream));
@@ -266,7 +289,7 @@ void state_sample(const ncsim_state* s, const double* uniforms, uint64_t shots, 
   const uint64_t nblocks = s->len / block;
   std::vector<double> w(nblocks);
   double* d_w = nullptr;
-  NCSIM_CUDA(cudaMallocAsync(&d_w, nblocks * sizeof(double), s->stream));
+  NCSIM_CUDA(pool_alloc(&d_w, nblocks * sizeof(double), s->stream));
   launch_block_weights(s, d_w, nblocks, block);
   NCSIM_CUDA(cudaMemcpyAsync(w.data(), d_w, nblocks * sizeof(double), cudaMemcpyDeviceToHost, s->stream));
   NCSIM_CUDA(cudaFreeAsync(d_w, s->stream));
@@ -293,10 +316,10 @@ void state_sample(const ncsim_state* s, const double* uniforms, uint64_t shots, 
   }
   double *d_u = nullptr, *d_acc = nullptr;
   uint64_t *d_blk = nullptr, *d_out = nullptr;
-  NCSIM_CUDA(cudaMallocAsync(&d_u, shots * sizeof(double), s->stream));
-  NCSIM_CUDA(cudaMallocAsync(&d_acc, shots * sizeof(double), s->stream));
-  NCSIM_CUDA(cudaMallocAsync(&d_blk, shots * sizeof(uint64_t), s->stream));
-  NCSIM_CUDA(cudaMallocAsync(&d_out, shots * sizeof(uint64_t), s->stream));
+  NCSIM_CUDA(pool_alloc(&d_u, shots * sizeof(double), s->stream));
+  NCSIM_CUDA(pool_alloc(&d_acc, shots * sizeof(double), s->stream));
+  NCSIM_CUDA(pool_alloc(&d_blk, shots * sizeof(uint64_t), s->stream));
+  NCSIM_CUDA(pool_alloc(&d_out, shots * sizeof(uint64_t), s->stream));
   NCSIM_CUDA(cudaMemcpyAsync(d_u, u.data(), shots * sizeof(double), cudaMemcpyHostToDevice, s->stream));
   NCSIM_CUDA(cudaMemcpyAsync(d_acc, acc.data(), shots * sizeof(double), cudaMemcpyHostToDevice, s->stream));
   NCSIM_CUDA(cudaMemcpyAsync(d_blk, blk.data(), shots * sizeof(uint64_t), cudaMemcpyHostToDevice, s->stream));
@@ -331,6 +354,21 @@ ncsim_status ncsim_device_info(int32_t* sm, uint64_t* free_b, uint64_t* total_b)
     if (sm) *sm = v;
     if (free_b) *free_b = f;
     if (total_b) *total_b = t;
+  });
+}
+
+ncsim_status ncsim_trim_memory(void) {
+  return guarded([&] { trim_lib_pools(); });
+}
+
+ncsim_status ncsim_pool_info(uint64_t* reserved_bytes, uint64_t* used_bytes) {
+  return guarded([&] {
+    cudaMemPool_t p = lib_pool();
+    uint64_t r = 0, u = 0;
+    NCSIM_CUDA(cudaMemPoolGetAttribute(p, cudaMemPoolAttrReservedMemCurrent, &r));
+    NCSIM_CUDA(cudaMemPoolGetAttribute(p, cudaMemPoolAttrUsedMemCurrent, &u));
+    if (reserved_bytes) *reserved_bytes = r;
+    if (used_bytes) *used_bytes = u;
   });
 }
 
@@ -418,6 +456,14 @@ ncsim_status ncsim_sv_get_amplitudes(const ncsim_state* s, double* amps, uint64_
     need(s, "state");
     std::lock_guard<std::recursive_mutex> lk(s->mu);
     state_get_amplitudes(s, amps, len);
+  });
+}
+
+ncsim_status ncsim_sv_get_amplitudes_range(const ncsim_state* s, uint64_t first, uint64_t count, double* amps) {
+  return guarded([&] {
+    need(s, "state");
+    std::lock_guard<std::recursive_mutex> lk(s->mu);
+    state_get_range(s, first, count, amps);
   });
 }
 
@@ -689,7 +735,7 @@ ncsim_status ncsim_sv_compare(const ncsim_state* a, const ncsim_state* b, double
     else std::lock(la, lb);
     if (a != b) NCSIM_CUDA(cudaStreamSynchronize(b->stream));
     double* d_max = nullptr;
-    NCSIM_CUDA(cudaMallocAsync(&d_max, sizeof(double) * MAX_REDUCE_BLOCKS, a->stream));
+    NCSIM_CUDA(pool_alloc(&d_max, sizeof(double) * MAX_REDUCE_BLOCKS, a->stream));
     int g = launch_compare_partials(a, b, d_max);
     std::vector<double> mx(g);
     NCSIM_CUDA(cudaMemcpyAsync(mx.data(), d_max, sizeof(double) * g, cudaMemcpyDeviceToHost, a->stream));

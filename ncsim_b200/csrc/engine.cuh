@@ -57,8 +57,14 @@ inline void cuda_check(cudaError_t e, const char* what) {
 // device facts
 // ---------------------------------------------------------------------------
 int sm_count();
-// the current device's default stream-ordered pool keeps freed memory (once per device)
-void keep_pool_memory();
+// the library's own stream-ordered pool on the current device (created on
+// first use; keeps freed memory until trim_lib_pools)
+cudaMemPool_t lib_pool();
+void trim_lib_pools();
+template <class T>
+inline cudaError_t pool_alloc(T** p, size_t bytes, cudaStream_t st) {
+  return cudaMallocFromPoolAsync(reinterpret_cast<void**>(p), bytes, lib_pool(), st);
+}
 
 // ---------------------------------------------------------------------------
 // the state handle

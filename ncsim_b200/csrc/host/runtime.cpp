@@ -318,9 +318,11 @@ ncsim_status ncsim_sv_measure(ncsim_state* s, uint64_t x, uint64_t z, uint32_t p
 namespace {
 
 // Runs of at least MIN_GRAPH_GATES consecutive gates (annotations between them
-// allowed) are captured once per state as CUDA graphs and replayed by later
-// runs of the same circuit on the same state: one graph launch instead of a
-// host lowering step and a kernel launch per gate.  Measurements, resets and
+// allowed) are captured as CUDA graphs on the second run of a circuit on a
+// state and replayed by every later run: one graph launch instead of a host
+// lowering step and a kernel launch per gate.  A circuit run only once (a
+// noisy trajectory drawn for one run) launches its kernels directly and pays
+// no capture.  Measurements, resets and
 // noise stay outside the graphs (their draws and decisions are made on the
 // host).  Not used while the launch profiler records per-launch events, nor
 // when the environment sets NCSIM_NO_GATE_GRAPHS (kernel-by-kernel launches).
@@ -331,6 +333,7 @@ struct GateGraphs {
   int device = -1;
   std::vector<std::pair<size_t, size_t>> runs;  // [first op, end op) of each run
   std::vector<cudaGraphExec_t> exec;            // null until captured
+  std::vector<char> seen;                       // the run has been launched directly once
   std::vector<char> failed;                     // capture did not succeed: launch directly
   ~GateGraphs() {
     for (auto e : exec)
@@ -363,6 +366,7 @@ std::shared_ptr<GateGraphs> gate_graphs_for(const ncsim_circuit* c, const ncsim_
     i = j;
   }
   g->exec.assign(g->runs.size(), nullptr);
+  g->seen.assign(g->runs.size(), 0);
   g->failed.assign(g->runs.size(), 0);
   c->gate_graphs = g;
   return g;
@@ -371,7 +375,7 @@ std::shared_ptr<GateGraphs> gate_graphs_for(const ncsim_circuit* c, const ncsim_
 // Launches the gates of ops[first, end) on the state's stream, as a graph when it can.
 void run_gates(ncsim_state* s, const ncsim_circuit* c, GateGraphs& g, size_t k) {
   const auto [first, end] = g.runs[k];
-  if (!g.exec[k] && !g.failed[k]) {
+  if (!g.exec[k] && !g.failed[k] && g.seen[k]) {
     cudaGraph_t graph = nullptr;
     bool ok = cudaStreamBeginCapture(s->stream, cudaStreamCaptureModeThreadLocal) == cudaSuccess;
     if (ok) {
@@ -392,6 +396,7 @@ void run_gates(ncsim_state* s, const ncsim_circuit* c, GateGraphs& g, size_t k) 
       g.failed[k] = 1;
     }
   }
+  g.seen[k] = 1;
   if (g.exec[k]) {
     NCSIM_CUDA(cudaGraphLaunch(g.exec[k], s->stream));
   } else {

@@ -7,6 +7,8 @@
 // arithmetic is 64-bit (registers up to 34 qubits).
 #include "engine.cuh"
 
+#include <cuda.h>
+
 #include <algorithm>
 #include <cmath>
 #include <type_traits>
@@ -1443,6 +1445,61 @@ double* noalloc_scratch(int dev) {
   return g_noalloc_ptr[dev];
 }
 
+// cuMemGetAddressRange through the runtime's driver entry point (the library
+// links no driver library); null when the driver does not provide it
+using MemRangeFn = CUresult (*)(CUdeviceptr*, size_t*, CUdeviceptr);
+MemRangeFn mem_range_fn() {
+  static MemRangeFn fn = [] {
+    void* f = nullptr;
+    cudaDriverEntryPointQueryResult q{};
+    if (cudaGetDriverEntryPoint("cuMemGetAddressRange", &f, cudaEnableDefault, &q) != cudaSuccess ||
+        q != cudaDriverEntryPointSuccess) {
+      cudaGetLastError();
+      f = nullptr;
+    }
+    return reinterpret_cast<MemRangeFn>(f);
+  }();
+  return fn;
+}
+
+// Host-side checks of a caller's buffer and stream, none of which allocates:
+// the buffer is device (or managed) memory of the current device and holds
+// `bytes` bytes from `p` inside one allocation, and a given stream belongs to
+// the current device.  A mistake is reported before anything is launched.
+void check_caller_buffer(const void* p, size_t bytes, int dev, cudaStream_t st) {
+  cudaPointerAttributes at{};
+  if (cudaPointerGetAttributes(&at, p) != cudaSuccess) {
+    cudaGetLastError();
+    throw Error(NCSIM_ERR_INVALID, "amplitudes: not a pointer the CUDA runtime knows");
+  }
+  if (at.type != cudaMemoryTypeDevice && at.type != cudaMemoryTypeManaged)
+    throw Error(NCSIM_ERR_INVALID, "amplitudes must be device or managed memory (host memory was given)");
+  if (at.type == cudaMemoryTypeDevice && at.device != dev)
+    throw Error(NCSIM_ERR_INVALID, "amplitudes live on device " + std::to_string(at.device) +
+                                       ", but device " + std::to_string(dev) + " is current");
+  if (MemRangeFn fn = mem_range_fn()) {
+    CUdeviceptr base = 0;
+    size_t size = 0;
+    if (fn(&base, &size, reinterpret_cast<CUdeviceptr>(p)) != CUDA_SUCCESS)
+      throw Error(NCSIM_ERR_INVALID, "amplitudes: no device allocation contains the pointer");
+    const uint64_t off = uint64_t(reinterpret_cast<uintptr_t>(p)) - uint64_t(base);
+    if (off > size || size - off < bytes)
+      throw Error(NCSIM_ERR_INVALID, "amplitude buffer too short: " + std::to_string(bytes) + " bytes needed, " +
+                                         std::to_string(size - std::min<uint64_t>(off, size)) +
+                                         " left in its allocation");
+  }
+  if (st) {
+    int sdev = -1;
+    if (cudaStreamGetDevice(st, &sdev) != cudaSuccess) {
+      cudaGetLastError();
+      throw Error(NCSIM_ERR_INVALID, "stream: not a valid CUDA stream");
+    }
+    if (sdev != dev)
+      throw Error(NCSIM_ERR_INVALID, "stream belongs to device " + std::to_string(sdev) + ", but device " +
+                                         std::to_string(dev) + " is current");
+  }
+}
+
 }  // namespace
 
 }  // namespace ncsim
@@ -1462,8 +1519,9 @@ extern "C" ncsim_status ncsim_measure_stats_noalloc(const void* amps, uint32_t n
     if ((x | z) & ~(len - 1)) throw Error(NCSIM_ERR_INVALID, "Pauli acts outside the register");
     int dev = 0;
     NCSIM_CUDA(cudaGetDevice(&dev));
-    double* scratch = noalloc_scratch(dev);
     cudaStream_t st = static_cast<cudaStream_t>(stream);
+    check_caller_buffer(amps, size_t(len) * (precision == NCSIM_C128 ? 16 : 8), dev, st);
+    double* scratch = noalloc_scratch(dev);
     const int ph = int(phase & 3);
     int g;
     auto launch = [&](auto tag) {

@@ -448,7 +448,7 @@ struct PairLock {
 template <class T>
 T* dalloc(size_t count, cudaStream_t st) {
   void* p = nullptr;
-  NCSIM_CUDA(cudaMallocAsync(&p, std::max<size_t>(1, count) * sizeof(T), st));
+  NCSIM_CUDA(pool_alloc(&p, std::max<size_t>(1, count) * sizeof(T), st));
   return static_cast<T*>(p);
 }
 void dfree(void* p, cudaStream_t st) {
@@ -976,7 +976,6 @@ ncsim_sparse* sp_new(uint32_t n) {
   auto s = std::make_unique<ncsim_sparse>();
   s->n = n;
   NCSIM_CUDA(cudaGetDevice(&s->device));
-  keep_pool_memory();
   NCSIM_CUDA(cudaStreamCreateWithFlags(&s->stream, cudaStreamNonBlocking));
   NCSIM_CUDA(cudaMalloc(&s->partials, SP_BLOCKS * 2 * sizeof(double)));
   NCSIM_CUDA(cudaMallocHost(&s->host_partials, SP_BLOCKS * 2 * sizeof(double)));

@@ -122,6 +122,30 @@ int oracle_sv_set_amplitudes(void* h, const double* a, uint64_t len) {
     for (uint64_t i = 0; i < len; ++i) s->amp[i] = C64(a[2 * i], a[2 * i + 1]);
   });
 }
+// amplitudes [first, first + count) from interleaved host doubles
+int oracle_sv_set_range(void* h, const double* a, uint64_t first, uint64_t count) {
+  return guard([&] {
+    auto* s = (StateVector*)h;
+    if (first > s->amp.size() || count > s->amp.size() - first) throw SimError(ErrKind::Invalid, "range");
+#pragma omp parallel for schedule(static)
+    for (int64_t i = 0; i < int64_t(count); ++i) s->amp[first + i] = C64(a[2 * i], a[2 * i + 1]);
+  });
+}
+// max |amp[first + i] - a[i]| over the range
+int oracle_sv_max_abs_diff(void* h, const double* a, uint64_t first, uint64_t count, double* out) {
+  return guard([&] {
+    auto* s = (StateVector*)h;
+    if (first > s->amp.size() || count > s->amp.size() - first) throw SimError(ErrKind::Invalid, "range");
+    double m = 0.0;
+#pragma omp parallel for schedule(static) reduction(max : m)
+    for (int64_t i = 0; i < int64_t(count); ++i) {
+      const C64 v = s->amp[first + i];
+      m = std::max(m, std::hypot(v.re - a[2 * i], v.im - a[2 * i + 1]));
+    }
+    *out = m;
+  });
+}
+
 int oracle_sv_get_amplitudes(void* h, double* a, uint64_t len) {
   return guard([&] {
     auto* s = (StateVector*)h;

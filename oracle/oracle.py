@@ -62,6 +62,8 @@ def lib():
             "oracle_sv_free": (None, [vp]),
             "oracle_sv_set_amplitudes": (i32, [vp, P(dbl), u64]),
             "oracle_sv_get_amplitudes": (i32, [vp, P(dbl), u64]),
+            "oracle_sv_set_range": (i32, [vp, P(dbl), u64, u64]),
+            "oracle_sv_max_abs_diff": (i32, [vp, P(dbl), u64, u64, P(dbl)]),
             "oracle_sv_apply_gate_text": (i32, [vp, C.c_char_p]),
             "oracle_sv_apply_matrix": (i32, [vp, P(u32), u32, P(dbl)]),
             "oracle_sv_apply_pauli": (i32, [vp, C.c_char_p]),
@@ -220,6 +222,18 @@ class StateVector:
         b = np.zeros(2 << self.n, dtype=np.float64)
         _check(lib().oracle_sv_get_amplitudes(self.h, _dp(b), 1 << self.n))
         return b.view(np.complex128)
+
+    def set_range(self, first: int, a: np.ndarray) -> None:
+        """Amplitudes first .. first+len(a)-1 from complex128 values."""
+        b = np.ascontiguousarray(np.asarray(a, dtype=np.complex128)).view(np.float64)
+        _check(lib().oracle_sv_set_range(self.h, _dp(b), first, b.size // 2))
+
+    def max_abs_diff(self, first: int, a: np.ndarray) -> float:
+        """max |amp[first + i] - a[i]| over the slice."""
+        b = np.ascontiguousarray(np.asarray(a, dtype=np.complex128)).view(np.float64)
+        out = C.c_double()
+        _check(lib().oracle_sv_max_abs_diff(self.h, _dp(b), first, b.size // 2, C.byref(out)))
+        return out.value
 
     def apply_gate_text(self, text: str) -> None:
         _check(lib().oracle_sv_apply_gate_text(self.h, text.encode()))

@@ -106,3 +106,20 @@ def test_results_before_run_refused(nb):
         b.results()
     with pytest.raises(nb.SimError):
         b.set_config(ctas_per_sm=2, buffers=2)
+
+
+def test_release_and_set_up_again(nb):
+    """A batch gives its device resources back (the path a batch takes when it
+    moves to another device) and runs again with the same results: every
+    buffer, capacity and slot count is set up anew, none is left dangling."""
+    b = nb.TrajectoryBatch.random_layers(48, seed0=5, n_lo=13, n_span=3, depth=5, p=0.01)
+    b.run()
+    r1 = b.results()
+    b.release()
+    with pytest.raises(nb.SimError):
+        b.results()  # the results went with the released pinned buffers
+    b.release()  # releasing twice is harmless
+    b.run()
+    r2 = b.results()
+    for x, y in zip(r1, r2):
+        assert np.array_equal(x, y)

@@ -253,7 +253,7 @@ def test_random_layers_with_measurements(nb, oracle):
 
 
 def test_gate_runs_replayed_as_graphs(nb, oracle):
-    """Runs of gates are captured as CUDA graphs on the first run of a circuit on
+    """Runs of gates are captured as CUDA graphs on the second run of a circuit on
     a state and replayed by later runs; measurements in between stay direct.  The
     register after each run, and the records, match the oracle; a run with the
     launch profiler on (direct launches) gives the same register."""
