@@ -7,17 +7,19 @@
  * functions and implements `GpuStateVector: QuantumState<C64>`; the core crate
  * keeps `#![forbid(unsafe_code)]` (src/lib.rs:36).
  *
- * Two layers are exported:
+ * Three layers are exported:
  *   1. state operations with plain-old-data arguments (pointers, sizes, bit
  *      masks, row-major complex128 arrays): what the Rust crate calls after it
  *      lowers a `Gate` through the reference's own views
  *      (`Gate::monomial/matrix`, src/gate.rs:519-747);
  *   2. a C++ host mirror of the trait's provided methods (run, measure,
- *      sample with a seeded StdRng, text circuits, workloads) for hosts that
- *      have no Rust toolchain, and the two GPU-only forms (fused precision
- *      form, batched trajectories);
+ *      sample with a seeded StdRng, text circuits) for hosts that have no
+ *      Rust toolchain, and the two GPU-only forms (fused precision form,
+ *      batched trajectories);
  *   3. the sparse form: SparseVector<C64> (src/state/sparse.rs) with its
  *      entries in device memory.
+ * The seeded synthetic workloads of the benchmark and the tests are not part
+ * of this interface: they live in libncsim_workloads.so (ncsim_workloads.h).
  *
  * Conventions (src/state/vector.rs:14, src/pauli/ops.rs:5):
  *   - qubit q is bit q of a basis index; a k-qubit gate matrix is row-major,
@@ -68,6 +70,19 @@ typedef struct ncsim_gate ncsim_gate;
 
 /* Thread-local message of the last failed call on this thread. */
 const char* ncsim_last_error(void);
+/* The fields of the last error on this thread, for the SimError variants
+ * that carry them (src/error.rs:17-33): QubitOutOfRange {qubit, num_qubits},
+ * DuplicateQubit(qubit), Arity {gate, expected, got}.  Fields a variant does
+ * not carry are zero (gate: empty). */
+typedef struct ncsim_error_info {
+  ncsim_status code;
+  uint64_t qubit;
+  uint64_t num_qubits;
+  uint64_t expected;
+  uint64_t got;
+  char gate[64]; /* the gate's text name, zero-terminated */
+} ncsim_error_info;
+ncsim_status ncsim_last_error_info(ncsim_error_info* out);
 /* ABI version (major * 10000 + minor * 100 + patch). */
 int32_t ncsim_abi_version(void);
 /* Streaming multiprocessors, free and total device memory of the current device. */
@@ -114,14 +129,17 @@ ncsim_status ncsim_sv_get_amplitude(const ncsim_state* s, uint64_t index, double
 ncsim_status ncsim_sv_gather_amplitudes(const ncsim_state* s, const uint64_t* indices, uint64_t count, double* out);
 
 /* Dense 2^k x 2^k complex128 matrix on qubits (StateVector::apply_matrix,
- * vector.rs:67-93).  k <= 6.  Exact-zero entries contribute nothing, as in
- * the reference's row-sparse product. */
+ * vector.rs:67-93).  k <= 13 (gates on 6..13 qubits run as a complex GEMM
+ * over gathered chunks of fibers, with the matrix in device memory for the
+ * call).  Exact-zero entries contribute nothing (a zero product), as in the
+ * reference's row-sparse product. */
 ncsim_status ncsim_sv_apply_matrix(ncsim_state* s, const uint32_t* qubits, uint32_t k, const double* matrix);
 /* Monomial gate given by its basis images (StateVector::apply_monomial,
  * vector.rs:96-139): U|x> = phase[x] |image[x]> over the local index x.
  * image must be a permutation of 0..2^k; phase is complex128.  Diagonal
  * tables (image[x] == x) touch only amplitudes whose phase is not exactly 1.
- * k <= 10. */
+ * k <= 24 (tables on more than 10 qubits run through gathered chunks of
+ * fibers, with the table in device memory for the call). */
 ncsim_status ncsim_sv_apply_monomial(ncsim_state* s, const uint32_t* qubits, uint32_t k, const uint64_t* image,
                                      const double* phase);
 /* Diagonal(PhasePoly) evaluated from each basis index (gate.rs:557 with
@@ -231,25 +249,10 @@ ncsim_status ncsim_circuit_info(const ncsim_circuit* c, uint32_t* num_qubits, ui
  * without the terminating zero, written only when cap > len. */
 ncsim_status ncsim_circuit_to_text(const ncsim_circuit* c, char* buf, size_t cap, size_t* len);
 
-/* Seeded synthetic workloads (StdRng::seed_from_u64(seed) draws every choice).
- * Random layer family: per layer one of {H, S, T, SQRT_X, RZ(theta)} on every
- * qubit, then CZ on a random perfect matching (optionally followed by
- * DEPOLARIZE2(noise_p)); Z measurements of qubits [m_lo, m_hi) at the end. */
-ncsim_status ncsim_workload_random_circuit(uint32_t n, uint32_t depth, uint64_t seed, double noise_p, uint32_t m_lo,
-                                           uint32_t m_hi, ncsim_circuit** out);
-/* The same family drawn from the caller's generator, which keeps its state
- * (a noisy trajectory draws its circuit and then its noise and measurement
- * outcomes from one StdRng). */
-ncsim_status ncsim_workload_random_circuit_rng(ncsim_rng* rng, uint32_t n, uint32_t depth, double noise_p,
-                                               uint32_t m_lo, uint32_t m_hi, ncsim_circuit** out);
-/* Permutation/diagonal family: H on min(16, n) qubits, then `gates` gates
- * from {CX, CCX, CCZ, DIAG over the register, MONOMIAL on 8 qubits}. */
-ncsim_status ncsim_workload_reversible_circuit(uint32_t n, uint32_t gates, uint64_t seed, ncsim_circuit** out);
-
 /* A gate from one text token ("H", "RZ(0.5)", "PHASE(3,4)", "DIAG(...)",
  * "MONOMIAL(...)") and its arity. */
 ncsim_status ncsim_gate_parse(const char* token, uint32_t arity_hint, ncsim_gate** out, uint32_t* arity);
-/* Gate::Unitary (gate.rs:427-428): a dense complex128 matrix on k qubits. */
+/* Gate::Unitary (gate.rs:427-428): a dense complex128 matrix on k <= 13 qubits. */
 ncsim_status ncsim_gate_unitary(uint32_t k, const double* matrix, ncsim_gate** out);
 /* Gate::Pauli (gate.rs:417-418): i^phase X^x Z^z on k local qubits. */
 ncsim_status ncsim_gate_pauli(uint32_t k, uint64_t x, uint64_t z, uint32_t phase, ncsim_gate** out);
@@ -336,12 +339,6 @@ typedef struct ncsim_batch_config {
   uint32_t buffers;     /* 2: tile prefetch, FP64 sums in shared memory; 1: no prefetch */
   uint32_t order;       /* NCSIM_BATCH_ORDER_* */
 } ncsim_batch_config;
-/* Trajectory t: StdRng::seed_from_u64(seed0 + t), n = n_lo + gen_range(0..n_span),
- * the random-layer circuit of `depth` layers with DEPOLARIZE2(p) after every
- * CZ and M on every qubit (ncsim_workload_random_circuit_rng), run with the
- * same generator. */
-ncsim_status ncsim_batch_random_layers(uint32_t count, uint64_t seed0, uint32_t n_lo, uint32_t n_span, uint32_t depth,
-                                       double p, ncsim_batch** out);
 /* Trajectory t: circuits[t] run with StdRng::seed_from_u64(seeds[t]). */
 ncsim_status ncsim_batch_from_circuits(uint32_t count, const ncsim_circuit* const* circuits, const uint64_t* seeds,
                                        ncsim_batch** out);

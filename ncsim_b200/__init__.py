@@ -41,21 +41,33 @@ STATUS_NAMES = {
 
 
 class SimError(RuntimeError):
-    """An error status of the engine; ``kind`` names the SimError variant."""
+    """An error status of the engine; ``kind`` names the SimError variant and
+    ``fields`` holds the variant's fields where it has some (src/error.rs:17-33):
+    ``{"qubit", "num_qubits"}`` for QubitOutOfRange, ``{"qubit"}`` for
+    DuplicateQubit, ``{"gate", "expected", "got"}`` for Arity."""
 
-    def __init__(self, status: int, message: str):
+    def __init__(self, status: int, message: str, fields: dict | None = None):
         self.status = status
         self.kind = STATUS_NAMES.get(status, f"status{status}")
+        self.fields = fields or {}
         super().__init__(f"{self.kind}: {message}")
 
 
+class ErrorInfo(C.Structure):
+    _fields_ = [("code", C.c_int32), ("qubit", C.c_uint64), ("num_qubits", C.c_uint64), ("expected", C.c_uint64),
+                ("got", C.c_uint64), ("gate", C.c_char * 64)]
+
+
 _lib = None
+_wlib = None
+WORKLOADS_PATH = os.path.join(_HERE, "libncsim_workloads.so")
 
 _P = C.POINTER
 _u32, _u64, _i32, _dbl, _vp = C.c_uint32, C.c_uint64, C.c_int32, C.c_double, C.c_void_p
 
 _SIGNATURES = {
     "ncsim_last_error": (C.c_char_p, []),
+    "ncsim_last_error_info": (_i32, [_vp]),
     "ncsim_abi_version": (_i32, []),
     "ncsim_device_info": (_i32, [_P(_i32), _P(_u64), _P(_u64)]),
     "ncsim_trim_memory": (_i32, []),
@@ -98,9 +110,6 @@ _SIGNATURES = {
     "ncsim_circuit_free": (_i32, [_vp]),
     "ncsim_circuit_info": (_i32, [_vp, _P(_u32), _P(_u64), _P(_u64), _P(_u64)]),
     "ncsim_circuit_to_text": (_i32, [_vp, C.c_char_p, C.c_size_t, _P(C.c_size_t)]),
-    "ncsim_workload_random_circuit": (_i32, [_u32, _u32, _u64, _dbl, _u32, _u32, _P(_vp)]),
-    "ncsim_workload_random_circuit_rng": (_i32, [_vp, _u32, _u32, _dbl, _u32, _u32, _P(_vp)]),
-    "ncsim_workload_reversible_circuit": (_i32, [_u32, _u32, _u64, _P(_vp)]),
     "ncsim_gate_parse": (_i32, [C.c_char_p, _u32, _P(_vp), _P(_u32)]),
     "ncsim_gate_unitary": (_i32, [_u32, _P(_dbl), _P(_vp)]),
     "ncsim_gate_pauli": (_i32, [_u32, _u64, _u64, _u32, _P(_vp)]),
@@ -122,7 +131,6 @@ _SIGNATURES = {
     "ncsim_sv_profile_enable": (_i32, [_vp, _i32]),
     "ncsim_sv_profile_read": (_i32, [_vp, _vp, _u32, _P(_u32)]),
     "ncsim_measure_stats_noalloc": (_i32, [_vp, _u32, _i32, _u64, _u64, _u32, _vp, _P(_dbl), _P(_dbl)]),
-    "ncsim_batch_random_layers": (_i32, [_u32, _u64, _u32, _u32, _u32, _dbl, _P(_vp)]),
     "ncsim_batch_from_circuits": (_i32, [_u32, _P(_vp), _P(_u64), _P(_vp)]),
     "ncsim_batch_free": (_i32, [_vp]),
     "ncsim_batch_release": (_i32, [_vp]),
@@ -184,9 +192,44 @@ def lib():
     return _lib
 
 
+# the seeded synthetic workloads (libncsim_workloads.so, include/ncsim_workloads.h)
+_WORKLOAD_SIGNATURES = {
+    "ncsim_workload_random_circuit": (_i32, [_u32, _u32, _u64, _dbl, _u32, _u32, _P(_vp)]),
+    "ncsim_workload_random_circuit_rng": (_i32, [_vp, _u32, _u32, _dbl, _u32, _u32, _P(_vp)]),
+    "ncsim_workload_reversible_circuit": (_i32, [_u32, _u32, _u64, _P(_vp)]),
+    "ncsim_batch_random_layers": (_i32, [_u32, _u64, _u32, _u32, _u32, _dbl, _P(_vp)]),
+}
+
+
+def workloads_lib():
+    """The workloads library (seeded synthetic circuits of the benchmark and the tests)."""
+    global _wlib
+    if _wlib is None:
+        lib()  # the engine first: the workloads library resolves its symbols from it
+        if not os.path.exists(WORKLOADS_PATH):
+            raise ImportError(f"{WORKLOADS_PATH} is missing: build it with `python -m ncsim_b200.build`")
+        L = C.CDLL(WORKLOADS_PATH)
+        for name, (res, args) in _WORKLOAD_SIGNATURES.items():
+            f = getattr(L, name)
+            f.restype = res
+            f.argtypes = args
+        _wlib = L
+    return _wlib
+
+
 def _check(status: int) -> None:
     if status != 0:
-        raise SimError(status, lib().ncsim_last_error().decode(errors="replace"))
+        msg = lib().ncsim_last_error().decode(errors="replace")
+        info = ErrorInfo()
+        lib().ncsim_last_error_info(C.byref(info))
+        fields = {}
+        if status == 2:
+            fields = {"qubit": info.qubit, "num_qubits": info.num_qubits}
+        elif status == 4:
+            fields = {"qubit": info.qubit}
+        elif status == 3:
+            fields = {"gate": info.gate.decode(errors="replace"), "expected": info.expected, "got": info.got}
+        raise SimError(status, msg, fields)
 
 
 def _dp(a: np.ndarray):
@@ -326,21 +369,21 @@ class Circuit:
     def random_layers(cls, n: int, depth: int, seed: int, noise_p: float = 0.0, m_lo: int = 0, m_hi: int = 0):
         """The seeded random layer family (H/S/T/SQRT_X/RZ on every qubit, CZ matching)."""
         h = _vp()
-        _check(lib().ncsim_workload_random_circuit(n, depth, seed, noise_p, m_lo, m_hi, C.byref(h)))
+        _check(workloads_lib().ncsim_workload_random_circuit(n, depth, seed, noise_p, m_lo, m_hi, C.byref(h)))
         return cls(h)
 
     @classmethod
     def random_layers_from(cls, rng: "StdRng", n: int, depth: int, noise_p: float = 0.0, m_lo: int = 0, m_hi: int = 0):
         """The random layer family drawn from ``rng``, which keeps its state."""
         h = _vp()
-        _check(lib().ncsim_workload_random_circuit_rng(rng._h, n, depth, noise_p, m_lo, m_hi, C.byref(h)))
+        _check(workloads_lib().ncsim_workload_random_circuit_rng(rng._h, n, depth, noise_p, m_lo, m_hi, C.byref(h)))
         return cls(h)
 
     @classmethod
     def reversible(cls, n: int, gates: int, seed: int) -> "Circuit":
         """The seeded permutation/diagonal family (CX, CCX, CCZ, DIAG, MONOMIAL)."""
         h = _vp()
-        _check(lib().ncsim_workload_reversible_circuit(n, gates, seed, C.byref(h)))
+        _check(workloads_lib().ncsim_workload_reversible_circuit(n, gates, seed, C.byref(h)))
         return cls(h)
 
     def __del__(self):
@@ -700,7 +743,7 @@ class TrajectoryBatch:
         """Trajectory t: StdRng(seed0 + t), n = n_lo + gen_range(0..n_span), the random
         layer circuit with DEPOLARIZE2(p) after every CZ and M on every qubit."""
         h = _vp()
-        _check(lib().ncsim_batch_random_layers(count, seed0, n_lo, n_span, depth, p, C.byref(h)))
+        _check(workloads_lib().ncsim_batch_random_layers(count, seed0, n_lo, n_span, depth, p, C.byref(h)))
         return cls(h)
 
     @classmethod

@@ -13,10 +13,12 @@ PKG = os.path.dirname(os.path.abspath(__file__))
 CSRC = os.path.join(PKG, "csrc")
 OBJ = os.path.join(PKG, "_build")
 LIB = os.path.join(PKG, "libncsim_cuda.so")
+WORKLOADS_LIB = os.path.join(PKG, "libncsim_workloads.so")
 
 SOURCES = [
     "csrc/capi_state.cu",
     "csrc/kernels_plain.cu",
+    "csrc/wide.cu",
     "csrc/fused.cu",
     "csrc/fused_plan.cpp",
     "csrc/batch.cu",
@@ -25,6 +27,9 @@ SOURCES = [
     "csrc/host/ir.cpp",
     "csrc/host/runtime.cpp",
 ]
+# the seeded synthetic workloads of the benchmark and the tests: a second
+# library on top of the engine, outside the drop-in interface
+WORKLOAD_SOURCES = ["csrc/workloads/workloads.cpp"]
 HEADERS = [
     "csrc/engine.cuh",
     "csrc/host_math.hpp",
@@ -33,6 +38,7 @@ HEADERS = [
     "csrc/host/ir.hpp",
     "csrc/host/rng.hpp",
     "../include/ncsim_cuda.h",
+    "../include/ncsim_workloads.h",
 ]
 
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
@@ -55,6 +61,9 @@ def _nvcc() -> str:
     raise RuntimeError("nvcc not found")
 
 
+CUDA_INCLUDE = "/usr/local/cuda/include"
+
+
 def _newer(target: str, deps: list[str]) -> bool:
     if not os.path.exists(target):
         return True
@@ -68,14 +77,17 @@ def build(force: bool = False, verbose: bool = False, ptxas_info: bool = False) 
     env = dict(os.environ)
     env.pop("CXX", None)  # the host compiler is nvcc's default (the system g++)
     headers = [os.path.join(PKG, h) for h in HEADERS]
-    objs = []
+    objs, wobjs = [], []
     procs = []
-    for src in SOURCES:
+    for src in SOURCES + WORKLOAD_SOURCES:
         path = os.path.join(PKG, src)
         obj = os.path.join(OBJ, src.replace("/", "_") + ".o")
-        objs.append(obj)
+        (wobjs if src in WORKLOAD_SOURCES else objs).append(obj)
         if force or _newer(obj, [path] + headers):
-            cmd = [nvcc] + NVFLAGS + ["-x", "cu", "-c", path, "-o", obj]
+            if src in WORKLOAD_SOURCES:  # host code only: compiled by the host compiler, no device image
+                cmd = ["g++", "-std=c++17", "-O3", "-fPIC", "-I" + CUDA_INCLUDE, "-c", path, "-o", obj]
+            else:
+                cmd = [nvcc] + NVFLAGS + ["-x", "cu", "-c", path, "-o", obj]
             if ptxas_info:
                 cmd += ["-Xptxas", "-v"]
             if verbose:
@@ -94,7 +106,14 @@ def build(force: bool = False, verbose: bool = False, ptxas_info: bool = False) 
             sys.stderr.write(f"--- {src}\n{text}\n")
         raise RuntimeError("nvcc failed for " + ", ".join(s for s, _ in failed))
     if force or _newer(LIB, objs):
-        cmd = [nvcc] + ARCH + ["-shared", "-o", LIB] + objs + ["-cudart", "static", "-lpthread"]
+        cmd = [nvcc] + ARCH + ["-shared", "-o", LIB] + objs + ["-cudart", "static", "-lpthread",
+                                                              "-Xlinker", "-soname=libncsim_cuda.so"]
+        if verbose:
+            print(" ".join(cmd), flush=True)
+        subprocess.run(cmd, check=True, env=env)
+    if force or _newer(WORKLOADS_LIB, wobjs + [LIB]):
+        # resolves the engine's symbols from libncsim_cuda.so beside it (no CUDA runtime of its own)
+        cmd = ["g++", "-shared", "-o", WORKLOADS_LIB] + wobjs + ["-L" + PKG, "-lncsim_cuda", "-Wl,-rpath,$ORIGIN"]
         if verbose:
             print(" ".join(cmd), flush=True)
         subprocess.run(cmd, check=True, env=env)

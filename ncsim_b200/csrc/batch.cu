@@ -966,23 +966,23 @@ void parallel_for(size_t count, F&& f) {
 
 }  // namespace
 
-extern "C" {
-
-ncsim_status ncsim_batch_random_layers(uint32_t count, uint64_t seed0, uint32_t n_lo, uint32_t n_span, uint32_t depth,
-                                       double p, ncsim_batch** out) {
-  return guarded([&] {
-    if (!out) throw Error(NCSIM_ERR_INVALID, "out is null");
-    *out = nullptr;
-    if (count == 0) throw Error(NCSIM_ERR_INVALID, "a batch needs at least one trajectory");
-    if (n_span < 1) throw Error(NCSIM_ERR_INVALID, "register span must be at least 1");
-    if (n_lo < MIN_QUBITS || n_lo + n_span - 1 > MAX_QUBITS)
-      throw Error(NCSIM_ERR_UNSUPPORTED, "batched trajectories need 13..26 qubits");
-    if (!(p >= 0.0 && p <= 1.0)) throw Error(NCSIM_ERR_INVALID, "noise probability outside [0, 1]");
-    std::vector<Trajectory> ts(count);
-    parallel_for(count, [&](size_t i) { ts[i] = make_random_layers(seed0 + i, n_lo, n_span, depth, p); });
-    *out = make_batch(std::move(ts));
-  });
+namespace ncsim {
+namespace batch {
+ncsim_batch* batch_random_layers(uint32_t count, uint64_t seed0, uint32_t n_lo, uint32_t n_span, uint32_t depth,
+                                 double p) {
+  if (count == 0) throw Error(NCSIM_ERR_INVALID, "a batch needs at least one trajectory");
+  if (n_span < 1) throw Error(NCSIM_ERR_INVALID, "register span must be at least 1");
+  if (n_lo < MIN_QUBITS || n_lo + n_span - 1 > MAX_QUBITS)
+    throw Error(NCSIM_ERR_UNSUPPORTED, "batched trajectories need 13..26 qubits");
+  if (!(p >= 0.0 && p <= 1.0)) throw Error(NCSIM_ERR_INVALID, "noise probability outside [0, 1]");
+  std::vector<Trajectory> ts(count);
+  parallel_for(count, [&](size_t i) { ts[i] = make_random_layers(seed0 + i, n_lo, n_span, depth, p); });
+  return make_batch(std::move(ts));
 }
+}  // namespace batch
+}  // namespace ncsim
+
+extern "C" {
 
 ncsim_status ncsim_batch_from_circuits(uint32_t count, const ncsim_circuit* const* circuits, const uint64_t* seeds,
                                        ncsim_batch** out) {

@@ -140,6 +140,10 @@ struct Program {
 Trajectory make_random_layers(uint64_t seed, uint32_t n_lo, uint32_t n_span, uint32_t depth, double p);
 // a parsed circuit run with StdRng::seed_from_u64(seed)
 Trajectory make_from_circuit(const ncsim_circuit& c, uint64_t seed);
+// a batch of the random-layer family (trajectory t from StdRng(seed0 + t)),
+// generated and compiled on the host threads (batch.cu)
+ncsim_batch* batch_random_layers(uint32_t count, uint64_t seed0, uint32_t n_lo, uint32_t n_span, uint32_t depth,
+                                 double p);
 // compiles trajectories (in parallel) into one program, in the given order
 Program compile(const std::vector<Trajectory>& ts, const PlanKnobs& knobs);
 

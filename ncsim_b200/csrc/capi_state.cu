@@ -14,7 +14,22 @@ using namespace ncsim;
 namespace ncsim {
 
 thread_local std::string g_last_error;
-void set_last_error(const std::string& m) { g_last_error = m; }
+thread_local ncsim_error_info g_last_info{};
+void set_last_error(const std::string& m) {
+  g_last_error = m;
+  g_last_info = ncsim_error_info{};
+  g_last_info.code = NCSIM_ERR_INVALID;
+}
+void set_last_error(const Error& e) {
+  g_last_error = e.what();
+  g_last_info = ncsim_error_info{};
+  g_last_info.code = e.code;
+  g_last_info.qubit = e.qubit;
+  g_last_info.num_qubits = e.num_qubits;
+  g_last_info.expected = e.expected;
+  g_last_info.got = e.got;
+  std::strncpy(g_last_info.gate, e.gate.c_str(), sizeof(g_last_info.gate) - 1);
+}
 
 int sm_count() {
   static int count = [] {
@@ -78,11 +93,9 @@ void need(const void* p, const char* what) {
 void check_qubits(const uint32_t* qubits, uint32_t k, uint32_t n) {
   if (k && !qubits) throw Error(NCSIM_ERR_INVALID, "qubit list is null");
   for (uint32_t i = 0; i < k; ++i) {
-    if (qubits[i] >= n)
-      throw Error(NCSIM_ERR_QUBIT_OUT_OF_RANGE,
-                  "qubit " + std::to_string(qubits[i]) + " out of range for " + std::to_string(n) + " qubits");
+    if (qubits[i] >= n) throw qubit_out_of_range(qubits[i], n);
     for (uint32_t j = 0; j < i; ++j)
-      if (qubits[j] == qubits[i]) throw Error(NCSIM_ERR_DUPLICATE_QUBIT, "qubit " + std::to_string(qubits[i]) + " listed twice");
+      if (qubits[j] == qubits[i]) throw duplicate_qubit(qubits[i]);
   }
 }
 
@@ -101,7 +114,8 @@ bool hermitian(uint64_t x, uint64_t z, uint32_t phase) {  // src/pauli/ops.rs:25
 const char* kernel_class_name(int c) {
   static const char* names[K_NUM_CLASSES] = {"dense1", "dense2", "dense_tile", "diag", "pairswap", "perm_tile",
                                              "phasepoly", "pauli", "norm", "expect", "inner", "project", "scale",
-                                             "sample", "fused_gemm", "fused_remap", "other"};
+                                             "sample", "fused_gemm", "fused_remap", "other", "dense_wide",
+                                             "perm_wide"};
   return (c >= 0 && c < K_NUM_CLASSES) ? names[c] : "other";
 }
 
@@ -341,6 +355,11 @@ static void state_apply_monomial(ncsim_state* s, const std::vector<uint32_t>& q,
 extern "C" {
 
 const char* ncsim_last_error(void) { return ncsim::g_last_error.c_str(); }
+ncsim_status ncsim_last_error_info(ncsim_error_info* out) {
+  if (!out) return NCSIM_ERR_INVALID;
+  *out = ncsim::g_last_info;
+  return NCSIM_OK;
+}
 int32_t ncsim_abi_version(void) { return 10000; }
 
 ncsim_status ncsim_device_info(int32_t* sm, uint64_t* free_b, uint64_t* total_b) {
@@ -490,7 +509,8 @@ ncsim_status ncsim_sv_apply_matrix(ncsim_state* s, const uint32_t* qubits, uint3
     need(s, "state");
     check_qubits(qubits, k, s->n);
     if (k == 0) return;
-    if (k > 5) throw Error(NCSIM_ERR_UNSUPPORTED, "dense matrices on more than 5 qubits");
+    if (k > uint32_t(MAX_WIDE_DENSE_K))
+      throw Error(NCSIM_ERR_UNSUPPORTED, "dense matrices on more than " + std::to_string(MAX_WIDE_DENSE_K) + " qubits");
     need(m, "matrix");
     std::vector<uint32_t> q(qubits, qubits + k);
     const size_t gd = size_t(1) << k;
@@ -507,7 +527,8 @@ ncsim_status ncsim_sv_apply_monomial(ncsim_state* s, const uint32_t* qubits, uin
     need(s, "state");
     check_qubits(qubits, k, s->n);
     if (k == 0) return;
-    if (k > 10) throw Error(NCSIM_ERR_UNSUPPORTED, "monomial tables on more than 10 qubits");
+    if (k > uint32_t(MAX_WIDE_MONOMIAL_K))
+      throw Error(NCSIM_ERR_UNSUPPORTED, "monomial tables on more than " + std::to_string(MAX_WIDE_MONOMIAL_K) + " qubits");
     need(image, "image");
     need(phase, "phase");
     const size_t gd = size_t(1) << k;

@@ -20,10 +20,35 @@ namespace ncsim {
 // ---------------------------------------------------------------------------
 struct Error : std::runtime_error {
   ncsim_status code;
+  // the fields of the variants that carry them (error.rs:17-33):
+  // QubitOutOfRange {qubit, num_qubits}, DuplicateQubit(qubit), Arity {gate, expected, got}
+  uint64_t qubit = 0, num_qubits = 0, expected = 0, got = 0;
+  std::string gate;
   Error(ncsim_status c, const std::string& m) : std::runtime_error(m), code(c) {}
 };
 
+// check_qubits's errors and apply_gate's arity error (error.rs:69-82, vector.rs:366-372)
+inline Error qubit_out_of_range(uint64_t q, uint64_t n) {
+  Error e(NCSIM_ERR_QUBIT_OUT_OF_RANGE, "qubit " + std::to_string(q) + " out of range for " + std::to_string(n) + " qubits");
+  e.qubit = q;
+  e.num_qubits = n;
+  return e;
+}
+inline Error duplicate_qubit(uint64_t q) {
+  Error e(NCSIM_ERR_DUPLICATE_QUBIT, "qubit " + std::to_string(q) + " listed twice");
+  e.qubit = q;
+  return e;
+}
+inline Error arity_error(const std::string& gate, uint64_t expected, uint64_t got) {
+  Error e(NCSIM_ERR_ARITY, "gate " + gate + " acts on " + std::to_string(expected) + " qubits, " + std::to_string(got) + " given");
+  e.gate = gate;
+  e.expected = expected;
+  e.got = got;
+  return e;
+}
+
 void set_last_error(const std::string& m);
+void set_last_error(const Error& e);
 
 template <class F>
 ncsim_status guarded(F&& f) {
@@ -31,7 +56,7 @@ ncsim_status guarded(F&& f) {
     f();
     return NCSIM_OK;
   } catch (const Error& e) {
-    set_last_error(e.what());
+    set_last_error(e);
     return e.code;
   } catch (const std::bad_alloc&) {
     set_last_error("host allocation failed");
@@ -79,7 +104,8 @@ namespace ncsim {
 // Kernel classes of the launch profiler.
 enum KernelClass : int {
   K_DENSE1, K_DENSE2, K_DENSE_TILE, K_DIAG, K_PAIRSWAP, K_PERM_TILE, K_PHASEPOLY, K_PAULI, K_NORM, K_EXPECT,
-  K_INNER, K_PROJECT, K_SCALE, K_SAMPLE, K_FUSED_GEMM, K_FUSED_REMAP, K_OTHER, K_NUM_CLASSES
+  K_INNER, K_PROJECT, K_SCALE, K_SAMPLE, K_FUSED_GEMM, K_FUSED_REMAP, K_OTHER, K_DENSE_WIDE, K_PERM_WIDE,
+  K_NUM_CLASSES
 };
 const char* kernel_class_name(int c);
 struct ProfRecord {
@@ -196,6 +222,13 @@ struct CplxD {
 };
 
 void launch_dense(ncsim_state* s, const std::vector<uint32_t>& qubits, const std::vector<CplxD>& m);
+// wide gates (wide.cu): dense matrices on 6..MAX_WIDE_DENSE_K qubits, monomial
+// tables on up to MAX_WIDE_MONOMIAL_K qubits, through gathered chunks of fibers
+constexpr int MAX_WIDE_DENSE_K = 13;
+constexpr int MAX_WIDE_MONOMIAL_K = 24;
+void launch_dense_wide(ncsim_state* s, const std::vector<uint32_t>& qubits, const std::vector<CplxD>& m);
+void launch_perm_wide(ncsim_state* s, const std::vector<uint32_t>& qubits, const std::vector<uint32_t>& image,
+                      const std::vector<CplxD>& phase);
 void launch_diag_table(ncsim_state* s, const std::vector<uint32_t>& qubits, const std::vector<CplxD>& diag);
 void launch_perm_table(ncsim_state* s, const std::vector<uint32_t>& qubits, const std::vector<uint32_t>& image,
                        const std::vector<CplxD>& phase);

@@ -1,5 +1,4 @@
-// Parsing, printing and lowering of the host-side circuit IR, and the seeded
-// workload generators.
+// Parsing, printing and lowering of the host-side circuit IR.
 #include "ir.hpp"
 
 #include <algorithm>
@@ -401,15 +400,11 @@ PolyTerms build_poly_terms(const PhasePolyIR& p, const std::vector<uint32_t>& qu
 LoweredOp lower_gate(const GateIR& g, const std::vector<uint32_t>& qubits, uint32_t n) {
   // check_qubits and the arity check of apply_gate (vector.rs:365-372)
   for (size_t i = 0; i < qubits.size(); ++i) {
-    if (qubits[i] >= n)
-      throw Error(NCSIM_ERR_QUBIT_OUT_OF_RANGE,
-                  "qubit " + std::to_string(qubits[i]) + " out of range for " + std::to_string(n) + " qubits");
+    if (qubits[i] >= n) throw qubit_out_of_range(qubits[i], n);
     for (size_t j = 0; j < i; ++j)
-      if (qubits[j] == qubits[i]) throw Error(NCSIM_ERR_DUPLICATE_QUBIT, "qubit " + std::to_string(qubits[i]) + " listed twice");
+      if (qubits[j] == qubits[i]) throw duplicate_qubit(qubits[i]);
   }
-  if (qubits.size() != g.arity())
-    throw Error(NCSIM_ERR_ARITY, "gate " + g.text() + " acts on " + std::to_string(g.arity()) + " qubits, " +
-                                     std::to_string(qubits.size()) + " given");
+  if (qubits.size() != g.arity()) throw arity_error(g.text(), g.arity(), qubits.size());
   LoweredOp op;
   op.qubits = qubits;
   if (g.kind == GateKind::Pauli) {  // Pauli::embed (pauli/mod.rs:292-301)
@@ -435,7 +430,8 @@ LoweredOp lower_gate(const GateIR& g, const std::vector<uint32_t>& qubits, uint3
   if (!monomial_view(g, mo)) {
     op.kind = LoweredKind::Dense;
     op.matrix = gate_matrix(g);
-    if (qubits.size() > 5) throw Error(NCSIM_ERR_UNSUPPORTED, "dense gates on more than 5 qubits");
+    if (qubits.size() > size_t(MAX_WIDE_DENSE_K))
+      throw Error(NCSIM_ERR_UNSUPPORTED, "dense gates on more than " + std::to_string(MAX_WIDE_DENSE_K) + " qubits");
     return op;
   }
   if (mo.affine_identity() && mo.k > 10) {
@@ -443,7 +439,8 @@ LoweredOp lower_gate(const GateIR& g, const std::vector<uint32_t>& qubits, uint3
     op.poly = poly_terms_for(mo.phase, qubits, mo.scalar);
     return op;
   }
-  if (mo.k > 10) throw Error(NCSIM_ERR_UNSUPPORTED, "monomial gates on more than 10 qubits");
+  if (mo.k > uint32_t(MAX_WIDE_MONOMIAL_K))
+    throw Error(NCSIM_ERR_UNSUPPORTED, "monomial gates on more than " + std::to_string(MAX_WIDE_MONOMIAL_K) + " qubits");
   op.kind = LoweredKind::Monomial;
   const size_t d = size_t(1) << mo.k;
   op.image.resize(d);
@@ -868,85 +865,6 @@ ncsim_circuit parse_circuit(const std::string& text) {
     }
   }
   return c;
-}
-
-// ---------------------------------------------------------------------------
-// seeded workloads (same definitions as the CPU oracle's generators; the
-// tests compare the two texts byte for byte)
-// ---------------------------------------------------------------------------
-std::string random_layer_text(uint32_t n, uint32_t depth, ncsim_rng& rng, double noise_p, uint32_t m_lo, uint32_t m_hi) {
-  std::string s = "QUBITS " + std::to_string(n) + "\n";
-  static const char* one[] = {"H", "S", "T", "SQRT_X"};
-  const double tau = 6.28318530717958647692;
-  std::vector<uint32_t> perm(n);
-  for (uint32_t layer = 0; layer < depth; ++layer) {
-    for (uint32_t q = 0; q < n; ++q) {
-      uint64_t g = rng.range64(0, 5);
-      if (g < 4) s += std::string(one[g]) + " " + std::to_string(q) + "\n";
-      else s += "RZ(" + fmt_f64(rng.f64() * tau) + ") " + std::to_string(q) + "\n";
-    }
-    for (uint32_t i = 0; i < n; ++i) perm[i] = i;
-    for (uint32_t i = n; i-- > 1;) std::swap(perm[i], perm[rng.range32(0, i + 1)]);
-    for (uint32_t i = 0; i + 1 < n; i += 2) {
-      const std::string pair = std::to_string(perm[i]) + " " + std::to_string(perm[i + 1]);
-      s += "CZ " + pair + "\n";
-      if (noise_p > 0.0) s += "DEPOLARIZE2(" + fmt_f64(noise_p) + ") " + pair + "\n";
-    }
-  }
-  for (uint32_t q = m_lo; q < m_hi && q < n; ++q) s += "M " + std::to_string(q) + "\n";
-  return s;
-}
-
-static std::vector<uint32_t> pick_distinct(ncsim_rng& rng, uint32_t n, uint32_t k) {
-  std::vector<uint32_t> v;
-  while (v.size() < k) {
-    uint32_t q = uint32_t(rng.range64(0, n));
-    if (std::find(v.begin(), v.end(), q) == v.end()) v.push_back(q);
-  }
-  return v;
-}
-
-static std::string random_terms(ncsim_rng& rng, uint32_t nv, uint32_t count) {
-  std::string s;
-  for (uint32_t t = 0; t < count; ++t) {
-    uint32_t deg = 1 + uint32_t(rng.range64(0, 3));
-    auto vars = pick_distinct(rng, nv, std::min(deg, nv));
-    uint64_t c = 1 + rng.range64(0, 7);
-    s += ";" + std::to_string(c) + ":";
-    for (size_t i = 0; i < vars.size(); ++i) s += (i ? "," : "") + std::to_string(uint64_t(1) << vars[i]);
-  }
-  return s;
-}
-
-std::string reversible_text(uint32_t n, uint32_t gates, ncsim_rng& rng) {
-  std::string s = "QUBITS " + std::to_string(n) + "\n";
-  for (uint32_t q = 0; q < std::min<uint32_t>(16, n); ++q) s += "H " + std::to_string(q) + "\n";
-  for (uint32_t i = 0; i < gates; ++i) {
-    uint64_t g = rng.range64(0, 5);
-    if (g <= 2) {
-      auto qs = pick_distinct(rng, n, g == 0 ? 2 : 3);
-      s += g == 0 ? "CX" : g == 1 ? "CCX" : "CCZ";
-      for (uint32_t q : qs) s += " " + std::to_string(q);
-      s += "\n";
-    } else if (g == 3) {
-      s += "DIAG(3;0" + random_terms(rng, n, 40) + ")";
-      for (uint32_t q = 0; q < n; ++q) s += " " + std::to_string(q);
-      s += "\n";
-    } else {
-      auto qs = pick_distinct(rng, n, 8);
-      std::vector<uint64_t> rows(8);
-      do {
-        for (auto& r : rows) r = rng.range64(0, 256);
-      } while (gf2_rank_of(rows) != 8);
-      uint64_t shift = rng.range64(0, 256);
-      s += "MONOMIAL(";
-      for (int r = 0; r < 8; ++r) s += (r ? "," : "") + std::to_string(rows[r]);
-      s += ";" + std::to_string(shift) + ";3;0" + random_terms(rng, 8, 8) + ";0,0,0)";
-      for (uint32_t q : qs) s += " " + std::to_string(q);
-      s += "\n";
-    }
-  }
-  return s;
 }
 
 }  // namespace ncsim

@@ -130,7 +130,5 @@ struct ncsim_gate {
 namespace ncsim {
 ncsim_circuit parse_circuit(const std::string& text);
 GateIR parse_gate_token(const std::string& tok, uint32_t nq_hint);
-std::string random_layer_text(uint32_t n, uint32_t depth, ncsim_rng& rng, double noise_p, uint32_t m_lo, uint32_t m_hi);
-std::string reversible_text(uint32_t n, uint32_t gates, ncsim_rng& rng);
 std::string fmt_f64(double v);
 }  // namespace ncsim

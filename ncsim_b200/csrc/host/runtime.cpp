@@ -149,36 +149,6 @@ ncsim_status ncsim_circuit_to_text(const ncsim_circuit* c, char* buf, size_t cap
     if (buf && cap > t.size()) std::memcpy(buf, t.c_str(), t.size() + 1);
   });
 }
-ncsim_status ncsim_workload_random_circuit(uint32_t n, uint32_t depth, uint64_t seed, double noise_p, uint32_t m_lo,
-                                           uint32_t m_hi, ncsim_circuit** out) {
-  return guarded([&] {
-    need(out, "out");
-    *out = nullptr;
-    if (n < 1 || n > 64) throw Error(NCSIM_ERR_INVALID, "workload register must have 1..64 qubits");
-    ncsim_rng rng(seed);
-    *out = new ncsim_circuit(parse_circuit(random_layer_text(n, depth, rng, noise_p, m_lo, m_hi)));
-  });
-}
-ncsim_status ncsim_workload_random_circuit_rng(ncsim_rng* rng, uint32_t n, uint32_t depth, double noise_p, uint32_t m_lo,
-                                               uint32_t m_hi, ncsim_circuit** out) {
-  return guarded([&] {
-    need(rng, "rng");
-    need(out, "out");
-    *out = nullptr;
-    if (n < 1 || n > 64) throw Error(NCSIM_ERR_INVALID, "workload register must have 1..64 qubits");
-    *out = new ncsim_circuit(parse_circuit(random_layer_text(n, depth, *rng, noise_p, m_lo, m_hi)));
-  });
-}
-ncsim_status ncsim_workload_reversible_circuit(uint32_t n, uint32_t gates, uint64_t seed, ncsim_circuit** out) {
-  return guarded([&] {
-    need(out, "out");
-    *out = nullptr;
-    if (n < 8 || n > 64) throw Error(NCSIM_ERR_INVALID, "reversible workload needs 8..64 qubits");
-    ncsim_rng rng(seed);
-    *out = new ncsim_circuit(parse_circuit(reversible_text(n, gates, rng)));
-  });
-}
-
 // ---- gates ----
 ncsim_status ncsim_gate_parse(const char* token, uint32_t arity_hint, ncsim_gate** out, uint32_t* arity) {
   return guarded([&] {
@@ -200,12 +170,14 @@ ncsim_status ncsim_gate_unitary(uint32_t k, const double* m, ncsim_gate** out) {
   return guarded([&] {
     need(m, "matrix");
     need(out, "out");
-    if (k < 1 || k > 5) throw Error(NCSIM_ERR_UNSUPPORTED, "dense gates on 1..5 qubits");
+    if (k < 1 || k > uint32_t(MAX_WIDE_DENSE_K))
+      throw Error(NCSIM_ERR_UNSUPPORTED, "dense gates on 1.." + std::to_string(MAX_WIDE_DENSE_K) + " qubits");
     auto* g = new ncsim_gate();
     g->g.kind = GateKind::Unitary;
     g->g.uk = k;
     const size_t d = size_t(1) << k;
-    for (size_t i = 0; i < d * d; ++i) g->g.umat.push_back({m[2 * i], m[2 * i + 1]});
+    g->g.umat.resize(d * d);
+    for (size_t i = 0; i < d * d; ++i) g->g.umat[i] = {m[2 * i], m[2 * i + 1]};
     *out = g;
   });
 }

@@ -995,7 +995,10 @@ void launch_dense(ncsim_state* s, const std::vector<uint32_t>& qubits, const std
     NCSIM_LAUNCHED("dense2");
     return;
   }
-  if (k > MAX_DENSE_K) throw Error(NCSIM_ERR_UNSUPPORTED, "dense gates on more than 5 qubits");
+  if (k > MAX_DENSE_K) {
+    launch_dense_wide(s, qubits, m);
+    return;
+  }
   NCSIM_DISPATCH(s, {
     auto* P = new DenseParams<R>();
     P->g = make_geom(s->n, qubits, tile_bits_for<R>(s->n, k));
@@ -1087,8 +1090,12 @@ void launch_perm_table(ncsim_state* s, const std::vector<uint32_t>& qubits, cons
   const int gd = 1 << k;
   bool diagonal = true;
   for (int x = 0; x < gd; ++x) diagonal &= image[x] == uint32_t(x);
-  if (diagonal) {
+  if (diagonal && k <= MAX_DIAG_K) {
     launch_diag_table(s, qubits, phase);
+    return;
+  }
+  if (k > MAX_TILE_K) {
+    launch_perm_wide(s, qubits, image, phase);
     return;
   }
   // pair-swap shape: moved patterns pair up under one xor d on a sub-cube,
@@ -1149,7 +1156,6 @@ void launch_perm_table(ncsim_state* s, const std::vector<uint32_t>& qubits, cons
       }
     }
   }
-  if (k > MAX_TILE_K) throw Error(NCSIM_ERR_UNSUPPORTED, "monomial gates on more than 10 qubits");
   NCSIM_DISPATCH(s, {
     auto* P = new PermParams<R>();
     P->g = make_geom(s->n, qubits, tile_bits_for<R>(s->n, k));

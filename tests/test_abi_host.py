@@ -12,8 +12,8 @@ import pytest
 ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 
 
-def _declared_symbols():
-    hdr = open(os.path.join(ROOT, "include", "ncsim_cuda.h")).read()
+def _declared_symbols(header="ncsim_cuda.h"):
+    hdr = open(os.path.join(ROOT, "include", header)).read()
     hdr = re.sub(r"/\*.*?\*/", "", hdr, flags=re.S)
     return sorted(set(re.findall(r"\b(ncsim_[a-z0-9_]+)\s*\(", hdr)))
 
@@ -25,6 +25,18 @@ def test_library_exports_every_declared_symbol(nb):
     missing = [s for s in syms if not hasattr(lib, s)]
     assert not missing, missing
     assert set(syms) <= set(nb._SIGNATURES), set(syms) - set(nb._SIGNATURES)
+
+
+def test_workloads_live_in_their_own_library(nb):
+    """The seeded workloads are declared in ncsim_workloads.h and exported by
+    libncsim_workloads.so, not by the engine's drop-in library."""
+    syms = _declared_symbols("ncsim_workloads.h")
+    assert set(syms) == set(nb._WORKLOAD_SIGNATURES)
+    assert not set(syms) & set(_declared_symbols())
+    w = nb.workloads_lib()
+    assert all(hasattr(w, s) for s in syms)
+    engine = C.CDLL(nb.LIB_PATH)
+    assert not any(hasattr(engine, s) for s in syms)
 
 
 def test_rng_matches_oracle(nb, oracle):

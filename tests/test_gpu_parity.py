@@ -354,6 +354,19 @@ def test_argument_errors_on_device(nb):
     with pytest.raises(nb.SimError) as e:
         s.apply_gate(nb.Gate.parse("CX"), [2, 2])
     assert e.value.kind == "DuplicateQubit"
+    # the variants' fields cross the ABI (error.rs:17-33)
+    with pytest.raises(nb.SimError) as e:
+        s.apply_gate(nb.Gate.parse("CCZ"), [0, 9, 1])
+    assert e.value.kind == "QubitOutOfRange" and e.value.fields == {"qubit": 9, "num_qubits": 6}
+    with pytest.raises(nb.SimError) as e:
+        s.apply_gate(nb.Gate.parse("CZ"), [3, 4, 3])
+    assert e.value.fields == {"qubit": 3}
+    with pytest.raises(nb.SimError) as e:
+        s.apply_gate(nb.Gate.parse("CCZ"), [0, 1])
+    assert e.value.fields == {"gate": "CCZ", "expected": 3, "got": 2}
+    with pytest.raises(nb.SimError) as e:
+        s.apply_matrix(np.eye(4), [0, 7])
+    assert e.value.fields == {"qubit": 7, "num_qubits": 6}
     with pytest.raises(nb.SimError) as e:
         s.run(nb.Circuit.parse("QUBITS 5\nH 0\n"), nb.StdRng(0))
     assert e.value.kind == "Invalid"
