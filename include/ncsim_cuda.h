@@ -182,6 +182,22 @@ ncsim_status ncsim_sv_sample(const ncsim_state* s, const double* uniforms, uint6
 ncsim_status ncsim_sv_kron(const ncsim_state* a, const ncsim_state* b, ncsim_state** out);
 /* Waits for the state's queued device work. */
 ncsim_status ncsim_sv_synchronize(const ncsim_state* s);
+/* The device address and size in bytes of the state's amplitude array (for
+ * zero-copy views by a communication layer: the sharded register exchanges
+ * halves of it between devices).  Work queued on the state must be finished
+ * (ncsim_sv_synchronize) before another stream touches the array. */
+ncsim_status ncsim_sv_device_pointer(const ncsim_state* s, void** ptr, uint64_t* bytes);
+/* Sum |a|^2 over each block of `block` consecutive amplitudes (a power of
+ * two), FP64, into nblocks = 2^n / block host doubles: the first step of
+ * StateVector::sample (vector.rs:494-501), for a sampler that spans several
+ * registers. */
+ncsim_status ncsim_sv_block_weights(const ncsim_state* s, uint64_t block, double* out, uint64_t nblocks);
+/* The last step of StateVector::sample (vector.rs:508-538) for given shots:
+ * shot k walks block blocks[k] from the running sum accs[k] (the weight of
+ * everything before that block) to the first index whose running sum exceeds
+ * targets[k]; zero-weight indices are never returned. */
+ncsim_status ncsim_sv_sample_walk(const ncsim_state* s, uint64_t block, const double* targets, const uint64_t* blocks,
+                                  const double* accs, uint64_t shots, uint64_t* out);
 /* Device time on the state's stream: start records an event; stop records a
  * second one, waits for it and writes the milliseconds between them. */
 ncsim_status ncsim_sv_timer_start(ncsim_state* s);

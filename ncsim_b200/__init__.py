@@ -82,6 +82,9 @@ _SIGNATURES = {
     "ncsim_sv_set_amplitudes": (_i32, [_vp, _P(_dbl), _u64]),
     "ncsim_sv_get_amplitudes": (_i32, [_vp, _P(_dbl), _u64]),
     "ncsim_sv_get_amplitudes_range": (_i32, [_vp, _u64, _u64, _P(_dbl)]),
+    "ncsim_sv_device_pointer": (_i32, [_vp, _P(_vp), _P(_u64)]),
+    "ncsim_sv_block_weights": (_i32, [_vp, _u64, _P(_dbl), _u64]),
+    "ncsim_sv_sample_walk": (_i32, [_vp, _u64, _P(_dbl), _P(_u64), _P(_dbl), _u64, _P(_u64)]),
     "ncsim_sv_get_amplitude": (_i32, [_vp, _u64, _P(_dbl)]),
     "ncsim_sv_gather_amplitudes": (_i32, [_vp, _P(_u64), _u64, _P(_dbl)]),
     "ncsim_sv_apply_matrix": (_i32, [_vp, _P(_u32), _u32, _P(_dbl)]),
@@ -500,6 +503,45 @@ class GpuStateVector:
     def set_amplitudes(self, amps: np.ndarray) -> None:
         b = np.ascontiguousarray(np.asarray(amps, dtype=np.complex128)).view(np.float64)
         _check(lib().ncsim_sv_set_amplitudes(self._h, _dp(b), 1 << self.n))
+
+    def device_pointer(self) -> tuple[int, int]:
+        """(device address, bytes) of the amplitude array."""
+        p, b = _vp(), _u64()
+        _check(lib().ncsim_sv_device_pointer(self._h, C.byref(p), C.byref(b)))
+        return int(p.value or 0), b.value
+
+    def torch_view(self):
+        """A torch tensor over the amplitude array, without a copy (complex128 or
+        complex64, on this state's device).  The state's queued work must be
+        finished (``synchronize``) before torch touches it, and torch's work
+        before the state's next call."""
+        import torch
+
+        ptr, nbytes = self.device_pointer()
+        dt = "<c16" if self.precision == C128 else "<c8"
+
+        class _View:
+            __cuda_array_interface__ = {"shape": (1 << self.n,), "typestr": dt, "data": (ptr, False),
+                                        "version": 3, "strides": None}
+
+        return torch.as_tensor(_View(), device="cuda")
+
+    def block_weights(self, block: int = 4096) -> np.ndarray:
+        """|a|^2 summed over each block of ``block`` consecutive amplitudes (FP64)."""
+        nbl = (1 << self.n) // block
+        out = np.empty(nbl)
+        _check(lib().ncsim_sv_block_weights(self._h, block, _dp(out), nbl))
+        return out
+
+    def sample_walk(self, block: int, targets, blocks, accs) -> np.ndarray:
+        """The in-block walk of one-pass sampling for the given shots (vector.rs:508-538)."""
+        t = np.ascontiguousarray(targets, dtype=np.float64)
+        b = np.ascontiguousarray(blocks, dtype=np.uint64)
+        a = np.ascontiguousarray(accs, dtype=np.float64)
+        out = np.empty(t.size, dtype=np.uint64)
+        _check(lib().ncsim_sv_sample_walk(self._h, block, _dp(t), b.ctypes.data_as(_P(_u64)), _dp(a), t.size,
+                                          out.ctypes.data_as(_P(_u64))))
+        return out
 
     def set_basis(self, index: int) -> None:
         """The register becomes the basis state |index> (in place)."""

@@ -714,6 +714,60 @@ ncsim_status ncsim_sv_kron(const ncsim_state* a, const ncsim_state* b, ncsim_sta
   });
 }
 
+ncsim_status ncsim_sv_device_pointer(const ncsim_state* s, void** ptr, uint64_t* bytes) {
+  return guarded([&] {
+    need(s, "state");
+    need(ptr, "out");
+    *ptr = s->amp;
+    if (bytes) *bytes = s->bytes();
+  });
+}
+
+ncsim_status ncsim_sv_block_weights(const ncsim_state* s, uint64_t block, double* out, uint64_t nblocks) {
+  return guarded([&] {
+    need(s, "state");
+    need(out, "out");
+    if (block == 0 || (block & (block - 1)) || block > s->len) throw Error(NCSIM_ERR_INVALID, "block must be a power of two <= 2^n");
+    if (nblocks != s->len / block) throw Error(NCSIM_ERR_INVALID, "output holds 2^n / block weights");
+    std::lock_guard<std::recursive_mutex> lk(s->mu);
+    double* d_w = nullptr;
+    NCSIM_CUDA(pool_alloc(&d_w, nblocks * sizeof(double), s->stream));
+    launch_block_weights(s, d_w, nblocks, block);
+    NCSIM_CUDA(cudaMemcpyAsync(out, d_w, nblocks * sizeof(double), cudaMemcpyDeviceToHost, s->stream));
+    NCSIM_CUDA(cudaFreeAsync(d_w, s->stream));
+    NCSIM_CUDA(cudaStreamSynchronize(s->stream));
+  });
+}
+
+ncsim_status ncsim_sv_sample_walk(const ncsim_state* s, uint64_t block, const double* targets, const uint64_t* blocks,
+                                  const double* accs, uint64_t shots, uint64_t* out) {
+  return guarded([&] {
+    need(s, "state");
+    if (block == 0 || (block & (block - 1)) || block > s->len) throw Error(NCSIM_ERR_INVALID, "block must be a power of two <= 2^n");
+    if (shots == 0) return;
+    need(targets, "targets");
+    need(blocks, "blocks");
+    need(accs, "accs");
+    need(out, "out");
+    for (uint64_t k = 0; k < shots; ++k)
+      if (blocks[k] >= s->len / block) throw Error(NCSIM_ERR_INVALID, "block index outside the register");
+    std::lock_guard<std::recursive_mutex> lk(s->mu);
+    double *d_u = nullptr, *d_acc = nullptr;
+    uint64_t *d_blk = nullptr, *d_out = nullptr;
+    NCSIM_CUDA(pool_alloc(&d_u, shots * sizeof(double), s->stream));
+    NCSIM_CUDA(pool_alloc(&d_acc, shots * sizeof(double), s->stream));
+    NCSIM_CUDA(pool_alloc(&d_blk, shots * sizeof(uint64_t), s->stream));
+    NCSIM_CUDA(pool_alloc(&d_out, shots * sizeof(uint64_t), s->stream));
+    NCSIM_CUDA(cudaMemcpyAsync(d_u, targets, shots * sizeof(double), cudaMemcpyHostToDevice, s->stream));
+    NCSIM_CUDA(cudaMemcpyAsync(d_acc, accs, shots * sizeof(double), cudaMemcpyHostToDevice, s->stream));
+    NCSIM_CUDA(cudaMemcpyAsync(d_blk, blocks, shots * sizeof(uint64_t), cudaMemcpyHostToDevice, s->stream));
+    launch_sample_walk(s, d_u, d_blk, d_acc, shots, block, d_out);
+    NCSIM_CUDA(cudaMemcpyAsync(out, d_out, shots * sizeof(uint64_t), cudaMemcpyDeviceToHost, s->stream));
+    for (void* p : {(void*)d_u, (void*)d_acc, (void*)d_blk, (void*)d_out}) NCSIM_CUDA(cudaFreeAsync(p, s->stream));
+    NCSIM_CUDA(cudaStreamSynchronize(s->stream));
+  });
+}
+
 ncsim_status ncsim_sv_synchronize(const ncsim_state* s) {
   return guarded([&] {
     need(s, "state");

@@ -124,6 +124,9 @@ extern "C" {
     pub fn ncsim_sv_sample(s: *const ncsim_state, uniforms: *const f64, shots: u64, out: *mut u64) -> ncsim_status;
     pub fn ncsim_sv_kron(a: *const ncsim_state, b: *const ncsim_state, out: *mut *mut ncsim_state) -> ncsim_status;
     pub fn ncsim_sv_synchronize(s: *const ncsim_state) -> ncsim_status;
+    pub fn ncsim_sv_device_pointer(s: *const ncsim_state, ptr: *mut *mut c_void, bytes: *mut u64) -> ncsim_status;
+    pub fn ncsim_sv_block_weights(s: *const ncsim_state, block: u64, out: *mut f64, nblocks: u64) -> ncsim_status;
+    pub fn ncsim_sv_sample_walk(s: *const ncsim_state, block: u64, targets: *const f64, blocks: *const u64, accs: *const f64, shots: u64, out: *mut u64) -> ncsim_status;
     pub fn ncsim_sv_timer_start(s: *mut ncsim_state) -> ncsim_status;
     pub fn ncsim_sv_timer_stop(s: *mut ncsim_state, milliseconds: *mut f64) -> ncsim_status;
     pub fn ncsim_sv_compare(a: *const ncsim_state, b: *const ncsim_state, inner_re_im: *mut f64, norm_a: *mut f64, norm_b: *mut f64, max_abs_diff: *mut f64) -> ncsim_status;
