@@ -375,8 +375,10 @@ def trajectory_bench(nb, args, dist, peak, peak_kind):
     if args.traj_launch:
         ctas, bufs = (int(v) for v in args.traj_launch.split(","))
         tb.set_config(ctas_per_sm=ctas, buffers=bufs)
-    tb.run()  # tunes the launch configuration on first use (unless it was given)
+    tb.run()  # tunes the planner's knobs per register size and the launch configuration on first use
     cfg = tb.config()
+    sizes = sorted(set(int(v) for v in tb.qubits()))
+    knobs = {str(n): tb.knobs(n) for n in sizes}
     for _ in range(args.warmup):
         tb.run()
     barrier(dist)
@@ -397,6 +399,10 @@ def trajectory_bench(nb, args, dist, peak, peak_kind):
                                f"depth {depth}, DEPOLARIZE2({p}) after every CZ, M on every qubit; "
                                f"StdRng(seed0 + t), seed0 = {seed0}",
                    "count": count, "depth": depth, "p": p, "launch": cfg,
+                   "planner_knobs_by_size": {n: {"set": k["knob_set"], "window_step": k["window_step"],
+                                                 "greedy_stages": k["greedy_stages"],
+                                                 "timed_ms": [round(v, 3) for v in k["timed_ms"]]}
+                                             for n, k in knobs.items()},
                    "l2": "about 1 TB of state traffic per step (no flush needed)"},
         "gpu_launches_per_step": 1,
         "plan": {k: info[k] for k in ("source_gates", "noise_events", "folded_ops", "passes", "tile_passes",

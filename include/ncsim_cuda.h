@@ -366,12 +366,36 @@ ncsim_status ncsim_batch_free(ncsim_batch* b);
 ncsim_status ncsim_batch_release(ncsim_batch* b);
 ncsim_status ncsim_batch_info(const ncsim_batch* b, ncsim_batch_stats* st);
 ncsim_status ncsim_batch_trajectory_qubits(const ncsim_batch* b, uint32_t* n);
+/* The host planner's knobs for registers of n qubits, chosen per size class by
+ * the autotuner: candidate windows (qubits 0..3 and 9 consecutive qubits every
+ * window_step qubits), the window and stage choice rules, and the device
+ * milliseconds each candidate knob set took on that class (0 when not timed).
+ * The choice is made on first use, or read from a cache file keyed by device,
+ * register size and program size (NCSIM_TUNE_CACHE, else
+ * $XDG_CACHE_HOME or ~/.cache /ncsim_b200/batch_knobs.txt). */
+typedef struct ncsim_batch_knobs_info {
+  uint32_t knob_set;
+  uint32_t window_step;
+  uint32_t greedy_windows;
+  uint32_t greedy_stages;
+  uint32_t final_;  /* 1: the program is compiled with these knobs */
+  double timed_ms[4];
+} ncsim_batch_knobs_info;
+ncsim_status ncsim_batch_knobs(const ncsim_batch* b, uint32_t n, ncsim_batch_knobs_info* out);
+/* Compiles registers of n qubits with candidate knob set `knob_set` (0..3)
+ * instead of the tuned one, while the batch still holds its trajectories;
+ * final_ != 0 makes the knobs final (no tuning on first use, trajectories
+ * dropped). */
+ncsim_status ncsim_batch_set_knob_set(ncsim_batch* b, uint32_t n, uint32_t knob_set, int32_t final_);
 ncsim_status ncsim_batch_set_config(ncsim_batch* b, const ncsim_batch_config* cfg);
 /* The configuration the next run uses (tuned on the current device if unset). */
 ncsim_status ncsim_batch_get_config(ncsim_batch* b, ncsim_batch_config* cfg);
-/* Times each candidate configuration on an evenly strided sample of the
- * batch (0 = the whole batch) and keeps the fastest; runs on first use when
- * no configuration was set, once per (device, count, largest register). */
+/* Times each candidate launch configuration on an evenly strided sample of
+ * the batch (0 = the whole batch) and keeps the fastest; runs on first use
+ * when no configuration was set, once per (device, count, largest register).
+ * While the batch still holds its trajectories (before its first run, when
+ * the knob cache lacked a size class), the planner's knobs are timed again
+ * per size class first. */
 ncsim_status ncsim_batch_tune(ncsim_batch* b, uint32_t sample, ncsim_batch_config* best);
 /* Runs every trajectory on the current device (one CUDA graph launch: counter
  * reset, the kernel, result copies to pinned host memory); device_ms

@@ -137,6 +137,8 @@ _SIGNATURES = {
     "ncsim_batch_from_circuits": (_i32, [_u32, _P(_vp), _P(_u64), _P(_vp)]),
     "ncsim_batch_free": (_i32, [_vp]),
     "ncsim_batch_release": (_i32, [_vp]),
+    "ncsim_batch_knobs": (_i32, [_vp, _u32, _vp]),
+    "ncsim_batch_set_knob_set": (_i32, [_vp, _u32, _u32, _i32]),
     "ncsim_batch_info": (_i32, [_vp, _vp]),
     "ncsim_batch_trajectory_qubits": (_i32, [_vp, _P(_u32)]),
     "ncsim_batch_set_config": (_i32, [_vp, _vp]),
@@ -768,6 +770,11 @@ class BatchConfig(C.Structure):
                 "order": "largest_first" if self.order == 0 else "given"}
 
 
+class BatchKnobs(C.Structure):
+    _fields_ = [("knob_set", C.c_uint32), ("window_step", C.c_uint32), ("greedy_windows", C.c_uint32),
+                ("greedy_stages", C.c_uint32), ("final_", C.c_uint32), ("timed_ms", C.c_double * 4)]
+
+
 class TrajectoryBatch:
     """Independent noisy trajectories, each ``QuantumState::run`` of its circuit
     with its own ``StdRng`` (src/state/mod.rs:168-183), run together on the GPU.
@@ -807,6 +814,16 @@ class TrajectoryBatch:
         """Gives back the batch's device memory, stream and graph; the next run
         sets them up again on the then-current device."""
         _check(lib().ncsim_batch_release(self._h))
+
+    def knobs(self, n: int) -> dict:
+        """The planner's knobs for registers of n qubits (and what each candidate took)."""
+        k = BatchKnobs()
+        _check(lib().ncsim_batch_knobs(self._h, n, C.byref(k)))
+        return {"knob_set": k.knob_set, "window_step": k.window_step, "greedy_windows": bool(k.greedy_windows),
+                "greedy_stages": bool(k.greedy_stages), "final": bool(k.final_), "timed_ms": list(k.timed_ms)}
+
+    def set_knob_set(self, n: int, knob_set: int, final: bool = False) -> None:
+        _check(lib().ncsim_batch_set_knob_set(self._h, n, knob_set, int(final)))
 
     def info(self) -> dict:
         st = BatchStats()

@@ -19,11 +19,18 @@
 // which keeps every 16-byte chunk whole and makes the three stage layouts,
 // the chunk copies and the FP64 sums conflict-free.
 #include <algorithm>
+#include <array>
 #include <atomic>
+#include <cstdlib>
+#include <fstream>
+#include <sstream>
 #include <cmath>
 #include <map>
 #include <numeric>
 #include <thread>
+
+#include <sys/stat.h>
+#include <unistd.h>
 
 #include "batch_plan.hpp"
 #include "engine.cuh"
@@ -630,6 +637,14 @@ void buf_free(void* p, size_t cap) {
 // ---------------------------------------------------------------------------
 struct ncsim_batch {
   Program prog;
+  // the folded trajectories, kept until the planner's knobs are final (the
+  // autotuner recompiles the program with other knobs), then dropped
+  std::vector<Trajectory> ts;
+  std::vector<PlanKnobs> knobs_by_n = std::vector<PlanKnobs>(MAX_QUBITS + 1);
+  std::vector<int> knob_set_by_n = std::vector<int>(MAX_QUBITS + 1, 0);
+  std::vector<std::array<double, NUM_KNOB_SETS>> knob_ms =
+      std::vector<std::array<double, NUM_KNOB_SETS>>(MAX_QUBITS + 1);  // timed per size class and knob set
+  bool knobs_final = false;
   std::vector<uint32_t> order_lpt, order_seq;
   std::mutex mu;
   int device = -1;
@@ -716,15 +731,20 @@ T* dev_ptr(ncsim_batch* b, size_t off) {
   return reinterpret_cast<T*>(b->d_prog + off);
 }
 
-void ensure_device(ncsim_batch* b) {
-  int dev = 0;
-  NCSIM_CUDA(cudaGetDevice(&dev));
-  if (b->device == dev) return;
-  if (b->device >= 0) b->release();  // on its old device; the caller's device stays current
-  b->device = dev;
-  NCSIM_CUDA(cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking));
-  NCSIM_CUDA(cudaEventCreate(&b->ev0));
-  NCSIM_CUDA(cudaEventCreate(&b->ev1));
+// (Re)uploads the program and the trajectory orders to the device (the
+// batch's device must be current).  A captured graph holds the old pointers.
+void upload_program(ncsim_batch* b) {
+  if (b->graph) {
+    NCSIM_CUDA(cudaStreamSynchronize(b->stream));
+    NCSIM_CUDA(cudaGraphExecDestroy(b->graph));
+    b->graph = nullptr;
+  }
+  if (b->d_prog) {
+    NCSIM_CUDA(cudaStreamSynchronize(b->stream));
+    buf_free(b->d_prog, b->prog_cap);
+    b->d_prog = nullptr;
+    b->prog_cap = 0;
+  }
   const Program& P = b->prog;
   const uint32_t c = b->count();
   size_t off = 0;
@@ -752,6 +772,20 @@ void ensure_device(ncsim_batch* b) {
   up(b->off_draws, P.draws.data(), P.draws.size() * sizeof(double));
   up(b->off_lpt, b->order_lpt.data(), size_t(c) * 4);
   up(b->off_seq, b->order_seq.data(), size_t(c) * 4);
+  NCSIM_CUDA(cudaStreamSynchronize(b->stream));
+}
+
+void ensure_device(ncsim_batch* b) {
+  int dev = 0;
+  NCSIM_CUDA(cudaGetDevice(&dev));
+  if (b->device == dev) return;
+  if (b->device >= 0) b->release();  // on its old device; the caller's device stays current
+  b->device = dev;
+  NCSIM_CUDA(cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking));
+  NCSIM_CUDA(cudaEventCreate(&b->ev0));
+  NCSIM_CUDA(cudaEventCreate(&b->ev1));
+  const uint32_t c = b->count();
+  upload_program(b);
   NCSIM_CUDA(cudaMalloc(&b->d_queue, 2 * sizeof(uint32_t)));
   NCSIM_CUDA(cudaMalloc(&b->d_rec, size_t(c) * 8));
   NCSIM_CUDA(cudaMalloc(&b->d_z0, size_t(c) * 8));
@@ -760,7 +794,6 @@ void ensure_device(ncsim_batch* b) {
   NCSIM_CUDA(cudaMallocHost(&b->h_z0, size_t(c) * 8));
   NCSIM_CUDA(cudaMallocHost(&b->h_norm, size_t(c) * 8));
   NCSIM_CUDA(cudaMallocHost(&b->h_err, sizeof(uint32_t)));
-  NCSIM_CUDA(cudaStreamSynchronize(b->stream));
   static bool attr_done[64] = {};
   if (dev < 64 && !attr_done[dev]) {
     NCSIM_CUDA(cudaFuncSetAttribute(k_batch<2>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(SMEM_NBUF2)));
@@ -907,6 +940,168 @@ ncsim_batch_config tune(ncsim_batch* b, uint32_t sample) {
   return best;
 }
 
+// ---------------------------------------------------------------------------
+// planner knobs per register size: timed per size class, kept in a cache file
+// ---------------------------------------------------------------------------
+// The file holds one "key knob_set" line per (device, register size, program
+// size): NCSIM_TUNE_CACHE names it, else $XDG_CACHE_HOME (or ~/.cache)
+// /ncsim_b200/batch_knobs.txt.
+std::string knob_cache_path() {
+  if (const char* p = std::getenv("NCSIM_TUNE_CACHE")) return p;
+  std::string base;
+  if (const char* x = std::getenv("XDG_CACHE_HOME")) base = x;
+  else if (const char* h = std::getenv("HOME")) base = std::string(h) + "/.cache";
+  else return "";
+  return base + "/ncsim_b200/batch_knobs.txt";
+}
+
+std::map<std::string, int> read_knob_cache() {
+  std::map<std::string, int> m;
+  const std::string path = knob_cache_path();
+  if (path.empty()) return m;
+  std::ifstream f(path);
+  std::string key;
+  int v;
+  while (f >> key >> v)
+    if (v >= 0 && v < int(NUM_KNOB_SETS)) m[key] = v;
+  return m;
+}
+
+void write_knob_cache(const std::map<std::string, int>& add) {
+  const std::string path = knob_cache_path();
+  if (path.empty()) return;
+  std::map<std::string, int> m = read_knob_cache();
+  for (const auto& kv : add) m[kv.first] = kv.second;
+  const size_t slash = path.rfind('/');
+  if (slash != std::string::npos) {
+    std::string dir = path.substr(0, slash), cmd;
+    for (size_t i = 1; i <= dir.size(); ++i)  // mkdir -p, one component at a time
+      if (i == dir.size() || dir[i] == '/') mkdir(dir.substr(0, i).c_str(), 0755);
+  }
+  const std::string tmp = path + ".tmp" + std::to_string(getpid());
+  {
+    std::ofstream f(tmp);
+    for (const auto& kv : m) f << kv.first << " " << kv.second << "\n";
+    if (!f) return;
+  }
+  std::rename(tmp.c_str(), path.c_str());  // a whole file or none
+}
+
+std::mutex g_knob_mu;
+std::map<std::string, int> g_knob_mem;  // this process's choices (and the file's, once read)
+bool g_knob_file_read = false;
+
+// the cache key of size class n: device, register size, and the class's mean
+// folded ops per trajectory on a log2 scale
+std::string knob_key(const std::string& device, uint32_t n, double mean_ops) {
+  std::ostringstream k;
+  k << device << "|n" << n << "|ops2^" << int(std::floor(std::log2(std::max(1.0, mean_ops))));
+  return k.str();
+}
+
+std::string device_tag() {
+  int dev = 0;
+  cudaDeviceProp pr{};
+  if (cudaGetDevice(&dev) != cudaSuccess || cudaGetDeviceProperties(&pr, dev) != cudaSuccess) {
+    cudaGetLastError();
+    return "";
+  }
+  std::string name = pr.name;
+  for (char& ch : name)
+    if (ch == ' ' || ch == '|') ch = '_';
+  return name + "_sm" + std::to_string(pr.multiProcessorCount);
+}
+
+// knob sets found in the cache for every size class of the batch (false: some missing)
+bool knobs_from_cache(ncsim_batch* b, const std::string& dev) {
+  if (dev.empty() || b->ts.empty()) return false;
+  std::map<uint32_t, std::pair<double, uint32_t>> ops;  // n -> (sum ops, count)
+  for (const Trajectory& t : b->ts) ops[t.n].first += double(t.ops.size()), ops[t.n].second += 1;
+  std::lock_guard<std::mutex> lk(g_knob_mu);
+  if (!g_knob_file_read) {
+    for (const auto& kv : read_knob_cache()) g_knob_mem.insert(kv);
+    g_knob_file_read = true;
+  }
+  for (const auto& kv : ops) {
+    auto it = g_knob_mem.find(knob_key(dev, kv.first, kv.second.first / kv.second.second));
+    if (it == g_knob_mem.end()) return false;
+    b->knob_set_by_n[kv.first] = it->second;
+    b->knobs_by_n[kv.first] = knob_set(uint32_t(it->second));
+  }
+  return true;
+}
+
+void set_orders(ncsim_batch* b) {
+  const uint32_t c = b->count();
+  b->order_seq.resize(c);
+  std::iota(b->order_seq.begin(), b->order_seq.end(), 0u);
+  b->order_lpt = b->order_seq;
+  std::stable_sort(b->order_lpt.begin(), b->order_lpt.end(),
+                   [&](uint32_t x, uint32_t y) { return b->prog.traj[x].n > b->prog.traj[y].n; });
+}
+
+void finalize_knobs(ncsim_batch* b) {
+  b->knobs_final = true;
+  std::vector<Trajectory>().swap(b->ts);
+}
+
+// Times every candidate knob set on every size class of the batch (each class's
+// trajectories alone, an evenly strided sample of at most 512, double-buffered
+// at one CTA per SM) and keeps, per class, the fastest; the program is then
+// compiled with the chosen knobs.  Runs on the batch's device.
+void tune_knobs(ncsim_batch* b) {
+  if (b->ts.empty()) return;
+  std::map<uint32_t, std::vector<uint32_t>> cls;
+  std::map<uint32_t, double> ops;
+  for (uint32_t i = 0; i < b->ts.size(); ++i) {
+    cls[b->ts[i].n].push_back(i);
+    ops[b->ts[i].n] += double(b->ts[i].ops.size());
+  }
+  const ncsim_batch_config cf{1, 2, NCSIM_BATCH_ORDER_GIVEN};
+  ensure_slots(b, grid_for(cf));
+  for (uint32_t k = 0; k < NUM_KNOB_SETS; ++k) {
+    b->prog = compile(b->ts, knob_set(k));
+    upload_program(b);
+    for (auto& kv : cls) {
+      const std::vector<uint32_t>& all = kv.second;
+      const size_t m = std::min<size_t>(all.size(), 512);
+      std::vector<uint32_t> pick(m);
+      for (size_t i = 0; i < m; ++i) pick[i] = all[i * all.size() / m];
+      NCSIM_CUDA(cudaMemcpyAsync(b->d_prog + b->off_sample, pick.data(), m * 4, cudaMemcpyHostToDevice, b->stream));
+      double best = 1e300;
+      for (int rep = 0; rep < 2; ++rep) {  // the first is a warm-up
+        enqueue_run(b, cf, b->off_sample, uint32_t(m), false);
+        const double t = finish_run(b);
+        if (rep > 0) best = std::min(best, t);
+      }
+      b->knob_ms[kv.first][k] = best;
+    }
+  }
+  const std::string dev = device_tag();
+  std::map<std::string, int> chosen;
+  for (auto& kv : cls) {
+    const auto& t = b->knob_ms[kv.first];
+    const int best = int(std::min_element(t.begin(), t.end()) - t.begin());
+    b->knob_set_by_n[kv.first] = best;
+    b->knobs_by_n[kv.first] = knob_set(uint32_t(best));
+    if (!dev.empty()) chosen[knob_key(dev, kv.first, ops[kv.first] / double(kv.second.size()))] = best;
+  }
+  b->prog = compile(b->ts, b->knobs_by_n);
+  upload_program(b);
+  {
+    std::lock_guard<std::mutex> lk(g_knob_mu);
+    for (const auto& kv : chosen) g_knob_mem[kv.first] = kv.second;
+  }
+  write_knob_cache(chosen);
+}
+
+// the planner's knobs final: from the cache, else timed (once per batch)
+void ensure_knobs(ncsim_batch* b) {
+  if (b->knobs_final) return;
+  tune_knobs(b);
+  finalize_knobs(b);
+}
+
 void ensure_config(ncsim_batch* b) {
   if (b->cfg.buffers != 0) return;
   const auto key = std::make_tuple(b->device, b->count(), b->prog.max_n);
@@ -923,17 +1118,17 @@ void ensure_config(ncsim_batch* b) {
   g_tuned[key] = b->cfg;
 }
 
+// The program is compiled with the knobs the cache holds for the current
+// device; when it lacks a size class of the batch, the default knobs are used
+// and the trajectories are kept for the autotuner, which runs on first use.
 ncsim_batch* make_batch(std::vector<Trajectory>&& ts) {
   auto* b = new ncsim_batch();
   try {
-    PlanKnobs kn;
-    b->prog = compile(ts, kn);
-    const uint32_t c = b->count();
-    b->order_seq.resize(c);
-    std::iota(b->order_seq.begin(), b->order_seq.end(), 0u);
-    b->order_lpt = b->order_seq;
-    std::stable_sort(b->order_lpt.begin(), b->order_lpt.end(),
-                     [&](uint32_t x, uint32_t y) { return b->prog.traj[x].n > b->prog.traj[y].n; });
+    b->ts = std::move(ts);
+    const bool cached = knobs_from_cache(b, device_tag());
+    b->prog = compile(b->ts, b->knobs_by_n);
+    set_orders(b);
+    if (cached) finalize_knobs(b);
   } catch (...) {
     delete b;
     throw;
@@ -1028,6 +1223,40 @@ ncsim_status ncsim_batch_info(const ncsim_batch* b, ncsim_batch_stats* st) {
   });
 }
 
+ncsim_status ncsim_batch_knobs(const ncsim_batch* b, uint32_t n, ncsim_batch_knobs_info* out) {
+  return guarded([&] {
+    if (!b || !out) throw Error(NCSIM_ERR_INVALID, "null argument");
+    if (n > MAX_QUBITS) throw Error(NCSIM_ERR_INVALID, "register size above 26");
+    const PlanKnobs& k = b->knobs_by_n[n];
+    out->knob_set = uint32_t(b->knob_set_by_n[n]);
+    out->window_step = k.window_step;
+    out->greedy_windows = k.greedy_windows;
+    out->greedy_stages = k.greedy_stages;
+    out->final_ = b->knobs_final;
+    for (uint32_t i = 0; i < 4; ++i) out->timed_ms[i] = i < NUM_KNOB_SETS ? b->knob_ms[n][i] : 0.0;
+  });
+}
+
+ncsim_status ncsim_batch_set_knob_set(ncsim_batch* b, uint32_t n, uint32_t knob_set_index, int32_t final_) {
+  return guarded([&] {
+    if (!b) throw Error(NCSIM_ERR_INVALID, "null batch");
+    if (n > MAX_QUBITS) throw Error(NCSIM_ERR_INVALID, "register size above 26");
+    if (knob_set_index >= NUM_KNOB_SETS) throw Error(NCSIM_ERR_INVALID, "unknown knob set");
+    std::lock_guard<std::mutex> lk(b->mu);
+    if (b->knobs_final) throw Error(NCSIM_ERR_INVALID, "the batch's knobs are final (its trajectories were dropped)");
+    b->knob_set_by_n[n] = int(knob_set_index);
+    b->knobs_by_n[n] = knob_set(knob_set_index);
+    b->prog = compile(b->ts, b->knobs_by_n);
+    if (b->device >= 0) {
+      int cur = 0;
+      NCSIM_CUDA(cudaGetDevice(&cur));
+      if (cur == b->device) upload_program(b);
+      else b->release();
+    }
+    if (final_) finalize_knobs(b);
+  });
+}
+
 ncsim_status ncsim_batch_set_config(ncsim_batch* b, const ncsim_batch_config* cfg) {
   return guarded([&] {
     if (!b || !cfg) throw Error(NCSIM_ERR_INVALID, "null argument");
@@ -1042,6 +1271,7 @@ ncsim_status ncsim_batch_get_config(ncsim_batch* b, ncsim_batch_config* cfg) {
     if (!b || !cfg) throw Error(NCSIM_ERR_INVALID, "null argument");
     std::lock_guard<std::mutex> lk(b->mu);
     ensure_device(b);
+    ensure_knobs(b);
     ensure_config(b);
     *cfg = b->cfg;
   });
@@ -1052,6 +1282,8 @@ ncsim_status ncsim_batch_tune(ncsim_batch* b, uint32_t sample, ncsim_batch_confi
     if (!b) throw Error(NCSIM_ERR_INVALID, "null batch");
     std::lock_guard<std::mutex> lk(b->mu);
     ensure_device(b);
+    if (!b->ts.empty()) tune_knobs(b);  // the planner's knobs too, while the trajectories are kept
+    finalize_knobs(b);
     b->cfg = tune(b, sample);
     {
       std::lock_guard<std::mutex> g(g_tune_mu);
@@ -1066,6 +1298,7 @@ ncsim_status ncsim_batch_run(ncsim_batch* b, double* device_ms) {
     if (!b) throw Error(NCSIM_ERR_INVALID, "null batch");
     std::lock_guard<std::mutex> lk(b->mu);
     ensure_device(b);
+    ensure_knobs(b);
     ensure_config(b);
     ensure_slots(b, grid_for(b->cfg));
     if (!b->graph || !same_cfg(b->graph_cfg, b->cfg)) {

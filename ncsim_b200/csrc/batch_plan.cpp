@@ -255,16 +255,18 @@ Trajectory make_from_circuit(const ncsim_circuit& c, uint64_t seed) {
 
 namespace {
 
-std::vector<std::vector<uint32_t>> windows_for(uint32_t n) {
+std::vector<std::vector<uint32_t>> windows_for(uint32_t n, uint32_t step) {
   std::vector<std::vector<uint32_t>> ws;
-  for (uint32_t g0 = LOW_BITS; g0 < n; g0 += TILE_BITS - LOW_BITS) {
+  step = std::max<uint32_t>(1, step);
+  for (uint32_t g0 = LOW_BITS; g0 < n; g0 += step) {
     std::vector<uint32_t> w;
     for (uint32_t q = 0; q < LOW_BITS; ++q) w.push_back(q);
     for (uint32_t q = g0; q < std::min(n, g0 + TILE_BITS - LOW_BITS); ++q) w.push_back(q);
     for (uint32_t q = n; w.size() < TILE_BITS && q-- > 0;)
       if (std::find(w.begin(), w.end(), q) == w.end()) w.push_back(q);
     std::sort(w.begin(), w.end());
-    ws.push_back(w);
+    if (std::find(ws.begin(), ws.end(), w) == ws.end()) ws.push_back(w);
+    if (g0 + TILE_BITS - LOW_BITS >= n) break;  // the block reached the top qubit
   }
   return ws;
 }
@@ -350,7 +352,7 @@ float f32(double v) { return float(v); }
 
 void compile_one(const Trajectory& t, const PlanKnobs& kn, Local& L) {
   const uint32_t n = t.n;
-  const auto ws = windows_for(n);
+  const auto ws = windows_for(n, kn.window_step);
   std::vector<std::vector<int>> wpos(ws.size(), std::vector<int>(n, -1));
   for (size_t w = 0; w < ws.size(); ++w)
     for (uint32_t b = 0; b < TILE_BITS; ++b) wpos[w][ws[w][b]] = int(b);
@@ -500,13 +502,17 @@ void compile_one(const Trajectory& t, const PlanKnobs& kn, Local& L) {
 }  // namespace
 
 Program compile(const std::vector<Trajectory>& ts, const PlanKnobs& knobs) {
+  return compile(ts, std::vector<PlanKnobs>(MAX_QUBITS + 1, knobs));
+}
+
+Program compile(const std::vector<Trajectory>& ts, const std::vector<PlanKnobs>& knobs_by_n) {
   std::vector<Local> loc(ts.size());
   std::atomic<size_t> next{0};
   std::vector<std::string> errs(ts.size());
   auto work = [&] {
     for (size_t i; (i = next.fetch_add(1)) < ts.size();) {
       try {
-        compile_one(ts[i], knobs, loc[i]);
+        compile_one(ts[i], knobs_by_n.at(ts[i].n), loc[i]);
       } catch (const std::exception& e) {
         errs[i] = e.what();
       }

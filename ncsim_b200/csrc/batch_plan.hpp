@@ -94,11 +94,23 @@ struct Trajectory {
   std::vector<double> draws;   // the nmeas uniforms after the noise draws
 };
 
-// tuning knobs of the host planner
+// tuning knobs of the host planner (chosen per register size by the autotuner)
 struct PlanKnobs {
   bool greedy_windows = true;  // pick the window that takes most ops (else alternate)
   bool greedy_stages = true;   // pick the register set that takes most gates (else cycle)
+  uint32_t window_step = TILE_BITS - LOW_BITS;  // candidate windows: qubits 0..3 and a block of 9
+                                                // consecutive qubits starting every window_step
+                                                // qubits (9: disjoint blocks; less: overlapping)
 };
+constexpr uint32_t NUM_KNOB_SETS = 4;
+// the candidate knob sets the autotuner times (set 0 is the default)
+inline PlanKnobs knob_set(uint32_t i) {
+  PlanKnobs k;
+  if (i == 1) k.window_step = 3;
+  if (i == 2) k.window_step = 5;
+  if (i == 3) k.greedy_stages = false;
+  return k;
+}
 
 // an allocator whose resize leaves trivially constructible elements
 // uninitialised (the program's arrays are filled in parallel after sizing)
@@ -146,6 +158,8 @@ ncsim_batch* batch_random_layers(uint32_t count, uint64_t seed0, uint32_t n_lo, 
                                  double p);
 // compiles trajectories (in parallel) into one program, in the given order
 Program compile(const std::vector<Trajectory>& ts, const PlanKnobs& knobs);
+// with the knobs of each trajectory's register size (indexed by n)
+Program compile(const std::vector<Trajectory>& ts, const std::vector<PlanKnobs>& knobs_by_n);
 
 // FP64 host run of trajectory t of the program in the device's pass, tile,
 // stage and op order, with the device's measurement rule; returns the record

@@ -4,6 +4,7 @@
 #include <algorithm>
 #include <cmath>
 #include <cstring>
+#include <cstdlib>
 #include <map>
 
 namespace ncsim {
@@ -212,6 +213,7 @@ struct PassBuilder {
   int emitted_unitaries = 0;
   size_t term_count = 0;
   CplxD global{1.0, 0.0};
+  bool extend_groups = std::getenv("NCSIM_FUSE_NO_EXTEND") == nullptr;
 
   void emit_group() {
     if (!g.open) return;
@@ -259,6 +261,16 @@ struct PassBuilder {
       // backward: the most recent unitary touching these qubits
       if (g.open && (g.mask & gi.mask)) {
         if ((gi.mask & ~g.mask) == 0) {
+          g.apply_diag(gi.q, gi.d);
+          return true;
+        }
+        // the open group takes the gate's other window qubits along while it has room:
+        // the gate becomes part of the unitary instead of a term that blocks later
+        // gates on those qubits
+        if (extend_groups && (gi.mask & ~window) == 0 && !(gi.mask & pending_mask) &&
+            __builtin_popcountll(g.mask | gi.mask) <= maxk) {
+          for (uint32_t q : gi.q)
+            if (g.local_of(q) < 0) g.add_qubit(q);
           g.apply_diag(gi.q, gi.d);
           return true;
         }
@@ -334,30 +346,62 @@ struct PassBuilder {
 
 // Passes for a run of fusable gates, in dependency order.
 void plan_run(const std::vector<GInfo>& gs, uint32_t n, int maxk, std::vector<Pass>& out, Plan& stats) {
+  static const bool lookahead_windows = std::getenv("NCSIM_FUSE_FIRST_COME") == nullptr;
   std::vector<size_t> remaining(gs.size());
   for (size_t i = 0; i < gs.size(); ++i) remaining[i] = i;
   const uint64_t low = (uint64_t(1) << LOW_BITS) - 1;
+  // the dense gates a fixed window lets through (gates behind a blocked qubit wait)
+  auto dense_through = [&](uint64_t W) {
+    uint64_t blocked = 0;
+    size_t dense = 0;
+    for (size_t i : remaining) {
+      const GInfo& g = gs[i];
+      if (g.mask & blocked) blocked |= g.mask;
+      else if (g.cls == GClass::Diag) continue;
+      else if ((g.mask & ~W) == 0) ++dense;
+      else blocked |= g.mask;
+    }
+    return dense;
+  };
   while (!remaining.empty()) {
-    // choose the window and the gates it can take (gates behind a blocked qubit wait)
+    // the window, first come first served: qubits of the gates in circuit order
     uint64_t W = low, blocked = 0;
+    for (size_t i : remaining) {
+      const GInfo& g = gs[i];
+      if (g.mask & blocked) blocked |= g.mask;
+      else if (g.cls == GClass::Diag) continue;
+      else if (__builtin_popcountll(W | g.mask) <= TILE_BITS) W |= g.mask;
+      else blocked |= g.mask;
+    }
+    for (uint32_t b = 0; b < n && __builtin_popcountll(W) < TILE_BITS; ++b) W |= uint64_t(1) << b;
+    // and a window grown one qubit at a time, each time the qubit that lets the most
+    // dense gates through; the better of the two is taken
+    if (lookahead_windows) {
+      uint64_t G = low;
+      while (__builtin_popcountll(G) < TILE_BITS) {
+        size_t best = 0;
+        uint32_t bq = n;
+        for (uint32_t q = 0; q < n; ++q) {
+          if ((G >> q) & 1) continue;
+          const size_t d = dense_through(G | (uint64_t(1) << q));
+          if (bq == n || d > best) best = d, bq = q;
+        }
+        G |= uint64_t(1) << bq;
+      }
+      if (dense_through(G) > dense_through(W)) W = G;
+    }
+    // the gates the window takes, in order
+    blocked = 0;
     std::vector<size_t> inc, rest;
     for (size_t i : remaining) {
       const GInfo& g = gs[i];
-      if (g.mask & blocked) {
+      if ((g.mask & blocked) || (g.cls != GClass::Diag && (g.mask & ~W))) {
         blocked |= g.mask;
         rest.push_back(i);
-      } else if (g.cls == GClass::Diag) {
-        inc.push_back(i);
-      } else if (__builtin_popcountll(W | g.mask) <= TILE_BITS) {
-        W |= g.mask;
-        inc.push_back(i);
       } else {
-        blocked |= g.mask;
-        rest.push_back(i);
+        inc.push_back(i);
       }
     }
-    // the window: exactly TILE_BITS qubits (filled with the lowest free ones)
-    for (uint32_t b = 0; b < n && __builtin_popcountll(W) < TILE_BITS; ++b) W |= uint64_t(1) << b;
     // fuse; gates past the pass's limits go back (they depend on nothing left behind)
     PassBuilder pb;
     pb.window = W;

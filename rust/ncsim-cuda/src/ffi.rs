@@ -91,6 +91,17 @@ pub struct ncsim_batch_config {
     pub order: u32,
 }
 
+#[repr(C)]
+#[derive(Clone, Copy, Debug, Default)]
+pub struct ncsim_batch_knobs_info {
+    pub knob_set: u32,
+    pub window_step: u32,
+    pub greedy_windows: u32,
+    pub greedy_stages: u32,
+    pub final_: u32,
+    pub timed_ms: [f64; 4],
+}
+
 #[link(name = "ncsim_cuda")]
 extern "C" {
     pub fn ncsim_last_error() -> *const c_char;
@@ -163,6 +174,8 @@ extern "C" {
     pub fn ncsim_batch_release(b: *mut ncsim_batch) -> ncsim_status;
     pub fn ncsim_batch_info(b: *const ncsim_batch, st: *mut ncsim_batch_stats) -> ncsim_status;
     pub fn ncsim_batch_trajectory_qubits(b: *const ncsim_batch, n: *mut u32) -> ncsim_status;
+    pub fn ncsim_batch_knobs(b: *const ncsim_batch, n: u32, out: *mut ncsim_batch_knobs_info) -> ncsim_status;
+    pub fn ncsim_batch_set_knob_set(b: *mut ncsim_batch, n: u32, knob_set: u32, final_: i32) -> ncsim_status;
     pub fn ncsim_batch_set_config(b: *mut ncsim_batch, cfg: *const ncsim_batch_config) -> ncsim_status;
     pub fn ncsim_batch_get_config(b: *mut ncsim_batch, cfg: *mut ncsim_batch_config) -> ncsim_status;
     pub fn ncsim_batch_tune(b: *mut ncsim_batch, sample: u32, best: *mut ncsim_batch_config) -> ncsim_status;

@@ -101,3 +101,22 @@ def test_register_range_refused(nb):
     assert e.value.kind == "Unsupported"
     with pytest.raises(nb.SimError):
         nb.TrajectoryBatch.random_layers(0, 1, 16, 2, 3, 0.0)
+
+
+@pytest.mark.parametrize("knob_set", [1, 2, 3])
+def test_every_knob_set_plans_correct_programs(nb, oracle, knob_set):
+    """The autotuner's candidate planner knob sets (overlapping windows every 3 or
+    5 qubits, cycled stage register sets) give programs with the same results."""
+    b = nb.TrajectoryBatch.random_layers(8, seed0=21, n_lo=15, n_span=4, depth=10, p=0.02)
+    nq = b.qubits()
+    for n in set(int(v) for v in nq):
+        b.set_knob_set(n, knob_set)
+        assert b.knobs(n)["knob_set"] == knob_set
+    for t in range(8):
+        rec, z0, norm = b.emulate(t)
+        n_o, z0_o, rec_o = oracle.trajectory(21 + t, 15, 4, 10, 0.02)
+        assert rec == _bits(rec_o) and abs(z0 - z0_o) < Z0_TOL
+    b.set_knob_set(int(nq[0]), 0, final=True)
+    assert b.knobs(int(nq[0]))["final"]
+    with pytest.raises(nb.SimError):
+        b.set_knob_set(int(nq[0]), 1)  # final: the trajectories were dropped

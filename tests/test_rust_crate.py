@@ -46,7 +46,7 @@ def test_structs_mirror_the_header():
     hdr = _header()
     src = open(os.path.join(CRATE, "src", "ffi.rs")).read()
     for name in ("ncsim_error_info", "ncsim_kernel_stat", "ncsim_fused_stats", "ncsim_batch_stats",
-                 "ncsim_batch_config"):
+                 "ncsim_batch_config", "ncsim_batch_knobs_info"):
         body = re.search(r"typedef struct %s \{(.*?)\} %s;" % (name, name), hdr, flags=re.S).group(1)
         c_fields = re.findall(r"(\w+)(?:\[\d+\])?;", body)
         rbody = re.search(r"pub struct %s \{(.*?)\}" % name, src, flags=re.S).group(1)
