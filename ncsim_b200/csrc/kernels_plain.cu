@@ -694,22 +694,30 @@ __device__ __forceinline__ void block_store(double (&acc)[SLOTS], double* partia
   }
 }
 
+// The reductions keep several independent loads in flight per thread (UNROLL
+// grid-stride steps per iteration, all loads before any arithmetic), so that
+// the 2 x 512 threads of an SM hold enough bytes in flight to stream HBM.
+constexpr int UNROLL = 4;
+
+template <class R>
+__device__ __forceinline__ V<R> load_or_zero(const V<R>* a, uint64_t i, uint64_t len) {
+  V<R> v;
+  v.x = v.y = R(0);
+  if (i < len) v = a[i];
+  return v;
+}
+
 template <class R>
 __global__ void __launch_bounds__(REDUCE_THREADS) k_norm(const V<R>* __restrict__ a, uint64_t len, double* partials) {
   double acc[1] = {0.0};
   const uint64_t stride = uint64_t(gridDim.x) * blockDim.x;
-  uint64_t i = uint64_t(blockIdx.x) * blockDim.x + threadIdx.x;
-  double acc2 = 0.0;
-  for (; i + stride < len; i += 2 * stride) {
-    V<R> v = a[i], w = a[i + stride];
-    acc[0] += double(v.x) * double(v.x) + double(v.y) * double(v.y);
-    acc2 += double(w.x) * double(w.x) + double(w.y) * double(w.y);
+  for (uint64_t i0 = uint64_t(blockIdx.x) * blockDim.x + threadIdx.x; i0 < len; i0 += UNROLL * stride) {
+    V<R> v[UNROLL];
+#pragma unroll
+    for (int u = 0; u < UNROLL; ++u) v[u] = load_or_zero<R>(a, i0 + u * stride, len);
+#pragma unroll
+    for (int u = 0; u < UNROLL; ++u) acc[0] += double(v[u].x) * double(v[u].x) + double(v[u].y) * double(v[u].y);
   }
-  if (i < len) {
-    V<R> v = a[i];
-    acc[0] += double(v.x) * double(v.x) + double(v.y) * double(v.y);
-  }
-  acc[0] += acc2;
   block_store<1>(acc, partials);
 }
 
@@ -720,14 +728,20 @@ __global__ void __launch_bounds__(REDUCE_THREADS) k_expect_diag(const V<R>* __re
   // sum_c i^{k(c)} |psi(c)|^2
   double acc[3] = {0.0, 0.0, 0.0};
   const uint64_t stride = uint64_t(gridDim.x) * blockDim.x;
-  for (uint64_t c = uint64_t(blockIdx.x) * blockDim.x + threadIdx.x; c < len; c += stride) {
-    V<R> v = a[c];
-    double w = double(v.x) * double(v.x) + double(v.y) * double(v.y);
-    int k = (ph + 2 * __popcll(z & c)) & 3;
-    double sgn = (k & 2) ? -1.0 : 1.0;
-    if (k & 1) acc[1] += sgn * w;
-    else acc[0] += sgn * w;
-    if (NORM) acc[2] += w;
+  for (uint64_t c0 = uint64_t(blockIdx.x) * blockDim.x + threadIdx.x; c0 < len; c0 += UNROLL * stride) {
+    V<R> v[UNROLL];
+#pragma unroll
+    for (int u = 0; u < UNROLL; ++u) v[u] = load_or_zero<R>(a, c0 + u * stride, len);
+#pragma unroll
+    for (int u = 0; u < UNROLL; ++u) {
+      const uint64_t c = c0 + u * stride;
+      const double w = double(v[u].x) * double(v[u].x) + double(v[u].y) * double(v[u].y);
+      const int k = (ph + 2 * __popcll(z & c)) & 3;
+      const double sw = (k & 2) ? -w : w;
+      if (k & 1) acc[1] += sw;
+      else acc[0] += sw;
+      if (NORM) acc[2] += w;
+    }
   }
   block_store<3>(acc, partials);
 }
@@ -738,17 +752,31 @@ __global__ void __launch_bounds__(REDUCE_THREADS) k_expect_pair(const V<R>* __re
   double acc[3] = {0.0, 0.0, 0.0};
   const uint64_t stride = uint64_t(gridDim.x) * blockDim.x;
   const uint64_t lo = (uint64_t(1) << h) - 1;
-  for (uint64_t p = uint64_t(blockIdx.x) * blockDim.x + threadIdx.x; p < npairs; p += stride) {
-    uint64_t c = ((p & ~lo) << 1) | (p & lo);
-    uint64_t d = c ^ x;
-    V<R> vc = a[c], vd = a[d];
-    double2 C = make_double2(vc.x, vc.y), D = make_double2(vd.x, vd.y);
-    // conj(psi(d)) i^{k(c)} psi(c) + conj(psi(c)) i^{k(d)} psi(d)
-    double2 t1 = ipow_mul((ph + 2 * __popcll(z & c)) & 3, C);
-    double2 t2 = ipow_mul((ph + 2 * __popcll(z & d)) & 3, D);
-    acc[0] += D.x * t1.x + D.y * t1.y + C.x * t2.x + C.y * t2.y;
-    acc[1] += D.x * t1.y - D.y * t1.x + C.x * t2.y - C.y * t2.x;
-    if (NORM) acc[2] += C.x * C.x + C.y * C.y + D.x * D.x + D.y * D.y;
+  for (uint64_t p0 = uint64_t(blockIdx.x) * blockDim.x + threadIdx.x; p0 < npairs; p0 += UNROLL * stride) {
+    V<R> vc[UNROLL], vd[UNROLL];
+#pragma unroll
+    for (int u = 0; u < UNROLL; ++u) {
+      const uint64_t p = p0 + u * stride;
+      const uint64_t c = ((p & ~lo) << 1) | (p & lo);
+      vc[u].x = vc[u].y = vd[u].x = vd[u].y = R(0);  // past the end: zeros add nothing
+      if (p < npairs) {
+        vc[u] = a[c];
+        vd[u] = a[c ^ x];
+      }
+    }
+#pragma unroll
+    for (int u = 0; u < UNROLL; ++u) {
+      const uint64_t p = p0 + u * stride;
+      const uint64_t c = ((p & ~lo) << 1) | (p & lo);
+      const uint64_t d = c ^ x;
+      double2 C = make_double2(vc[u].x, vc[u].y), D = make_double2(vd[u].x, vd[u].y);
+      // conj(psi(d)) i^{k(c)} psi(c) + conj(psi(c)) i^{k(d)} psi(d)
+      double2 t1 = ipow_mul((ph + 2 * __popcll(z & c)) & 3, C);
+      double2 t2 = ipow_mul((ph + 2 * __popcll(z & d)) & 3, D);
+      acc[0] += D.x * t1.x + D.y * t1.y + C.x * t2.x + C.y * t2.y;
+      acc[1] += D.x * t1.y - D.y * t1.x + C.x * t2.y - C.y * t2.x;
+      if (NORM) acc[2] += C.x * C.x + C.y * C.y + D.x * D.x + D.y * D.y;
+    }
   }
   block_store<3>(acc, partials);
 }
@@ -758,10 +786,18 @@ __global__ void __launch_bounds__(REDUCE_THREADS) k_inner(const V<R>* __restrict
                                                           double* partials) {
   double acc[2] = {0.0, 0.0};
   const uint64_t stride = uint64_t(gridDim.x) * blockDim.x;
-  for (uint64_t i = uint64_t(blockIdx.x) * blockDim.x + threadIdx.x; i < len; i += stride) {
-    V<R> u = a[i], v = b[i];
-    acc[0] += double(u.x) * double(v.x) + double(u.y) * double(v.y);
-    acc[1] += double(u.x) * double(v.y) - double(u.y) * double(v.x);
+  for (uint64_t i0 = uint64_t(blockIdx.x) * blockDim.x + threadIdx.x; i0 < len; i0 += UNROLL * stride) {
+    V<R> u[UNROLL], v[UNROLL];
+#pragma unroll
+    for (int k = 0; k < UNROLL; ++k) {
+      u[k] = load_or_zero<R>(a, i0 + k * stride, len);
+      v[k] = load_or_zero<R>(b, i0 + k * stride, len);
+    }
+#pragma unroll
+    for (int k = 0; k < UNROLL; ++k) {
+      acc[0] += double(u[k].x) * double(v[k].x) + double(u[k].y) * double(v[k].y);
+      acc[1] += double(u[k].x) * double(v[k].y) - double(u[k].y) * double(v[k].x);
+    }
   }
   block_store<2>(acc, partials);
 }
@@ -802,15 +838,21 @@ __global__ void __launch_bounds__(REDUCE_THREADS) k_project_diag(V<R>* __restric
                                                                  double* partials) {
   double acc[1] = {0.0};
   const uint64_t stride = uint64_t(gridDim.x) * blockDim.x;
-  for (uint64_t c = uint64_t(blockIdx.x) * blockDim.x + threadIdx.x; c < len; c += stride) {
-    V<R> v = a[c];
-    if (is_zero(v)) continue;
-    int k = (ph + 2 * __popcll(z & c) + (outcome ? 2 : 0)) & 3;
-    V<R> nv = ipow_mul(k, v);
-    nv.x = (v.x + nv.x) * R(0.5);
-    nv.y = (v.y + nv.y) * R(0.5);
-    if (nv.x != v.x || nv.y != v.y) a[c] = nv;
-    acc[0] += double(nv.x) * double(nv.x) + double(nv.y) * double(nv.y);
+  for (uint64_t c0 = uint64_t(blockIdx.x) * blockDim.x + threadIdx.x; c0 < len; c0 += UNROLL * stride) {
+    V<R> v[UNROLL];
+#pragma unroll
+    for (int u = 0; u < UNROLL; ++u) v[u] = load_or_zero<R>(a, c0 + u * stride, len);
+#pragma unroll
+    for (int u = 0; u < UNROLL; ++u) {
+      const uint64_t c = c0 + u * stride;
+      if (is_zero(v[u])) continue;  // (also every index past the end)
+      const int k = (ph + 2 * __popcll(z & c) + (outcome ? 2 : 0)) & 3;
+      V<R> nv = ipow_mul(k, v[u]);
+      nv.x = (v[u].x + nv.x) * R(0.5);
+      nv.y = (v[u].y + nv.y) * R(0.5);
+      if (nv.x != v[u].x || nv.y != v[u].y) a[c] = nv;
+      acc[0] += double(nv.x) * double(nv.x) + double(nv.y) * double(nv.y);
+    }
   }
   block_store<1>(acc, partials);
 }
@@ -822,21 +864,36 @@ __global__ void __launch_bounds__(REDUCE_THREADS) k_project_pair(V<R>* __restric
   const uint64_t stride = uint64_t(gridDim.x) * blockDim.x;
   const uint64_t lo = (uint64_t(1) << h) - 1;
   const int so = outcome ? 2 : 0;
-  for (uint64_t p = uint64_t(blockIdx.x) * blockDim.x + threadIdx.x; p < npairs; p += stride) {
-    uint64_t c = ((p & ~lo) << 1) | (p & lo);
-    uint64_t d = c ^ x;
-    V<R> vc = a[c], vd = a[d];
-    V<R> tc = ipow_mul((ph + 2 * __popcll(z & d) + so) & 3, vd);
-    V<R> td = ipow_mul((ph + 2 * __popcll(z & c) + so) & 3, vc);
-    V<R> nc, nd;
-    nc.x = (vc.x + tc.x) * R(0.5);
-    nc.y = (vc.y + tc.y) * R(0.5);
-    nd.x = (vd.x + td.x) * R(0.5);
-    nd.y = (vd.y + td.y) * R(0.5);
-    a[c] = nc;
-    a[d] = nd;
-    acc[0] += double(nc.x) * double(nc.x) + double(nc.y) * double(nc.y) + double(nd.x) * double(nd.x) +
-              double(nd.y) * double(nd.y);
+  for (uint64_t p0 = uint64_t(blockIdx.x) * blockDim.x + threadIdx.x; p0 < npairs; p0 += UNROLL * stride) {
+    V<R> vc[UNROLL], vd[UNROLL];
+#pragma unroll
+    for (int u = 0; u < UNROLL; ++u) {
+      const uint64_t p = p0 + u * stride;
+      const uint64_t c = ((p & ~lo) << 1) | (p & lo);
+      vc[u].x = vc[u].y = vd[u].x = vd[u].y = R(0);
+      if (p < npairs) {
+        vc[u] = a[c];
+        vd[u] = a[c ^ x];
+      }
+    }
+#pragma unroll
+    for (int u = 0; u < UNROLL; ++u) {
+      const uint64_t p = p0 + u * stride;
+      if (p >= npairs) break;
+      const uint64_t c = ((p & ~lo) << 1) | (p & lo);
+      const uint64_t d = c ^ x;
+      V<R> tc = ipow_mul((ph + 2 * __popcll(z & d) + so) & 3, vd[u]);
+      V<R> td = ipow_mul((ph + 2 * __popcll(z & c) + so) & 3, vc[u]);
+      V<R> nc, nd;
+      nc.x = (vc[u].x + tc.x) * R(0.5);
+      nc.y = (vc[u].y + tc.y) * R(0.5);
+      nd.x = (vd[u].x + td.x) * R(0.5);
+      nd.y = (vd[u].y + td.y) * R(0.5);
+      a[c] = nc;
+      a[d] = nd;
+      acc[0] += double(nc.x) * double(nc.x) + double(nc.y) * double(nc.y) + double(nd.x) * double(nd.x) +
+                double(nd.y) * double(nd.y);
+    }
   }
   block_store<1>(acc, partials);
 }
