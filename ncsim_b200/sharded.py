@@ -95,7 +95,7 @@ class GpuShard:
         import torch
 
         self.s.synchronize()
-        out = self._half_view(l, c).contiguous()
+        out = self._half_view(l, c).contiguous().view(-1)
         torch.cuda.synchronize()
         return out
 
