@@ -3,10 +3,11 @@
 // A persistent CTA per SM streams tiles of 2^12 complex64 amplitudes (32 KB)
 // through shared memory: two producer warps copy 16-byte chunks with cp.async
 // (completion on the tile's mbarrier through cp.async.mbarrier.arrive) into
-// five rotating tile buffers and write finished tiles back with 16-byte
-// stores.  The CTA takes its tiles in sets of four, and four warpgroups run
-// the pass's program, one on each tile of a set, so that a group splits
-// amplitudes while the others' MMAs and read-backs run.  The unitaries' B
+// five rotating tile buffers.  The CTA takes its tiles in sets of four, and
+// four warpgroups run the pass's program, one on each tile of a set, so that a
+// group splits amplitudes while the others' MMAs and read-backs run; each group
+// writes its finished tile back itself (16-byte stores), so the stores overlap
+// the other groups' work and the producers only load.  The unitaries' B
 // operands (16 KB bf16 images each) stream from L2 into three rotating slots
 // (a third producer warp); each group's tcgen05.commit (or release) frees a
 // slot.  Per group and tile:
@@ -176,8 +177,7 @@ __device__ __forceinline__ void cp_async16(uint32_t dst, const void* src) {
 __device__ __forceinline__ void cp_async_arrive(uint32_t bar) {
   asm volatile("cp.async.mbarrier.arrive.noinc.shared::cta.b64 [%0];" ::"r"(bar) : "memory");
 }
-constexpr int BAR_TILES = 1 + GROUPS;  // named barriers: 1..GROUPS the groups, then the tile threads
-__device__ __forceinline__ void bar_tiles() { asm volatile("bar.sync %0, %1;" ::"n"(BAR_TILES), "n"(TILE_THREADS) : "memory"); }
+constexpr int BAR_TILES = 1 + GROUPS;  // named barriers: 1..GROUPS the groups, then the tile loaders
 // A named barrier that also ORs a flag over its threads: every thread gets the
 // same answer, so a stop decided from it is uniform across the barrier's threads.
 __device__ __forceinline__ bool bar_any(int id, int count, bool v) {
@@ -414,21 +414,14 @@ __global__ void __launch_bounds__(THREADS, 1) k_fused_pass(const __grid_constant
   auto have = [&](uint64_t it) { return tile_of(it) < P.ntiles; };
   float2* tiles = reinterpret_cast<float2*>(smem + SM_TILE0);
   auto at = [&](uint32_t e) { return e ^ uint32_t(swz[e >> 4]); };  // stored position of tile element e
+  const uint32_t cshift = uint32_t(P.wl) - 1u;  // 16-byte chunks of 2 amplitudes per run: 2^(wl-1)
+  auto chunk_addr = [&](uint64_t base, uint32_t c) {
+    return P.amp + (base | run_off[c >> cshift]) + 2u * (c & ((1u << cshift) - 1u));
+  };
 
   if (warp == WARP_TILES || warp == WARP_TILES + 1) {
-    // ---------------- tile loads (cp.async) and stores: 64 threads, 16-byte chunks ----------------
+    // ---------------- tile loads (cp.async): 64 threads, 16-byte chunks ----------------
     const int pt = tid - COMPUTE_THREADS;
-    const uint32_t cshift = uint32_t(P.wl) - 1u;  // chunks of 2 amplitudes per run: 2^(wl-1)
-    auto chunk_addr = [&](uint64_t base, uint32_t c) {
-      return P.amp + (base | run_off[c >> cshift]) + 2u * (c & ((1u << cshift) - 1u));
-    };
-    auto store_tile = [&](uint64_t j) {  // smem reads are synchronous: the buffer is free afterwards
-      const uint64_t base = tile_base(tile_of(j), P);
-      const float4* buf = reinterpret_cast<const float4*>(tiles + size_t(j % NTILEBUF) * TILE);
-#pragma unroll 4
-      for (uint32_t c = uint32_t(pt); c < uint32_t(TILE) / 2; c += TILE_THREADS)
-        *reinterpret_cast<float4*>(chunk_addr(base, c)) = buf[at(2u * c) >> 1];
-    };
     auto load_tile = [&](uint64_t it) {
       const int b = int(it % NTILEBUF);
       const uint64_t base = tile_base(tile_of(it), P);
@@ -437,25 +430,14 @@ __global__ void __launch_bounds__(THREADS, 1) k_fused_pass(const __grid_constant
       for (uint32_t c = uint32_t(pt); c < uint32_t(TILE) / 2; c += TILE_THREADS) cp_async16(dst + 8u * at(2u * c), chunk_addr(base, c));
       cp_async_arrive(bar_tfull(b));
     };
-    // wait (one thread) until the group is done with tile j; false (for all 64 threads alike) to stop
+    // wait (one thread) until the group has written tile j back; false (for all 64 threads alike) to stop
     auto wait_done = [&](uint64_t j) -> bool {
       if (pt == 0 && have(j) && !mbar_wait(bar_tdone(int(j % NTILEBUF)), uint32_t((j / NTILEBUF) & 1))) fail(3);
       return !bar_any(BAR_TILES, TILE_THREADS, abort_sh);
     };
-    uint64_t it = 0;
-    for (; it < my_tiles; ++it) {
-      if (it >= NTILEBUF) {
-        if (!wait_done(it - NTILEBUF)) break;
-        if (have(it - NTILEBUF)) store_tile(it - NTILEBUF);
-        bar_tiles();  // every thread has read the buffer before anyone refills it
-      }
+    for (uint64_t it = 0; it < my_tiles; ++it) {
+      if (it >= NTILEBUF && !wait_done(it - NTILEBUF)) break;  // the buffer is free once its tile is written back
       if (have(it)) load_tile(it);
-    }
-    if (it == my_tiles) {
-      for (uint64_t j = my_tiles >= NTILEBUF ? my_tiles - NTILEBUF : 0; j < my_tiles; ++j) {
-        if (!wait_done(j)) break;
-        if (have(j)) store_tile(j);
-      }
     }
     // copies of this thread still in flight land before the CTA exits
     asm volatile("cp.async.wait_all;" ::: "memory");
@@ -688,7 +670,15 @@ __global__ void __launch_bounds__(THREADS, 1) k_fused_pass(const __grid_constant
         if (bar_any(1 + g, GROUP_THREADS, abort_sh)) break;
       }
       if (bar_any(1 + g, GROUP_THREADS, abort_sh)) break;
-      if (mine) mbar_arrive(bar_tdone(b));
+      if (mine) {
+        // the group writes its tile back; each thread's shared-memory reads are done once its
+        // stores are issued, so the buffer is free for the next load after every thread arrives
+        const float4* buf = reinterpret_cast<const float4*>(T);
+#pragma unroll 4
+        for (uint32_t c = uint32_t(tg); c < uint32_t(TILE) / 2; c += GROUP_THREADS)
+          *reinterpret_cast<float4*>(chunk_addr(base, c)) = buf[at(2u * c) >> 1];
+        mbar_arrive(bar_tdone(b));
+      }
     }
   }
   tc_fence_before();

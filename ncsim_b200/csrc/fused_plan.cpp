@@ -4,7 +4,6 @@
 #include <algorithm>
 #include <cmath>
 #include <cstring>
-#include <cstdlib>
 #include <map>
 
 namespace ncsim {
@@ -213,7 +212,6 @@ struct PassBuilder {
   int emitted_unitaries = 0;
   size_t term_count = 0;
   CplxD global{1.0, 0.0};
-  bool extend_groups = std::getenv("NCSIM_FUSE_NO_EXTEND") == nullptr;
 
   void emit_group() {
     if (!g.open) return;
@@ -267,7 +265,7 @@ struct PassBuilder {
         // the open group takes the gate's other window qubits along while it has room:
         // the gate becomes part of the unitary instead of a term that blocks later
         // gates on those qubits
-        if (extend_groups && (gi.mask & ~window) == 0 && !(gi.mask & pending_mask) &&
+        if ((gi.mask & ~window) == 0 && !(gi.mask & pending_mask) &&
             __builtin_popcountll(g.mask | gi.mask) <= maxk) {
           for (uint32_t q : gi.q)
             if (g.local_of(q) < 0) g.add_qubit(q);
@@ -345,8 +343,11 @@ struct PassBuilder {
 };
 
 // Passes for a run of fusable gates, in dependency order.
-void plan_run(const std::vector<GInfo>& gs, uint32_t n, int maxk, std::vector<Pass>& out, Plan& stats) {
-  static const bool lookahead_windows = std::getenv("NCSIM_FUSE_FIRST_COME") == nullptr;
+// lookahead: each pass's window may also be grown qubit by qubit (the one that
+// lets the most dense gates through), keeping it when it lets more through than
+// the first-come window.
+void plan_run(const std::vector<GInfo>& gs, uint32_t n, int maxk, bool lookahead_windows, std::vector<Pass>& out,
+              Plan& stats) {
   std::vector<size_t> remaining(gs.size());
   for (size_t i = 0; i < gs.size(); ++i) remaining[i] = i;
   const uint64_t low = (uint64_t(1) << LOW_BITS) - 1;
@@ -432,7 +433,21 @@ Plan make_plan(const ncsim_circuit& c, uint32_t max_fuse) {
     if (run.empty()) return;
     Segment s;
     s.fused = true;
-    plan_run(run, c.n, maxk, s.passes, p);
+    // Both window rules, and the cheaper plan by the pass kernel's measured cost:
+    // a pass costs about as much as 1.36 unitaries (its streaming), so fewer passes
+    // win only when they do not add more unitaries than that.
+    Plan pa, pb;
+    std::vector<Pass> a, b;
+    plan_run(run, c.n, maxk, false, a, pa);
+    plan_run(run, c.n, maxk, true, b, pb);
+    auto cost = [](const std::vector<Pass>& v, const Plan& st) {
+      return 1.36 * double(v.size()) + double(st.unitaries) + 1e-4 * double(st.terms);
+    };
+    const bool take_b = cost(b, pb) < cost(a, pa);
+    s.passes = take_b ? std::move(b) : std::move(a);
+    const Plan& ps = take_b ? pb : pa;
+    p.unitaries += ps.unitaries;
+    p.terms += ps.terms;
     p.passes += s.passes.size();
     p.segments.push_back(std::move(s));
     run.clear();
