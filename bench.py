@@ -461,6 +461,104 @@ def trajectory_bench(nb, args, dist, peak, peak_kind):
     return out
 
 
+FRAMES_PUBLISHED_MS = 31.0  # the reference's README: 100 000 shots of this circuit on a 16-thread desktop
+
+
+def frames_bench(nb, args, dist, peak, peak_kind):
+    """The reference's frame-sampler benchmark (examples/bench.rs:264-294):
+    1000 qubits, 20 rounds of 500 CX + DEPOLARIZE2(1e-3) and 100 Z
+    measurements (10 500 gates, 2000 measurements), 100 000 shots per step.
+    A step is one sample_packed call: the host scan of the seven batches'
+    random streams (noise hits, mask positions), their upload, the mask and
+    frame kernels; the packed records stay on the device for `value` and come
+    back to host memory for `e2e`.  The reference record (FrameSampler::new)
+    is built once, outside the timed region, as the reference times it apart."""
+    import numpy as np
+    import torch
+
+    shots = 100_000
+    c = nb.Circuit.frames_workload(1000, 20, 100, 1e-3, 9)
+    t0 = time.perf_counter()
+    f = nb.FrameSampler(c, 0)
+    new_s = time.perf_counter() - t0
+    words = f.words(shots)
+    d_out = torch.empty(f.m * words, dtype=torch.int64, device="cuda")
+    rng = nb.StdRng(9 + RANK)
+
+    def seeds():
+        return [rng.next_u64() for _ in range((shots + f.BATCH - 1) // f.BATCH)]
+
+    for _ in range(args.warmup):
+        f.sample_packed_device(shots, seeds(), d_out.data_ptr(), d_out.numel())
+    barrier(dist)
+    kern, wall = [], []
+    for _ in range(args.steps):
+        sd = seeds()
+        torch.cuda.synchronize()
+        t1 = time.perf_counter()
+        f.sample_packed_device(shots, sd, d_out.data_ptr(), d_out.numel())
+        torch.cuda.synchronize()
+        wall.append(time.perf_counter() - t1)
+        kern.append(f.last_kernel_ms())
+    ms = max_over_ranks(dist, 1e3 * statistics.mean(wall))
+    kms = max_over_ranks(dist, statistics.mean(kern))
+    masks = 1000 + 2000  # initial randomisations, then one per measurement
+    alg = (masks + f.m) * words * 8  # masks written and read once, records written once
+    out = {
+        "metric": "shots/s",
+        "value": WORLD * shots / (ms / 1e3),
+        "unit": "shots/s",
+        "ms_per_step": ms,
+        "kernel_ms_per_step": kms,
+        "published_ms": FRAMES_PUBLISHED_MS,
+        "vs_published": round(FRAMES_PUBLISHED_MS / ms, 2),
+        "config": {"workload": "frame-sampler benchmark: n=1000, 20 rounds x (500 CX + DEPOLARIZE2(0.001), 100 M), "
+                               "10500 gates, 2000 measurements, 100000 shots (7 batches of 16384)",
+                   "layers": f.num_layers, "reference_record_s": round(new_s, 3)},
+        "roofline": {"bound": "hbm", "kernel": "k_frame_masks + k_frame_run",
+                     "achieved": round(alg / (kms / 1e3) / 1e9, 1), "peak": peak, "unit": "GB/s",
+                     "frac": round(alg / (kms / 1e3) / 1e9 / peak, 4), "peak_kind": peak_kind,
+                     "algorithmic_bytes_per_launch": alg,
+                     "note": "frames live in shared memory; HBM carries only the masks and records, so the "
+                             "kernels are bound by their dependency layers, not by HBM"},
+        "gpu_launches_per_step": 2,
+    }
+    if not args.no_e2e:
+        host = np.zeros((f.m, words), dtype=np.uint64)
+        f.sample_packed_seeds(shots, seeds(), out=host)
+        barrier(dist)
+        t1 = time.perf_counter()
+        e2e_steps = max(1, min(args.steps, 3))
+        for _ in range(e2e_steps):
+            f.sample_packed_seeds(shots, seeds(), out=host)
+        dt = max_over_ranks(dist, time.perf_counter() - t1)
+        out["e2e"] = {"value": WORLD * e2e_steps * shots / dt, "unit": "shots/s", "h2d_bytes_per_step": None,
+                      "d2h_bytes_per_step": host.nbytes,
+                      "note": "per step: the same call with the packed records copied to host memory; "
+                              "host wall clock"}
+    if RANK == 0 and WORLD == 1 and not args.no_cpu_baseline:
+        out["cpu_baseline"] = cpu_frames(c.to_text(), f.reference(), shots)
+        out["vs_cpu"] = round(out["cpu_baseline"]["value"] and out["value"] / out["cpu_baseline"]["value"], 1)
+    return out
+
+
+def cpu_frames(text: str, reference, shots: int, reps: int = 2):
+    """The oracle's restatement of frame.rs on the host cores, the same workload."""
+    from oracle import oracle as O
+
+    threads = max(1, min(os.cpu_count() or 1, 64))
+    r = O.StdRng(9)
+    times = []
+    for _ in range(reps):
+        seeds = [r.next_u64() for _ in range((shots + (1 << 14) - 1) >> 14)]
+        t0 = time.perf_counter()
+        O.frame_sample_packed(text, reference, shots, seeds, threads=threads)
+        times.append(time.perf_counter() - t0)
+    t = min(times)
+    return {"value": shots / t, "unit": "shots/s", "cores": min(threads, (shots + (1 << 14) - 1) >> 14),
+            "kind": "port", "sample": f"{shots} shots of the frame benchmark, {reps} runs, best"}
+
+
 def config_rates(nb, peak, peak_kind):
     """The other sized workloads of the path, plain complex128 kernels, one GPU:
     C0 (n = 20, depth 40, with its readouts), C1 (n = 30, depth 20, M on the
@@ -636,6 +734,8 @@ def main():
     ap.add_argument("--traj-launch", default="",
                     help="CTAS_PER_SM,BUFFERS: a fixed launch configuration of the batch kernel (default: tuned)")
     ap.add_argument("--no-configs", action="store_true", help="skip the C0, C1 and C3 plain-path rates")
+    ap.add_argument("--no-frames", action="store_true", help="skip the frame-sampler benchmark")
+    ap.add_argument("--frames-only", action="store_true", help="only the frame-sampler benchmark")
     ap.add_argument("--no-headline", action="store_true",
                     help="only the trajectories/s part (for profiling the batch kernel)")
     args = ap.parse_args()
@@ -649,6 +749,17 @@ def main():
     dist = dist_init()
     seed = 1 + RANK
     peak, peak_kind = measured_peaks()
+
+    if args.frames_only:
+        with ClockSampler() as fclk:
+            fr = frames_bench(nb, args, dist, peak, peak_kind)
+        fr["clocks"] = fclk.summary()
+        if RANK == 0:
+            print(json.dumps({"metric": METRIC, "n_gpus": WORLD, "frames": fr}), flush=True)
+        if dist is not None:
+            dist.barrier()
+            dist.destroy_process_group()
+        return 0
 
     if args.no_headline:
         with ClockSampler() as tclk:
@@ -798,6 +909,11 @@ def main():
             head["traj_mean_z0_error"] = acc["mean_z0_error"]
     if not args.no_configs and WORLD == 1:
         result["configs"] = config_rates(nb, peak, peak_kind)
+    if not args.no_frames:
+        with ClockSampler() as fclk:
+            result["frames"] = frames_bench(nb, args, dist, peak, peak_kind)
+        result["frames"]["clocks"] = fclk.summary()
+        head["frames_shots_per_s"] = round(result["frames"]["value"], 1)
 
     clocks = clk.summary() if clk else None
     line = {

@@ -17,7 +17,9 @@
  *      Rust toolchain, and the two GPU-only forms (fused precision form,
  *      batched trajectories);
  *   3. the sparse form: SparseVector<C64> (src/state/sparse.rs) with its
- *      entries in device memory.
+ *      entries in device memory;
+ *   4. the Pauli-frame sampler (FrameSampler, src/frame.rs) for noisy
+ *      Clifford circuits of up to 2^24 qubits.
  * The seeded synthetic workloads of the benchmark and the tests are not part
  * of this interface: they live in libncsim_workloads.so (ncsim_workloads.h).
  *
@@ -465,6 +467,53 @@ ncsim_status ncsim_sparse_run(ncsim_sparse* s, const ncsim_circuit* c, ncsim_rng
 ncsim_status ncsim_sparse_synchronize(const ncsim_sparse* s);
 ncsim_status ncsim_sparse_timer_start(ncsim_sparse* s);
 ncsim_status ncsim_sparse_timer_stop(ncsim_sparse* s, double* milliseconds);
+
+/* ---- Pauli-frame sampler: FrameSampler (src/frame.rs:34-300) on the device ----
+ * Circuits of any width up to 2^24 qubits; every gate Clifford.  Shots run in
+ * batches of 16384 (frame.rs:31), each with its own StdRng seeded by one u64
+ * drawn from the caller's generator per batch, in order (frame.rs:72-74).
+ * Packed outputs: measurement (detector, observable) k's bits over the shots
+ * are nwords = ceil(shots / 64) words at out[k * nwords] (bit s of word
+ * s / 64 = shot s).  The sampler keeps its device buffers on the device that
+ * is current at its first sample call. */
+typedef struct ncsim_frames ncsim_frames;
+/* FrameSampler::new (frame.rs:41-60): NCSIM_ERR_UNSUPPORTED for a non-Clifford
+ * gate; the reference record of the noiseless circuit, random outcomes drawn
+ * from StdRng::seed_from_u64(reference_seed) as the stabilizer tableau draws
+ * them (stabilizer.rs:591). */
+ncsim_status ncsim_frames_new(const ncsim_circuit* c, uint64_t reference_seed, ncsim_frames** out);
+/* The same with a reference record given by the caller (m = the circuit's
+ * measurements, one byte 0/1 each), e.g. ncsim's own FrameSampler::reference(). */
+ncsim_status ncsim_frames_with_reference(const ncsim_circuit* c, const uint8_t* reference, uint64_t m,
+                                         ncsim_frames** out);
+ncsim_status ncsim_frames_free(ncsim_frames* f);
+/* num_measurements, detectors() and observables() counts (circuit.rs:297-327),
+ * and the dependency layers of the device program. */
+ncsim_status ncsim_frames_info(const ncsim_frames* f, uint32_t* num_qubits, uint64_t* num_measurements,
+                               uint64_t* num_detectors, uint64_t* num_observables, uint64_t* num_layers);
+/* FrameSampler::reference (frame.rs:66-68): cap >= num_measurements bytes. */
+ncsim_status ncsim_frames_reference(const ncsim_frames* f, uint8_t* out, uint64_t cap);
+/* sample_packed (frame.rs:69-89) into host memory: cap >= num_measurements * nwords. */
+ncsim_status ncsim_frames_sample_packed(ncsim_frames* f, uint64_t shots, ncsim_rng* rng, uint64_t* out, uint64_t cap);
+/* The same with the batch seeds given (nseeds = ceil(shots / 16384)): what a
+ * caller with its own generator passes after drawing one u64 per batch. */
+ncsim_status ncsim_frames_sample_packed_seeds(ncsim_frames* f, uint64_t shots, const uint64_t* seeds, uint64_t nseeds,
+                                              uint64_t* out, uint64_t cap);
+/* The same into device memory on the sampler's device (d_out: cap words). */
+ncsim_status ncsim_frames_sample_packed_device(ncsim_frames* f, uint64_t shots, const uint64_t* seeds, uint64_t nseeds,
+                                               uint64_t* d_out, uint64_t cap);
+/* sample (frame.rs:90-102): shot s's record is ceil(m / 64) words at
+ * out[s * ceil(m / 64)], bit k = measurement k; cap >= shots * ceil(m / 64). */
+ncsim_status ncsim_frames_sample(ncsim_frames* f, uint64_t shots, ncsim_rng* rng, uint64_t* out, uint64_t cap);
+/* sample_detectors (frame.rs:155-205): detector and observable flips, packed. */
+ncsim_status ncsim_frames_sample_detectors(ncsim_frames* f, uint64_t shots, ncsim_rng* rng, uint64_t* det,
+                                           uint64_t det_cap, uint64_t* obs, uint64_t obs_cap);
+/* The same with the batch seeds given. */
+ncsim_status ncsim_frames_sample_detectors_seeds(ncsim_frames* f, uint64_t shots, const uint64_t* seeds,
+                                                 uint64_t nseeds, uint64_t* det, uint64_t det_cap, uint64_t* obs,
+                                                 uint64_t obs_cap);
+/* Device time of the last call's mask and frame kernels (CUDA events on its stream). */
+ncsim_status ncsim_frames_last_kernel_ms(const ncsim_frames* f, double* ms);
 
 #ifdef __cplusplus
 }

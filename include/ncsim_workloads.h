@@ -32,6 +32,13 @@ ncsim_status ncsim_workload_random_circuit_rng(ncsim_rng* rng, uint32_t n, uint3
  * from {CX, CCX, CCZ, DIAG over the register, MONOMIAL on 8 qubits}. */
 ncsim_status ncsim_workload_reversible_circuit(uint32_t n, uint32_t gates, uint64_t seed, ncsim_circuit** out);
 
+/* The frame-sampler benchmark circuit (ncsim's examples/bench.rs:264-294 with
+ * n = 1000, rounds = 20, meas = 100, p = 1e-3, seed = 9): H on qubits 0..n/2;
+ * per round CX(q, b) and DEPOLARIZE2(p) on (q, b) for every even q, with
+ * b = (q + 1 + gen_range(0..n-1)) mod n, then `meas` Z measurements of
+ * gen_range(0..n) qubits. */
+ncsim_status ncsim_workload_frames_circuit(uint32_t n, uint32_t rounds, uint32_t meas, double p, uint64_t seed,
+                                           ncsim_circuit** out);
 /* Trajectory t: StdRng::seed_from_u64(seed0 + t), n = n_lo + gen_range(0..n_span),
  * the random-layer circuit of `depth` layers with DEPOLARIZE2(p) after every
  * CZ and M on every qubit (ncsim_workload_random_circuit_rng), run with the

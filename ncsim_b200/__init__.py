@@ -172,6 +172,18 @@ _SIGNATURES = {
     "ncsim_sparse_synchronize": (_i32, [_vp]),
     "ncsim_sparse_timer_start": (_i32, [_vp]),
     "ncsim_sparse_timer_stop": (_i32, [_vp, _P(_dbl)]),
+    "ncsim_frames_new": (_i32, [_vp, _u64, _P(_vp)]),
+    "ncsim_frames_with_reference": (_i32, [_vp, _P(C.c_uint8), _u64, _P(_vp)]),
+    "ncsim_frames_free": (_i32, [_vp]),
+    "ncsim_frames_info": (_i32, [_vp, _P(_u32), _P(_u64), _P(_u64), _P(_u64), _P(_u64)]),
+    "ncsim_frames_reference": (_i32, [_vp, _P(C.c_uint8), _u64]),
+    "ncsim_frames_sample_packed": (_i32, [_vp, _u64, _vp, _P(_u64), _u64]),
+    "ncsim_frames_sample_packed_seeds": (_i32, [_vp, _u64, _P(_u64), _u64, _P(_u64), _u64]),
+    "ncsim_frames_sample_packed_device": (_i32, [_vp, _u64, _P(_u64), _u64, _vp, _u64]),
+    "ncsim_frames_sample": (_i32, [_vp, _u64, _vp, _P(_u64), _u64]),
+    "ncsim_frames_sample_detectors": (_i32, [_vp, _u64, _vp, _P(_u64), _u64, _P(_u64), _u64]),
+    "ncsim_frames_sample_detectors_seeds": (_i32, [_vp, _u64, _P(_u64), _u64, _P(_u64), _u64, _P(_u64), _u64]),
+    "ncsim_frames_last_kernel_ms": (_i32, [_vp, _P(_dbl)]),
 }
 
 
@@ -202,6 +214,7 @@ _WORKLOAD_SIGNATURES = {
     "ncsim_workload_random_circuit": (_i32, [_u32, _u32, _u64, _dbl, _u32, _u32, _P(_vp)]),
     "ncsim_workload_random_circuit_rng": (_i32, [_vp, _u32, _u32, _dbl, _u32, _u32, _P(_vp)]),
     "ncsim_workload_reversible_circuit": (_i32, [_u32, _u32, _u64, _P(_vp)]),
+    "ncsim_workload_frames_circuit": (_i32, [_u32, _u32, _u32, _dbl, _u64, _P(_vp)]),
     "ncsim_batch_random_layers": (_i32, [_u32, _u64, _u32, _u32, _u32, _dbl, _P(_vp)]),
 }
 
@@ -382,6 +395,14 @@ class Circuit:
         """The random layer family drawn from ``rng``, which keeps its state."""
         h = _vp()
         _check(workloads_lib().ncsim_workload_random_circuit_rng(rng._h, n, depth, noise_p, m_lo, m_hi, C.byref(h)))
+        return cls(h)
+
+    @classmethod
+    def frames_workload(cls, n: int = 1000, rounds: int = 20, meas: int = 100, p: float = 1e-3,
+                        seed: int = 9) -> "Circuit":
+        """The reference's frame-sampler benchmark circuit (examples/bench.rs:264-294)."""
+        h = _vp()
+        _check(workloads_lib().ncsim_workload_frames_circuit(n, rounds, meas, p, seed, C.byref(h)))
         return cls(h)
 
     @classmethod
@@ -1017,6 +1038,96 @@ class GpuSparseVector:
         ms = _dbl()
         _check(lib().ncsim_sparse_timer_stop(self._h, C.byref(ms)))
         return ms.value
+
+
+class FrameSampler:
+    """Bulk sampler of a noisy Clifford circuit by Pauli frames on the GPU: the
+    drop-in for ncsim's ``FrameSampler`` (``src/frame.rs:34-300``).
+
+    Records come packed as the reference returns them: row k of the
+    ``(measurements, ceil(shots / 64))`` uint64 array holds measurement k over
+    the shots (bit s of word s // 64 = shot s).  Shots run in batches of 16384,
+    each seeded by one ``next_u64`` of the caller's generator.
+    """
+
+    BATCH = 1 << 14
+
+    def __init__(self, circuit: Circuit, reference_seed: int = 0, reference: Sequence[int] | None = None):
+        h = _vp()
+        if reference is None:
+            _check(lib().ncsim_frames_new(circuit._h, reference_seed, C.byref(h)))
+        else:
+            r = np.ascontiguousarray(np.asarray(list(reference), dtype=np.uint8))
+            _check(lib().ncsim_frames_with_reference(circuit._h, r.ctypes.data_as(_P(C.c_uint8)), r.size, C.byref(h)))
+        self._h = h
+        n, m, d, o, layers = _u32(), _u64(), _u64(), _u64(), _u64()
+        _check(lib().ncsim_frames_info(h, C.byref(n), C.byref(m), C.byref(d), C.byref(o), C.byref(layers)))
+        self.n, self.m = n.value, m.value
+        self.num_detectors, self.num_observables, self.num_layers = d.value, o.value, layers.value
+
+    def __del__(self):
+        h = getattr(self, "_h", None)
+        if h and _lib is not None:
+            _lib.ncsim_frames_free(h)
+            self._h = None
+
+    def reference(self) -> list[bool]:
+        """``FrameSampler::reference`` (frame.rs:66-68): the noiseless record."""
+        r = np.zeros(max(self.m, 1), dtype=np.uint8)
+        _check(lib().ncsim_frames_reference(self._h, r.ctypes.data_as(_P(C.c_uint8)), r.size))
+        return [bool(v) for v in r[: self.m]]
+
+    @staticmethod
+    def words(shots: int) -> int:
+        return (shots + 63) // 64
+
+    def sample_packed(self, shots: int, rng: StdRng) -> np.ndarray:
+        """``sample_packed`` (frame.rs:69-89): (measurements, words) uint64."""
+        out = np.zeros((self.m, self.words(shots)), dtype=np.uint64)
+        _check(lib().ncsim_frames_sample_packed(self._h, shots, rng._h, out.ctypes.data_as(_P(_u64)), out.size))
+        return out
+
+    def sample_packed_seeds(self, shots: int, seeds: Sequence[int], out: np.ndarray | None = None) -> np.ndarray:
+        """The same with the per-batch seeds given (one per 16384 shots)."""
+        sd = np.ascontiguousarray(np.asarray(list(seeds), dtype=np.uint64))
+        if out is None:
+            out = np.zeros((self.m, self.words(shots)), dtype=np.uint64)
+        _check(lib().ncsim_frames_sample_packed_seeds(self._h, shots, sd.ctypes.data_as(_P(_u64)), sd.size,
+                                                      out.ctypes.data_as(_P(_u64)), out.size))
+        return out
+
+    def sample_packed_device(self, shots: int, seeds: Sequence[int], d_out: int, cap_words: int) -> None:
+        """The same into device memory (``d_out``: a device pointer of ``cap_words`` words)."""
+        sd = np.ascontiguousarray(np.asarray(list(seeds), dtype=np.uint64))
+        _check(lib().ncsim_frames_sample_packed_device(self._h, shots, sd.ctypes.data_as(_P(_u64)), sd.size,
+                                                       _vp(d_out), cap_words))
+
+    def sample(self, shots: int, rng: StdRng) -> np.ndarray:
+        """``sample`` (frame.rs:90-102): (shots, ceil(m / 64)) uint64, bit k = measurement k."""
+        mw = (self.m + 63) // 64
+        out = np.zeros((shots, mw), dtype=np.uint64)
+        _check(lib().ncsim_frames_sample(self._h, shots, rng._h, out.ctypes.data_as(_P(_u64)), out.size))
+        return out
+
+    def sample_detectors(self, shots: int, rng: StdRng):
+        """``sample_detectors`` (frame.rs:155-205): packed detector and observable flips."""
+        w = self.words(shots)
+        det = np.zeros((self.num_detectors, w), dtype=np.uint64)
+        obs = np.zeros((self.num_observables, w), dtype=np.uint64)
+        _check(lib().ncsim_frames_sample_detectors(self._h, shots, rng._h, det.ctypes.data_as(_P(_u64)), det.size,
+                                                   obs.ctypes.data_as(_P(_u64)), obs.size))
+        return det, obs
+
+    def last_kernel_ms(self) -> float:
+        """Device time of the last call's mask and frame kernels."""
+        ms = _dbl()
+        _check(lib().ncsim_frames_last_kernel_ms(self._h, C.byref(ms)))
+        return ms.value
+
+
+def packed_bit(packed: np.ndarray, k: int, s: int) -> bool:
+    """Bit s of packed row k (``bits::get``)."""
+    return bool((int(packed[k, s // 64]) >> (s % 64)) & 1)
 
 
 def device_info() -> dict:

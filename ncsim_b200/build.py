@@ -24,6 +24,8 @@ SOURCES = [
     "csrc/batch.cu",
     "csrc/batch_plan.cpp",
     "csrc/sparse.cu",
+    "csrc/frames.cu",
+    "csrc/frames_plan.cpp",
     "csrc/host/ir.cpp",
     "csrc/host/runtime.cpp",
 ]
@@ -35,6 +37,7 @@ HEADERS = [
     "csrc/host_math.hpp",
     "csrc/fused_plan.hpp",
     "csrc/batch_plan.hpp",
+    "csrc/frames_plan.hpp",
     "csrc/host/ir.hpp",
     "csrc/host/rng.hpp",
     "../include/ncsim_cuda.h",

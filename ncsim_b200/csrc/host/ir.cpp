@@ -89,7 +89,7 @@ std::string fmt_f64(double v) {
 }
 
 // ---------------------------------------------------------------------------
-PauliOp parse_pauli(const std::string& text, int64_t nreg) {
+PauliSites parse_pauli_sites(const std::string& text, int64_t nreg) {
   auto bad = [&](const std::string& m) { return parse_error("Pauli '" + text + "': " + m); };
   std::string rest = strip(text);
   uint32_t ph = 0;
@@ -103,18 +103,19 @@ PauliOp parse_pauli(const std::string& text, int64_t nreg) {
       break;
     }
   }
-  PauliOp p;
+  auto bits_of = [](char c) -> uint8_t { return c == 'X' ? 1 : c == 'Z' ? 2 : c == 'Y' ? 3 : 0; };
+  PauliSites p;
+  p.phase = ph;
   const bool dense = !rest.empty() && rest.find_first_not_of("IXYZ_") == std::string::npos;
   if (dense) {
-    if (rest.size() > 64) throw bad("more than 64 qubits");
+    if (rest.size() > MAX_CIRCUIT_QUBITS) throw bad("more than " + std::to_string(MAX_CIRCUIT_QUBITS) + " qubits");
     if (nreg >= 0 && size_t(nreg) != rest.size())
       throw bad(std::to_string(rest.size()) + " letters for " + std::to_string(nreg) + " qubits");
     p.n = uint32_t(rest.size());
-    for (uint32_t q = 0; q < p.n; ++q) set_letter(p, q, rest[q]);
-    p.phase = (p.phase + ph) & 3;
+    for (uint32_t q = 0; q < p.n; ++q)
+      if (uint8_t b = bits_of(rest[q])) p.sites.push_back({q, b});
     return p;
   }
-  std::vector<std::pair<uint64_t, char>> sites;
   std::string tok;
   auto flush = [&] {
     if (tok.empty()) return;
@@ -126,9 +127,10 @@ PauliOp parse_pauli(const std::string& text, int64_t nreg) {
     if (c != 'I' && c != 'X' && c != 'Y' && c != 'Z') throw bad("token '" + t + "'");
     uint64_t q;
     if (!to_u64(t.substr(1), q) || t.size() < 2) throw bad("token '" + t + "'");
-    for (auto& s : sites)
+    if (q >= MAX_CIRCUIT_QUBITS) throw bad("qubit " + std::to_string(q) + " above the register limit");
+    for (auto& s : p.sites)
       if (s.first == q) throw bad("qubit " + std::to_string(q) + " repeated");
-    sites.push_back({q, c});
+    p.sites.push_back({uint32_t(q), bits_of(c)});  // identity letters hold a place until the sort
   };
   for (char c : rest) {
     if (c == '*' || std::isspace((unsigned char)c)) flush();
@@ -138,15 +140,34 @@ PauliOp parse_pauli(const std::string& text, int64_t nreg) {
   uint64_t n = 0;
   if (nreg >= 0) n = uint64_t(nreg);
   else
-    for (auto& s : sites) n = std::max(n, s.first + 1);
-  if (n > 64) throw bad("more than 64 qubits");
+    for (auto& s : p.sites) n = std::max<uint64_t>(n, uint64_t(s.first) + 1);
   p.n = uint32_t(n);
-  for (auto& s : sites) {
+  for (auto& s : p.sites)
     if (s.first >= n) throw bad("qubit " + std::to_string(s.first) + " out of range for " + std::to_string(n) + " qubits");
-    set_letter(p, uint32_t(s.first), s.second);
-  }
-  p.phase = (p.phase + ph) & 3;
+  p.sites.erase(std::remove_if(p.sites.begin(), p.sites.end(), [](const std::pair<uint32_t, uint8_t>& s) { return s.second == 0; }),
+                p.sites.end());
+  std::sort(p.sites.begin(), p.sites.end());
   return p;
+}
+
+PauliOp pauli_from_sites(const PauliSites& s) {
+  if (s.n > 64) throw parse_error("Paulis on more than 64 qubits have no one-word form");
+  PauliOp p;
+  p.n = s.n;
+  uint32_t ys = 0;
+  for (auto& st : s.sites) {
+    if (st.second & 1) p.x |= uint64_t(1) << st.first;
+    if (st.second & 2) p.z |= uint64_t(1) << st.first;
+    ys += st.second == 3;
+  }
+  p.phase = (s.phase + ys) & 3;
+  return p;
+}
+
+PauliOp parse_pauli(const std::string& text, int64_t nreg) {
+  PauliSites s = parse_pauli_sites(text, nreg);
+  if (s.n > 64) throw parse_error("Pauli '" + text + "': more than 64 qubits");
+  return pauli_from_sites(s);
 }
 
 static std::string pauli_sparse(const PauliOp& p) {
@@ -274,6 +295,8 @@ MonomialIR diag_mono(uint32_t k, uint32_t bits, std::initializer_list<std::pair<
   return m;
 }
 
+}  // namespace
+
 // Gate::monomial (gate.rs:519-564); false when the gate has no monomial view
 bool monomial_view(const GateIR& g, MonomialIR& m) {
   switch (g.kind) {
@@ -308,8 +331,6 @@ bool monomial_view(const GateIR& g, MonomialIR& m) {
     default: return false;
   }
 }
-
-}  // namespace
 
 std::vector<CplxD> gate_matrix(const GateIR& g) {
   const double h = 0.5 * 1.41421356237309504880;  // sqrt2_pow(-1)
@@ -640,15 +661,25 @@ std::string ncsim_circuit::text() const {
         for (uint32_t q : o.qubits) s += " " + std::to_string(q);
         break;
       case OpKind::Measure: {
-        uint64_t sup = o.pauli.x | o.pauli.z;
-        uint32_t ys = uint32_t(__builtin_popcountll(o.pauli.x & o.pauli.z));
-        uint32_t letter_phase = (o.pauli.phase + 4 - (ys & 3)) & 3;
-        if (__builtin_popcountll(sup) == 1 && letter_phase == 0) {
-          uint32_t q = uint32_t(__builtin_ctzll(sup));
-          bool bx = (o.pauli.x >> q) & 1, bz = (o.pauli.z >> q) & 1;
-          s += std::string("M") + ((bx && bz) ? 'Y' : bx ? 'X' : 'Z') + " " + std::to_string(q);
+        const auto& st = o.sites;
+        static const char letters[] = "IXZY";
+        if (st.sites.size() == 1 && st.phase == 0) {
+          s += std::string("M") + letters[st.sites[0].second] + " " + std::to_string(st.sites[0].first);
         } else {
-          s += "MPP " + pauli_sparse(o.pauli);
+          static const char* pre[] = {"", "i*", "-", "-i*"};
+          std::string body;
+          for (auto& t : st.sites) {
+            if (!body.empty()) body += "*";
+            body += letters[t.second];
+            body += std::to_string(t.first);
+          }
+          if (body.empty()) {
+            static const char* sc[] = {"1", "i", "-1", "-i"};
+            body = sc[st.phase & 3];
+          } else {
+            body = pre[st.phase & 3] + body;
+          }
+          s += "MPP " + body;
         }
         break;
       }
@@ -725,9 +756,9 @@ ncsim_circuit parse_circuit(const std::string& text) {
     p.name = upcase(lp == std::string::npos ? p.head : p.head.substr(0, lp));
     if (p.name == "MPP") {
       for (size_t i = 1; i < L.toks.size(); ++i) {
-        PauliOp q;
+        PauliSites q;
         try {
-          q = parse_pauli(L.toks[i], -1);
+          q = parse_pauli_sites(L.toks[i], -1);
         } catch (const Error& e) {
           throw at(L.ln, e.what());
         }
@@ -746,7 +777,7 @@ ncsim_circuit parse_circuit(const std::string& text) {
     } else {
       for (size_t i = 1; i < L.toks.size(); ++i) {
         uint64_t q;
-        if (!to_u64(L.toks[i], q) || q > 63) throw at(L.ln, "bad qubit '" + L.toks[i] + "'");
+        if (!to_u64(L.toks[i], q) || q >= MAX_CIRCUIT_QUBITS) throw at(L.ln, "bad qubit '" + L.toks[i] + "'");
         p.qs.push_back(uint32_t(q));
         max_q = std::max<uint64_t>(max_q, q + 1);
       }
@@ -755,7 +786,7 @@ ncsim_circuit parse_circuit(const std::string& text) {
   }
   const uint64_t n = declared >= 0 ? uint64_t(declared) : max_q;
   if (n < max_q) throw parse_error("QUBITS " + std::to_string(n) + " but qubit " + std::to_string(max_q - 1) + " is used");
-  if (n > 64) throw parse_error("registers of more than 64 qubits");
+  if (n > MAX_CIRCUIT_QUBITS) throw parse_error("registers of more than " + std::to_string(MAX_CIRCUIT_QUBITS) + " qubits");
   ncsim_circuit c;
   c.n = uint32_t(n);
   uint64_t measured = 0;
@@ -765,7 +796,20 @@ ncsim_circuit parse_circuit(const std::string& text) {
     o.gate = g;
     o.qubits = qs;
     try {
-      o.lowered = lower_gate(g, qs, c.n);
+      if (c.n <= 64) {
+        o.lowered = lower_gate(g, qs, c.n);
+      } else {
+        // wider than any state form: the same checks, the gate lowered on its own qubits only
+        std::vector<uint32_t> local(qs.size());
+        for (size_t i = 0; i < qs.size(); ++i) {
+          if (qs[i] >= c.n) throw qubit_out_of_range(qs[i], c.n);
+          for (size_t j = 0; j < i; ++j)
+            if (qs[j] == qs[i]) throw duplicate_qubit(qs[i]);
+          local[i] = uint32_t(i);
+        }
+        if (qs.size() <= 64) lower_gate(g, local, uint32_t(qs.size()));
+        else if (qs.size() != g.arity()) throw arity_error(g.text(), g.arity(), qs.size());
+      }
     } catch (const Error& e) {
       throw Error(e.code == NCSIM_ERR_PARSE ? e.code : NCSIM_ERR_PARSE, "line " + std::to_string(ln + 1) + ": " + e.what());
     }
@@ -778,8 +822,10 @@ ncsim_circuit parse_circuit(const std::string& text) {
       for (uint32_t q : p.qs) {
         OpIR o;
         o.kind = OpKind::Measure;
+        o.sites.n = c.n;
+        o.sites.sites = {{q, uint8_t(letter == 'X' ? 1 : letter == 'Z' ? 2 : 3)}};
         o.pauli.n = c.n;
-        set_letter(o.pauli, q, letter);
+        if (c.n <= 64) set_letter(o.pauli, q, letter);
         c.ops.push_back(o);
         ++measured;
       }
@@ -788,11 +834,13 @@ ncsim_circuit parse_circuit(const std::string& text) {
         OpIR o;
         o.kind = OpKind::Measure;
         try {
-          o.pauli = parse_pauli(t, int64_t(c.n));
+          o.sites = parse_pauli_sites(t, int64_t(c.n));
         } catch (const Error& e) {
           throw at(p.ln, e.what());
         }
-        if (!o.pauli.hermitian()) throw at(p.ln, "measured operator " + t + " is not Hermitian");
+        if (!o.sites.hermitian()) throw at(p.ln, "measured operator " + t + " is not Hermitian");
+        o.pauli.n = c.n;
+        if (c.n <= 64) o.pauli = pauli_from_sites(o.sites);
         c.ops.push_back(o);
         ++measured;
       }

@@ -22,7 +22,22 @@ struct PauliOp {
   uint32_t phase = 0;
   bool hermitian() const { return ((phase & 1) == 1) == bool(__builtin_popcountll(x & z) & 1); }
 };
+// Circuits (and the Paulis they measure) may name up to this many qubits; the
+// state forms take registers of at most 64, the frame sampler any of these.
+constexpr uint32_t MAX_CIRCUIT_QUBITS = 1u << 24;
+
+// A Pauli on any number of qubits as its non-identity sites (qubit ascending;
+// letter bits 1 = X, 2 = Z, 3 = Y) and the phase i^phase in front of the
+// letters (so Y counts as a letter, not as i X Z).
+struct PauliSites {
+  uint32_t n = 0;
+  std::vector<std::pair<uint32_t, uint8_t>> sites;
+  uint32_t phase = 0;
+  bool hermitian() const { return (phase & 1) == 0; }
+};
 // Pauli::from_string / Pauli::parse (src/pauli/mod.rs:344-414); n < 0 infers the size
+PauliSites parse_pauli_sites(const std::string& text, int64_t n);
+PauliOp pauli_from_sites(const PauliSites& s);  // registers of at most 64 qubits
 PauliOp parse_pauli(const std::string& text, int64_t n);
 
 // f(x) = constant + sum_t c_t prod_{l in t} [l . x] mod 2^bits over nvars
@@ -45,6 +60,9 @@ struct MonomialIR {
   Phase scalar;
   bool affine_identity() const;
 };
+struct GateIR;
+// Gate::monomial (gate.rs:519-564); false when the gate has no monomial view
+bool monomial_view(const GateIR& g, MonomialIR& out);
 
 enum class GateKind : int {
   I, X, Y, Z, H, S, Sdg, SqrtX, SqrtXdg, SqrtY, SqrtYdg, T, Tdg, Cx, Cy, Cz, Swap, Cs, Csdg, Ccz, Ccx,
@@ -100,8 +118,9 @@ struct OpIR {
   OpKind kind = OpKind::Tick;
   GateIR gate;
   std::vector<uint32_t> qubits;
-  LoweredOp lowered;
-  PauliOp pauli;
+  LoweredOp lowered;  // registers of at most 64 qubits (the state forms' limit)
+  PauliOp pauli;      // measured Pauli, registers of at most 64 qubits
+  PauliSites sites;   // measured Pauli, any register
   NoiseIR noise;
   std::vector<uint64_t> lookback;
   uint64_t index = 0;

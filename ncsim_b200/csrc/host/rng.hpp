@@ -83,6 +83,20 @@ struct ncsim_rng {
   // Standard f64: 53 high bits times 2^-53
   double f64() { return double(u64() >> 11) * 0x1.0p-53; }
 
+  // Index of the next u32 word in the key stream.  The buffer holds four
+  // consecutive blocks and a u64 draw that straddles a refill takes the last
+  // word of one buffer and the first of the next, so every draw reads the
+  // stream's next words in order: skipping draws is moving this index.
+  uint64_t position() const { return next_block * 16 + pos - 64; }
+  void seek(uint64_t p) {
+    next_block = (p / 64) * 4;
+    pos = 64;
+    if (p % 64) {
+      refill();
+      pos = unsigned(p % 64);
+    }
+  }
+
   // UniformInt sample_single over [lo, hi) with u64 words
   uint64_t range64(uint64_t lo, uint64_t hi) {
     if (hi <= lo) throw std::invalid_argument("empty range");

@@ -53,6 +53,25 @@ std::string random_layer_text(uint32_t n, uint32_t depth, ncsim_rng& rng, double
   return s;
 }
 
+// The frame-sampler benchmark of the reference (examples/bench.rs:264-294):
+// H on qubits 0..n/2, then `rounds` rounds of CX(q, b) + DEPOLARIZE2(p) for
+// every even q with b = (q + 1 + gen_range(0..n-1)) mod n, followed by
+// `meas` Z measurements of gen_range(0..n) qubits.
+std::string frames_text(uint32_t n, uint32_t rounds, uint32_t meas, double p, ncsim_rng& rng) {
+  std::string s = "QUBITS " + std::to_string(n) + "\n";
+  for (uint32_t q = 0; q < n / 2; ++q) s += "H " + std::to_string(q) + "\n";
+  const std::string noise = "DEPOLARIZE2(" + fmt_f64(p) + ") ";
+  for (uint32_t r = 0; r < rounds; ++r) {
+    for (uint32_t q = 0; q < n; q += 2) {
+      const uint64_t b = (q + 1 + rng.range64(0, n - 1)) % n;
+      const std::string pair = std::to_string(q) + " " + std::to_string(b);
+      s += "CX " + pair + "\n" + noise + pair + "\n";
+    }
+    for (uint32_t k = 0; k < meas; ++k) s += "M " + std::to_string(rng.range64(0, n)) + "\n";
+  }
+  return s;
+}
+
 std::vector<uint32_t> pick_distinct(ncsim_rng& rng, uint32_t n, uint32_t k) {
   std::vector<uint32_t> v;
   while (v.size() < k) {
@@ -135,6 +154,16 @@ ncsim_status ncsim_workload_random_circuit_rng(ncsim_rng* rng, uint32_t n, uint3
     *out = nullptr;
     if (n < 1 || n > 64) throw Error(NCSIM_ERR_INVALID, "workload register must have 1..64 qubits");
     *out = new ncsim_circuit(parse_circuit(random_layer_text(n, depth, *rng, noise_p, m_lo, m_hi)));
+  });
+}
+ncsim_status ncsim_workload_frames_circuit(uint32_t n, uint32_t rounds, uint32_t meas, double p, uint64_t seed,
+                                           ncsim_circuit** out) {
+  return guarded([&] {
+    need(out, "out");
+    *out = nullptr;
+    if (n < 2 || n > MAX_CIRCUIT_QUBITS) throw Error(NCSIM_ERR_INVALID, "frame workload needs 2..2^24 qubits");
+    ncsim_rng rng(seed);
+    *out = new ncsim_circuit(parse_circuit(frames_text(n, rounds, meas, p, rng)));
   });
 }
 ncsim_status ncsim_workload_reversible_circuit(uint32_t n, uint32_t gates, uint64_t seed, ncsim_circuit** out) {

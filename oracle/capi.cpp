@@ -3,6 +3,7 @@
 // A flat C interface to the restatement so that pytest (ctypes) and the CPU
 // baseline leg of bench.py can drive it.  Errors return a negative status and
 // leave a message in oracle_last_error().
+#include "frames_ref.hpp"
 #include "ncsim_ref.hpp"
 #include "workloads_ref.hpp"
 
@@ -61,6 +62,11 @@ int oracle_random_circuit_text(uint32_t n, uint32_t depth, uint64_t seed, double
                                char* buf, size_t cap) {
   StdRng rng = StdRng::seed_from_u64(seed);
   return copy_text(random_circuit_text(n, depth, rng, noise_p, m_lo, m_hi), buf, cap);
+}
+int oracle_frames_circuit_text(uint32_t n, uint32_t rounds, uint32_t meas, double p, uint64_t seed, char* buf,
+                               size_t cap) {
+  StdRng rng = StdRng::seed_from_u64(seed);
+  return copy_text(frames_circuit_text(n, rounds, meas, p, rng), buf, cap);
 }
 int oracle_reversible_circuit_text(uint32_t n, uint32_t gates, uint64_t seed, char* buf, size_t cap) {
   StdRng rng = StdRng::seed_from_u64(seed);
@@ -327,4 +333,41 @@ void oracle_sparse_get(void* h, uint64_t* idx, double* amp) {
 }
 void oracle_sparse_free(void* h) { delete (SparseState*)h; }
 
+
+// ---- frame sampler (frame.rs) ----
+// The reference record of FrameSampler::new; returns the number of measurements.
+int oracle_frames_reference(const char* text, uint64_t seed, uint8_t* out, size_t cap) {
+  int m = 0;
+  int st = guard([&] {
+    auto r = frame_reference(Circuit::parse(text), seed);
+    if (cap < r.size()) throw SimError(ErrKind::Invalid, "buffer too small");
+    for (size_t i = 0; i < r.size(); ++i) out[i] = r[i];
+    m = int(r.size());
+  });
+  return st == 0 ? m : st;
+}
+// sample_packed with the batch seeds given: out holds m rows of nwords(shots)
+int oracle_frames_sample_packed(const char* text, const uint8_t* reference, size_t m, uint64_t shots,
+                                const uint64_t* seeds, size_t nseeds, int threads, uint64_t* out) {
+  return guard([&] {
+    FrameSamplerRef f(Circuit::parse(text), std::vector<bool>(reference, reference + m));
+    auto rec = f.sample_packed_seeds(shots, std::vector<uint64_t>(seeds, seeds + nseeds), threads);
+    const size_t W = nwords(shots);
+    for (size_t k = 0; k < rec.size(); ++k) std::memcpy(out + k * W, rec[k].data(), W * 8);
+  });
+}
+// sample_detectors with the batch seeds given
+int oracle_frames_sample_detectors(const char* text, const uint8_t* reference, size_t m, uint64_t shots,
+                                   const uint64_t* seeds, size_t nseeds, uint64_t* det, size_t det_rows, uint64_t* obs,
+                                   size_t obs_rows) {
+  return guard([&] {
+    FrameSamplerRef f(Circuit::parse(text), std::vector<bool>(reference, reference + m));
+    std::vector<std::vector<uint64_t>> d, o;
+    f.sample_detectors_seeds(shots, std::vector<uint64_t>(seeds, seeds + nseeds), d, o);
+    if (d.size() != det_rows || o.size() != obs_rows) throw SimError(ErrKind::Invalid, "detector or observable count");
+    const size_t W = nwords(shots);
+    for (size_t k = 0; k < d.size(); ++k) std::memcpy(det + k * W, d[k].data(), W * 8);
+    for (size_t k = 0; k < o.size(); ++k) std::memcpy(obs + k * W, o[k].data(), W * 8);
+  });
+}
 }  // extern "C"

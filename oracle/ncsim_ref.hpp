@@ -473,6 +473,79 @@ struct Pauli {
   static Pauli from_string(size_t n, const std::string& s) { return parse_with(s, n); }
 };
 
+// A Pauli on a register of any width (src/pauli/mod.rs keeps Bits of any
+// length): its non-identity letters by qubit (1 = X, 2 = Z, 3 = Y) and the
+// phase i^phase in front of the letters.  The same grammar as Pauli::parse.
+struct WidePauli {
+  size_t n = 0;
+  std::vector<std::pair<size_t, uint8_t>> sites;  // ascending qubits
+  uint8_t phase = 0;
+  bool is_hermitian() const { return (phase & 1) == 0; }
+  static WidePauli parse_with(const std::string& s, std::optional<size_t> nreg) {
+    auto err = [&](const std::string& m) { return SimError(ErrKind::Parse, "Pauli '" + s + "': " + m); };
+    auto trim = [](std::string t) {
+      size_t a = t.find_first_not_of(" \t\r\n");
+      if (a == std::string::npos) return std::string();
+      size_t b = t.find_last_not_of(" \t\r\n");
+      return t.substr(a, b - a + 1);
+    };
+    std::string rest = trim(s);
+    WidePauli w;
+    const std::pair<const char*, uint8_t> pres[] = {{"-i", 3}, {"+i", 1}, {"-", 2}, {"+", 0}, {"i", 1}};
+    for (auto& pr : pres) {
+      std::string pre = pr.first;
+      if (rest.compare(0, pre.size(), pre) == 0) {
+        std::string r = trim(rest.substr(pre.size()));
+        if (!r.empty() && r[0] == '*') r = trim(r.substr(1));
+        w.phase = pr.second;
+        rest = r;
+        break;
+      }
+    }
+    auto letter = [](char c) -> uint8_t { return c == 'X' ? 1 : c == 'Z' ? 2 : c == 'Y' ? 3 : 0; };
+    bool dense = !rest.empty() && rest.find_first_not_of("IXYZ_") == std::string::npos;
+    if (dense) {
+      if (nreg && *nreg != rest.size())
+        throw err(std::to_string(rest.size()) + " letters for " + std::to_string(*nreg) + " qubits");
+      w.n = rest.size();
+      for (size_t q = 0; q < rest.size(); ++q)
+        if (letter(rest[q])) w.sites.push_back({q, letter(rest[q])});
+      return w;
+    }
+    std::vector<std::pair<size_t, uint8_t>> all;
+    std::string tok;
+    auto flush = [&]() {
+      if (tok.empty()) return;
+      std::string t = tok;
+      tok.clear();
+      if (t == "1") return;
+      char c = t[0];
+      if (c != 'I' && c != '_' && c != 'X' && c != 'Y' && c != 'Z') throw err("token '" + t + "'");
+      std::string num = t.substr(1);
+      if (num.empty() || num.find_first_not_of("0123456789") != std::string::npos) throw err("token '" + t + "'");
+      size_t idx = std::stoull(num);
+      for (auto& st : all)
+        if (st.first == idx) throw err("qubit " + std::to_string(idx) + " repeated");
+      all.push_back({idx, letter(c)});
+    };
+    for (char c : rest) {
+      if (c == '*' || std::isspace((unsigned char)c)) flush();
+      else tok.push_back(c);
+    }
+    flush();
+    if (nreg) w.n = *nreg;
+    else
+      for (auto& st : all) w.n = std::max(w.n, st.first + 1);
+    for (auto& st : all) {
+      if (st.first >= w.n)
+        throw err("qubit " + std::to_string(st.first) + " out of range for " + std::to_string(w.n) + " qubits");
+      if (st.second) w.sites.push_back(st);
+    }
+    std::sort(w.sites.begin(), w.sites.end());
+    return w;
+  }
+};
+
 // ---------------------------------------------------------------------------
 // PhasePoly: src/phasepoly.rs:540-678 (variables fit one word)
 // ---------------------------------------------------------------------------
@@ -852,9 +925,12 @@ struct Op {
   OpKind kind = OpKind::Tick;
   Gate gate;
   std::vector<size_t> qubits;
-  Pauli pauli;
+  Pauli pauli;      // measured Pauli (registers of at most 64 qubits)
+  WidePauli wide;   // measured Pauli, any register
   size_t qubit = 0;
   Noise noise;
+  std::vector<size_t> lookback;  // DETECTOR / OBSERVABLE_INCLUDE rec[-k]
+  size_t index = 0;              // OBSERVABLE_INCLUDE(index)
 };
 
 struct Circuit {
@@ -880,8 +956,9 @@ struct Circuit {
                                              " qubits, " + std::to_string(op.qubits.size()) + " given");
         break;
       case OpKind::Measure:
-        if (op.pauli.n != n) throw SimError(ErrKind::Invalid, "measurement on the wrong register");
-        if (!op.pauli.is_hermitian()) throw SimError(ErrKind::Invalid, "measured operator is not Hermitian");
+        if (op.pauli.n != n || op.wide.n != n) throw SimError(ErrKind::Invalid, "measurement on the wrong register");
+        if (!op.pauli.is_hermitian() || !op.wide.is_hermitian())
+          throw SimError(ErrKind::Invalid, "measured operator is not Hermitian");
         break;
       case OpKind::Reset: check_qubits({op.qubit}, n); break;
       case OpKind::NoiseOp:
@@ -1113,7 +1190,7 @@ inline Circuit Circuit::parse(const std::string& text) {  // circuit.rs:459-565
     } else if (name == "MPP") {
       pl.kind = 2;
       for (size_t i = 1; i < toks.size(); ++i) {
-        Pauli::parse(toks[i]);  // validates
+        WidePauli::parse_with(toks[i], std::nullopt);  // validates
         pl.mpp.push_back(toks[i]);
       }
     } else if (name == "R") {
@@ -1155,7 +1232,7 @@ inline Circuit Circuit::parse(const std::string& text) {  // circuit.rs:459-565
       throw err(ln, "unknown instruction '" + name + "'");
     }
     if (pl.kind == 2) {
-      for (auto& s : pl.mpp) max_q = std::max(max_q, Pauli::parse(s).n);
+      for (auto& s : pl.mpp) max_q = std::max(max_q, WidePauli::parse_with(s, std::nullopt).n);
     } else {
       for (size_t q : pl.qs) max_q = std::max(max_q, q + 1);
     }
@@ -1184,7 +1261,9 @@ inline Circuit Circuit::parse(const std::string& text) {  // circuit.rs:459-565
             Op o;
             o.kind = OpKind::Measure;
             if (q >= n) throw SimError(ErrKind::QubitOutOfRange, "qubit out of range");
-            o.pauli = Pauli::single(n, q, p.pk);
+            o.pauli = n <= 64 ? Pauli::single(n, q, p.pk) : Pauli::identity(n);
+            o.wide.n = n;
+            o.wide.sites = {{q, uint8_t(p.pk == PauliKind::X ? 1 : p.pk == PauliKind::Z ? 2 : 3)}};
             c.push(o);
           }
           break;
@@ -1192,7 +1271,8 @@ inline Circuit Circuit::parse(const std::string& text) {  // circuit.rs:459-565
           for (auto& s : p.mpp) {
             Op o;
             o.kind = OpKind::Measure;
-            o.pauli = Pauli::from_string(n, s);
+            o.wide = WidePauli::parse_with(s, n);
+            o.pauli = n <= 64 ? Pauli::from_string(n, s) : Pauli::identity(n);
             c.push(o);
           }
           break;
@@ -1222,6 +1302,8 @@ inline Circuit Circuit::parse(const std::string& text) {  // circuit.rs:459-565
             if (k == 0 || k > m) throw SimError(ErrKind::Invalid, "rec[-" + std::to_string(k) + "] out of range");
           Op o;
           o.kind = p.kind == 5 ? OpKind::Detector : OpKind::Observable;
+          o.lookback = p.recs;
+          o.index = p.index;
           c.ops.push_back(o);
           break;
         }

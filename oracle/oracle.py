@@ -49,6 +49,7 @@ def lib():
             "oracle_chacha_block": (None, [P(u32), u64, i32, P(u32)]),
             "oracle_random_circuit_text": (i32, [u32, u32, u64, dbl, u32, u32, C.c_char_p, C.c_size_t]),
             "oracle_reversible_circuit_text": (i32, [u32, u32, u64, C.c_char_p, C.c_size_t]),
+            "oracle_frames_circuit_text": (i32, [u32, u32, u32, dbl, u64, C.c_char_p, C.c_size_t]),
             "oracle_circuit_parse": (vp, [C.c_char_p]),
             "oracle_circuit_free": (None, [vp]),
             "oracle_circuit_num_qubits": (u32, [vp]),
@@ -86,6 +87,11 @@ def lib():
             "oracle_sparse_len": (u64, [vp]),
             "oracle_sparse_get": (None, [vp, P(u64), P(dbl)]),
             "oracle_sparse_free": (None, [vp]),
+            "oracle_frames_reference": (i32, [C.c_char_p, u64, P(C.c_uint8), C.c_size_t]),
+            "oracle_frames_sample_packed": (i32, [C.c_char_p, P(C.c_uint8), C.c_size_t, u64, P(u64), C.c_size_t, i32,
+                                                  P(u64)]),
+            "oracle_frames_sample_detectors": (i32, [C.c_char_p, P(C.c_uint8), C.c_size_t, u64, P(u64), C.c_size_t,
+                                                     P(u64), C.c_size_t, P(u64), C.c_size_t]),
         }
         for name, (res, args) in sig.items():
             f = getattr(L, name)
@@ -150,6 +156,11 @@ def _text(fn, *args) -> str:
 
 def random_circuit_text(n: int, depth: int, seed: int, noise_p: float = 0.0, m_lo: int = 0, m_hi: int = 0) -> str:
     return _text(lib().oracle_random_circuit_text, n, depth, seed, noise_p, m_lo, m_hi)
+
+
+def frames_circuit_text(n: int = 1000, rounds: int = 20, meas: int = 100, p: float = 1e-3, seed: int = 9) -> str:
+    """The reference's frame-sampler benchmark circuit (examples/bench.rs:264-294)."""
+    return _text(lib().oracle_frames_circuit_text, n, rounds, meas, p, seed)
 
 
 def reversible_circuit_text(n: int, gates: int, seed: int) -> str:
@@ -335,3 +346,45 @@ def sparse_run(text: str):
         return idx, amp.view(np.complex128)
     finally:
         lib().oracle_sparse_free(h)
+
+
+FRAME_BATCH = 1 << 14
+
+
+def frame_reference(text: str, seed: int) -> list[bool]:
+    """FrameSampler::new's reference record (frame.rs:41-60) on the oracle's tableau."""
+    cap = text.count("\n") * 64 + 64
+    out = np.zeros(cap, dtype=np.uint8)
+    m = _check(lib().oracle_frames_reference(text.encode(), seed, out.ctypes.data_as(C.POINTER(C.c_uint8)), cap))
+    return [bool(v) for v in out[:m]]
+
+
+def _frame_args(reference, seeds):
+    r = np.ascontiguousarray(np.asarray(list(reference), dtype=np.uint8))
+    sd = np.ascontiguousarray(np.asarray(list(seeds), dtype=np.uint64))
+    return r, sd
+
+
+def frame_sample_packed(text: str, reference, shots: int, seeds, threads: int = 1) -> np.ndarray:
+    """sample_packed (frame.rs:69-89) with the batch seeds given: (measurements, words) uint64."""
+    r, sd = _frame_args(reference, seeds)
+    out = np.zeros((r.size, (shots + 63) // 64), dtype=np.uint64)
+    P = C.POINTER
+    _check(lib().oracle_frames_sample_packed(text.encode(), r.ctypes.data_as(P(C.c_uint8)), r.size, shots,
+                                             sd.ctypes.data_as(P(C.c_uint64)), sd.size, threads,
+                                             out.ctypes.data_as(P(C.c_uint64))))
+    return out
+
+
+def frame_sample_detectors(text: str, reference, shots: int, seeds, num_detectors: int, num_observables: int):
+    """sample_detectors (frame.rs:155-205) with the batch seeds given."""
+    r, sd = _frame_args(reference, seeds)
+    w = (shots + 63) // 64
+    det = np.zeros((num_detectors, w), dtype=np.uint64)
+    obs = np.zeros((num_observables, w), dtype=np.uint64)
+    P = C.POINTER
+    _check(lib().oracle_frames_sample_detectors(text.encode(), r.ctypes.data_as(P(C.c_uint8)), r.size, shots,
+                                                sd.ctypes.data_as(P(C.c_uint64)), sd.size,
+                                                det.ctypes.data_as(P(C.c_uint64)), num_detectors,
+                                                obs.ctypes.data_as(P(C.c_uint64)), num_observables))
+    return det, obs

@@ -111,4 +111,19 @@ inline std::string reversible_circuit_text(size_t n, size_t gates, StdRng& rng) 
   return os.str();
 }
 
+
+// The frame-sampler benchmark of the reference (examples/bench.rs:264-294)
+inline std::string frames_circuit_text(size_t n, size_t rounds, size_t meas, double p, StdRng& rng) {
+  std::ostringstream os;
+  os << "QUBITS " << n << '\n';
+  for (size_t q = 0; q < n / 2; ++q) os << "H " << q << '\n';
+  for (size_t r = 0; r < rounds; ++r) {
+    for (size_t q = 0; q < n; q += 2) {
+      const size_t b = (q + 1 + rng.gen_range_u64(0, n - 1)) % n;
+      os << "CX " << q << ' ' << b << '\n' << "DEPOLARIZE2(" << fmt_double(p) << ") " << q << ' ' << b << '\n';
+    }
+    for (size_t k = 0; k < meas; ++k) os << "M " << rng.gen_range_u64(0, n) << '\n';
+  }
+  return os.str();
+}
 }  // namespace ref

@@ -35,7 +35,7 @@ macro_rules! opaque {
         }
     )*};
 }
-opaque!(ncsim_state, ncsim_rng, ncsim_circuit, ncsim_gate, ncsim_batch, ncsim_sparse);
+opaque!(ncsim_state, ncsim_rng, ncsim_circuit, ncsim_gate, ncsim_batch, ncsim_sparse, ncsim_frames);
 
 #[repr(C)]
 #[derive(Clone, Copy, Debug)]
@@ -207,4 +207,16 @@ extern "C" {
     pub fn ncsim_sparse_synchronize(s: *const ncsim_sparse) -> ncsim_status;
     pub fn ncsim_sparse_timer_start(s: *mut ncsim_sparse) -> ncsim_status;
     pub fn ncsim_sparse_timer_stop(s: *mut ncsim_sparse, milliseconds: *mut f64) -> ncsim_status;
+    pub fn ncsim_frames_new(c: *const ncsim_circuit, reference_seed: u64, out: *mut *mut ncsim_frames) -> ncsim_status;
+    pub fn ncsim_frames_with_reference(c: *const ncsim_circuit, reference: *const u8, m: u64, out: *mut *mut ncsim_frames) -> ncsim_status;
+    pub fn ncsim_frames_free(f: *mut ncsim_frames) -> ncsim_status;
+    pub fn ncsim_frames_info(f: *const ncsim_frames, num_qubits: *mut u32, num_measurements: *mut u64, num_detectors: *mut u64, num_observables: *mut u64, num_layers: *mut u64) -> ncsim_status;
+    pub fn ncsim_frames_reference(f: *const ncsim_frames, out: *mut u8, cap: u64) -> ncsim_status;
+    pub fn ncsim_frames_sample_packed(f: *mut ncsim_frames, shots: u64, rng: *mut ncsim_rng, out: *mut u64, cap: u64) -> ncsim_status;
+    pub fn ncsim_frames_sample_packed_seeds(f: *mut ncsim_frames, shots: u64, seeds: *const u64, nseeds: u64, out: *mut u64, cap: u64) -> ncsim_status;
+    pub fn ncsim_frames_sample_packed_device(f: *mut ncsim_frames, shots: u64, seeds: *const u64, nseeds: u64, d_out: *mut u64, cap: u64) -> ncsim_status;
+    pub fn ncsim_frames_sample(f: *mut ncsim_frames, shots: u64, rng: *mut ncsim_rng, out: *mut u64, cap: u64) -> ncsim_status;
+    pub fn ncsim_frames_sample_detectors(f: *mut ncsim_frames, shots: u64, rng: *mut ncsim_rng, det: *mut u64, det_cap: u64, obs: *mut u64, obs_cap: u64) -> ncsim_status;
+    pub fn ncsim_frames_sample_detectors_seeds(f: *mut ncsim_frames, shots: u64, seeds: *const u64, nseeds: u64, det: *mut u64, det_cap: u64, obs: *mut u64, obs_cap: u64) -> ncsim_status;
+    pub fn ncsim_frames_last_kernel_ms(f: *const ncsim_frames, ms: *mut f64) -> ncsim_status;
 }

@@ -572,3 +572,118 @@ impl Drop for TrajectoryBatch {
         }
     }
 }
+
+/// The Pauli-frame sampler on the device: the drop-in for ncsim's
+/// `FrameSampler` (src/frame.rs:34-300).  The reference record comes from
+/// ncsim's own `FrameSampler::new` (its stabilizer tableau), so the records
+/// are those of the reference for the same `reference_seed`; the batches'
+/// seeds are drawn from the caller's generator, one `next_u64` per batch of
+/// 16384 shots in order (frame.rs:72-74), and the frames run on the device.
+pub struct GpuFrameSampler {
+    h: *mut ffi::ncsim_frames,
+    reference: Vec<bool>,
+    detectors: usize,
+    observables: usize,
+}
+
+// SAFETY: the library serialises the calls made on one sampler.
+unsafe impl Send for GpuFrameSampler {}
+
+const FRAME_BATCH: usize = 1 << 14;
+
+impl GpuFrameSampler {
+    /// `FrameSampler::new` (frame.rs:41-60): Unsupported for a non-Clifford gate.
+    pub fn new(circuit: &Circuit, reference_seed: u64) -> Result<Self> {
+        let reference = ncsim::FrameSampler::new(circuit, reference_seed)?.reference().to_vec();
+        let c = CCircuit::from_circuit(circuit)?;
+        let bytes: Vec<u8> = reference.iter().map(|&b| b as u8).collect();
+        let mut h = std::ptr::null_mut();
+        // SAFETY: `bytes` holds `len` entries; `h` is a valid out pointer.
+        check(unsafe { ffi::ncsim_frames_with_reference(c.0, bytes.as_ptr(), bytes.len() as u64, &mut h) })?;
+        Ok(GpuFrameSampler {
+            h,
+            reference,
+            detectors: circuit.detectors().len(),
+            observables: circuit.observables().len(),
+        })
+    }
+
+    /// The noiseless reference record.
+    pub fn reference(&self) -> &[bool] {
+        &self.reference
+    }
+
+    fn seeds(shots: usize, rng: &mut dyn RngCore) -> Vec<u64> {
+        (0..shots.div_ceil(FRAME_BATCH)).map(|_| rng.next_u64()).collect()
+    }
+
+    fn unpack(flat: &[u64], rows: usize, shots: usize) -> Vec<Bits> {
+        let w = bits::nwords(shots);
+        (0..rows).map(|k| flat[k * w..(k + 1) * w].to_vec()).collect()
+    }
+
+    /// `sample_packed` (frame.rs:69-89): entry `k` holds measurement `k` over the shots.
+    pub fn sample_packed(&self, shots: usize, rng: &mut dyn RngCore) -> Result<Vec<Bits>> {
+        let seeds = Self::seeds(shots, rng);
+        let m = self.reference.len();
+        let mut flat = vec![0u64; m * bits::nwords(shots)];
+        // SAFETY: `seeds` and `flat` hold the lengths passed.
+        check(unsafe {
+            ffi::ncsim_frames_sample_packed_seeds(
+                self.h,
+                shots as u64,
+                seeds.as_ptr(),
+                seeds.len() as u64,
+                flat.as_mut_ptr(),
+                flat.len() as u64,
+            )
+        })?;
+        Ok(Self::unpack(&flat, m, shots))
+    }
+
+    /// `sample` (frame.rs:90-102): one record per shot (bit `k` = measurement `k`).
+    pub fn sample(&self, shots: usize, rng: &mut dyn RngCore) -> Result<Vec<Bits>> {
+        let packed = self.sample_packed(shots, rng)?;
+        let m = self.reference.len();
+        let mut out = vec![bits::zero(m); shots];
+        for (k, col) in packed.iter().enumerate() {
+            for s in bits::ones(col) {
+                if s < shots {
+                    bits::set(&mut out[s], k, true);
+                }
+            }
+        }
+        Ok(out)
+    }
+
+    /// `sample_detectors` (frame.rs:155-205): detector and observable flips, packed.
+    pub fn sample_detectors(&self, shots: usize, rng: &mut dyn RngCore) -> Result<(Vec<Bits>, Vec<Bits>)> {
+        let seeds = Self::seeds(shots, rng);
+        let w = bits::nwords(shots);
+        let mut det = vec![0u64; self.detectors * w];
+        let mut obs = vec![0u64; self.observables * w];
+        // SAFETY: `seeds`, `det` and `obs` hold the lengths passed.
+        check(unsafe {
+            ffi::ncsim_frames_sample_detectors_seeds(
+                self.h,
+                shots as u64,
+                seeds.as_ptr(),
+                seeds.len() as u64,
+                det.as_mut_ptr(),
+                det.len() as u64,
+                obs.as_mut_ptr(),
+                obs.len() as u64,
+            )
+        })?;
+        Ok((Self::unpack(&det, self.detectors, shots), Self::unpack(&obs, self.observables, shots)))
+    }
+}
+
+impl Drop for GpuFrameSampler {
+    fn drop(&mut self) {
+        // SAFETY: owned, dropped once.
+        unsafe {
+            ffi::ncsim_frames_free(self.h);
+        }
+    }
+}
