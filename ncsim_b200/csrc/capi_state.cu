@@ -112,7 +112,7 @@ bool hermitian(uint64_t x, uint64_t z, uint32_t phase) {  // src/pauli/ops.rs:25
 }  // namespace
 
 const char* kernel_class_name(int c) {
-  static const char* names[K_NUM_CLASSES] = {"dense1", "dense2", "dense_tile", "diag", "pairswap", "perm_tile",
+  static const char* names[K_NUM_CLASSES] = {"dense1", "dense2", "dense_fiber", "diag", "pairswap", "perm_tile",
                                              "phasepoly", "pauli", "norm", "expect", "inner", "project", "scale",
                                              "sample", "fused_gemm", "fused_remap", "other", "dense_wide",
                                              "perm_wide"};

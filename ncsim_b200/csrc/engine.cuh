@@ -103,7 +103,7 @@ constexpr int PARTIAL_SLOTS = 4;  // doubles per block partial
 namespace ncsim {
 // Kernel classes of the launch profiler.
 enum KernelClass : int {
-  K_DENSE1, K_DENSE2, K_DENSE_TILE, K_DIAG, K_PAIRSWAP, K_PERM_TILE, K_PHASEPOLY, K_PAULI, K_NORM, K_EXPECT,
+  K_DENSE1, K_DENSE2, K_DENSE_FIBER, K_DIAG, K_PAIRSWAP, K_PERM_TILE, K_PHASEPOLY, K_PAULI, K_NORM, K_EXPECT,
   K_INNER, K_PROJECT, K_SCALE, K_SAMPLE, K_FUSED_GEMM, K_FUSED_REMAP, K_OTHER, K_DENSE_WIDE, K_PERM_WIDE,
   K_NUM_CLASSES
 };

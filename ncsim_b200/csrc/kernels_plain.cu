@@ -189,50 +189,36 @@ __device__ __forceinline__ void tile_load_async(V<R>* tile, const V<R>* src, con
   asm volatile("cp.async.commit_group;\ncp.async.wait_group 0;\n" ::: "memory");
 }
 
-constexpr int MAX_DENSE_K = 5;  // matrices up to 32x32 travel in the kernel parameters
+constexpr int MAX_DENSE_K = 5;  // matrices up to 32x32 travel in the kernel parameters (k_dense_fiber)
 
-template <class R>
-struct DenseParams {
-  TileGeom g;
-  V<R> m[1 << (2 * MAX_DENSE_K)];
+// k = 3..5 dense gate, one fiber per thread: the fiber's 2^K amplitudes are
+// loaded into registers (all loads before any arithmetic), each output row is
+// a sum over the matrix row, and the matrix stays in the kernel parameters,
+// read with warp-uniform, compile-time addresses (the constant cache
+// broadcasts them).  In place: a thread owns its fiber.
+template <class R, int K>
+struct FiberParams {
+  uint8_t pos[K];            // gate qubits, ascending (for the zero insertion)
+  uint64_t off[1 << K];      // global offset bits of local pattern b (bit j = qubits[j])
+  V<R> m[1 << (2 * K)];      // row-major
 };
 
-template <class R>
-__global__ void __launch_bounds__(THREADS) k_dense_tile(V<R>* __restrict__ a, uint64_t ntiles, const __grid_constant__ DenseParams<R> P) {
-  extern __shared__ __align__(16) unsigned char smem_raw[];
-  const TileGeom& g = P.g;
-  const int gd = 1 << g.k;
-  const uint32_t tsz = 1u << g.T;
-  V<R>* tile = reinterpret_cast<V<R>*>(smem_raw);
-  V<R>* mat = tile + tsz;
-  uint32_t* pat = reinterpret_cast<uint32_t*>(mat + gd * gd);
-  for (int i = threadIdx.x; i < gd * gd; i += blockDim.x) mat[i] = P.m[i];
-  for (int b = threadIdx.x; b < gd; b += blockDim.x) {
-    uint32_t o = 0;
-    for (int j = 0; j < g.k; ++j) o |= ((uint32_t(b) >> j) & 1u) << g.pos[j];
-    pat[b] = o;
-  }
-  __shared__ uint64_t roff[32];
-  __shared__ uint32_t rx[32];
-  const TileRounds tr = tile_rounds(g, roff, rx);
-  uint32_t gtile = 0;
-  for (int j = 0; j < g.k; ++j) gtile |= 1u << g.pos[j];
-  for (uint64_t t = blockIdx.x; t < ntiles; t += gridDim.x) {
-    V<R>* amp = a + (tile_base(t, g) | tr.toff);
-    __syncthreads();
-    tile_load_async<R>(tile, amp, roff, tr.nr, tsz);
-    __syncthreads();
-    for (uint32_t q = 0; q < tr.nr; ++q) {
-      const uint32_t e = threadIdx.x + q * blockDim.x;
-      if (e >= tsz) break;
-      const uint32_t row = tr.tx | rx[q];
-      const uint32_t r = e & ~gtile;
-      const V<R>* mr = mat + row * gd;
-      V<R> acc;
-      acc.x = 0;
-      acc.y = 0;
-      for (int b = 0; b < gd; ++b) acc = cfma(mr[b], tile[r | pat[b]], acc);
-      amp[roff[q]] = acc;
+template <class R, int K>
+__global__ void __launch_bounds__(THREADS) k_dense_fiber(V<R>* __restrict__ a, uint64_t nfib,
+                                                         const __grid_constant__ FiberParams<R, K> P) {
+  constexpr int D = 1 << K;
+  const uint64_t stride = uint64_t(gridDim.x) * blockDim.x;
+  for (uint64_t f = uint64_t(blockIdx.x) * blockDim.x + threadIdx.x; f < nfib; f += stride) {
+    const uint64_t base = insert_zeros(f, P.pos, K);
+    V<R> v[D];
+#pragma unroll
+    for (int b = 0; b < D; ++b) v[b] = a[base | P.off[b]];
+#pragma unroll
+    for (int r = 0; r < D; ++r) {
+      V<R> acc = cmul(P.m[r * D], v[0]);
+#pragma unroll
+      for (int b = 1; b < D; ++b) acc = cfma(P.m[r * D + b], v[b], acc);
+      a[base | P.off[r]] = acc;
     }
   }
 }
@@ -578,14 +564,25 @@ __global__ void __launch_bounds__(THREADS) k_phasepoly_sliced(V<R>* __restrict__
 // ---------------------------------------------------------------------------
 // Pauli i^ph X^x Z^z (vector.rs:143-164)
 // ---------------------------------------------------------------------------
+// Four grid-stride steps per iteration, their loads issued together: the
+// amplitudes whose phase is 1 are neither read nor written, so a thread has
+// about half as many loads in flight as indices it visits.
 template <class R>
 __global__ void __launch_bounds__(THREADS) k_pauli_diag(V<R>* __restrict__ a, uint64_t len, uint64_t z, int ph) {
+  constexpr int U = 4;
   const uint64_t stride = uint64_t(gridDim.x) * blockDim.x;
-  for (uint64_t c = uint64_t(blockIdx.x) * blockDim.x + threadIdx.x; c < len; c += stride) {
-    int k = (ph + 2 * __popcll(z & c)) & 3;
-    if (k == 0) continue;
-    V<R> v = a[c];
-    if (!is_zero(v)) a[c] = ipow_mul(k, v);
+  for (uint64_t c0 = uint64_t(blockIdx.x) * blockDim.x + threadIdx.x; c0 < len; c0 += U * stride) {
+    V<R> v[U];
+    int k[U];
+#pragma unroll
+    for (int u = 0; u < U; ++u) {
+      const uint64_t c = c0 + u * stride;
+      k[u] = c < len ? (ph + 2 * __popcll(z & c)) & 3 : 0;
+      if (k[u]) v[u] = a[c];
+    }
+#pragma unroll
+    for (int u = 0; u < U; ++u)
+      if (k[u] && !is_zero(v[u])) a[c0 + u * stride] = ipow_mul(k[u], v[u]);
   }
 }
 
@@ -1056,18 +1053,37 @@ void launch_dense(ncsim_state* s, const std::vector<uint32_t>& qubits, const std
     launch_dense_wide(s, qubits, m);
     return;
   }
-  NCSIM_DISPATCH(s, {
-    auto* P = new DenseParams<R>();
-    P->g = make_geom(s->n, qubits, tile_bits_for<R>(s->n, k));
-    for (int i = 0; i < gd * gd; ++i) P->m[i] = cv<R>(m[i]);
-    uint64_t ntiles = len >> P->g.T;
-    size_t smem = (size_t(1) << P->g.T) * sizeof(V<R>) + size_t(gd) * gd * sizeof(V<R>) + gd * sizeof(uint32_t);
-    cudaFuncSetAttribute(k_dense_tile<R>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
-    ProfScope ps(s, K_DENSE_TILE, full_bytes(s));
-    k_dense_tile<R><<<grid_for(ntiles, 1, 1, 8), THREADS, smem, s->stream>>>(amp_of<R>(s), ntiles, *P);
-    delete P;
-  });
-  NCSIM_LAUNCHED("dense_tile");
+  auto fiber = [&](auto tagR, auto tagK) {
+    using R = decltype(tagR);
+    constexpr int K = decltype(tagK)::value;
+    FiberParams<R, K> P{};
+    std::vector<uint32_t> sq(qubits.begin(), qubits.end());
+    std::sort(sq.begin(), sq.end());
+    for (int j = 0; j < K; ++j) P.pos[j] = uint8_t(sq[j]);
+    for (int b = 0; b < (1 << K); ++b) {
+      uint64_t o = 0;
+      for (int j = 0; j < K; ++j)
+        if ((b >> j) & 1) o |= uint64_t(1) << qubits[j];
+      P.off[b] = o;
+    }
+    for (int i = 0; i < (1 << (2 * K)); ++i) P.m[i] = cv<R>(m[i]);
+    const uint64_t nfib = len >> K;
+    ProfScope ps(s, K_DENSE_FIBER, full_bytes(s));
+    k_dense_fiber<R, K><<<grid_for(nfib, THREADS), THREADS, 0, s->stream>>>(amp_of<R>(s), nfib, P);
+  };
+  using K3 = std::integral_constant<int, 3>;
+  using K4 = std::integral_constant<int, 4>;
+  using K5 = std::integral_constant<int, 5>;
+  if (s->precision == NCSIM_C128) {
+    if (k == 3) fiber(double(), K3());
+    else if (k == 4) fiber(double(), K4());
+    else fiber(double(), K5());
+  } else {
+    if (k == 3) fiber(float(), K3());
+    else if (k == 4) fiber(float(), K4());
+    else fiber(float(), K5());
+  }
+  NCSIM_LAUNCHED("dense_fiber");
 }
 
 void launch_diag_table(ncsim_state* s, const std::vector<uint32_t>& qubits, const std::vector<CplxD>& diag) {

@@ -33,6 +33,7 @@ def cases(n: int):
     h, cx, cz, rz = Gate.parse("H"), Gate.parse("CX"), Gate.parse("CZ"), Gate.parse("RZ(0.3)")
     ccx = Gate.parse("CCX")
     u2, u3, u6 = _unitary(2, 1), _unitary(3, 2), _unitary(6, 3)
+    u4, u5 = _unitary(4, 4), _unitary(5, 6)
     r = np.random.default_rng(5)
     perm6 = r.permutation(64)
     ph6 = np.exp(2j * np.pi * r.integers(0, 8, 64) / 8)
@@ -43,7 +44,9 @@ def cases(n: int):
         ("dense1", lambda s: s.apply_gate(h, [n - 3])),
         ("dense1_low", lambda s: s.apply_gate(h, [0])),
         ("dense2", lambda s: s.apply_matrix(u2, [3, n - 5])),
-        ("dense_tile", lambda s: s.apply_matrix(u3, [2, 9, n - 4])),
+        ("dense_fiber3", lambda s: s.apply_matrix(u3, [2, 9, n - 4])),
+        ("dense_fiber4", lambda s: s.apply_matrix(u4, [0, 6, 13, n - 3])),
+        ("dense_fiber5", lambda s: s.apply_matrix(u5, [1, 4, 10, 16, n - 1])),
         ("dense_wide", lambda s: s.apply_matrix(u6, [1, 5, 8, 12, 17, n - 2])),
         ("diag_const", lambda s: s.apply_gate(cz, [4, n - 6])),
         ("diag_1q", lambda s: s.apply_gate(rz, [n - 7])),
@@ -57,7 +60,8 @@ def cases(n: int):
         ("norm", lambda s: s.norm_sq()),
         ("expect_diag", lambda s: s.expectation(Pauli(n, 0, (1 << 1) | (1 << (n - 1)), 0))),
         ("expect_pair", lambda s: s.expectation(Pauli(n, (1 << 4) | (1 << (n - 2)), 1 << 7, 0))),
-        ("project_diag", lambda s: s.project(Pauli(n, 0, 1 << (n - 4), 0), False)),
+        # the projection zeroes half the register; H on that qubit makes it dense again (a dense1 line)
+        ("project_diag", lambda s: (s.project(Pauli(n, 0, 1 << (n - 4), 0), False), s.apply_gate(h, [n - 4]))),
         ("project_pair", lambda s: s.project(Pauli(n, 1 << (n - 5), 0, 0), False)),
         ("sample", lambda s: s.sample(StdRng(3), 1024)),
     ]
