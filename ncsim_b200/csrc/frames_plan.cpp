@@ -407,6 +407,138 @@ NoiseChannel channel_of(const NoiseIR& nz) {  // Noise::errors (circuit.rs:119-1
   return ch;
 }
 
+constexpr uint64_t K_END = uint64_t(1) << 53;  // draws are k 2^-53 with k < 2^53
+
+// the reference's expressions, as functions of the draw's 53 bits
+inline double skip_of(uint64_t k, double l) {
+  const double u = double(k) * 0x1.0p-53;
+  return std::floor(std::log(1.0 - u) / l);
+}
+inline uint32_t pick_of(uint64_t k, const NoiseChannel& ch) {
+  double u = double(k) * 0x1.0p-53 * ch.total;
+  for (uint32_t i = 0; i < ch.p.size(); ++i) {
+    if (u < ch.p[i]) return i;
+    u -= ch.p[i];
+  }
+  return uint32_t(ch.p.size() - 1);
+}
+
+// least k in [lo, K_END] with pred(k) (pred monotone: false ... false true ... true)
+template <class Pred>
+uint64_t least_true(uint64_t lo, uint64_t guess, Pred pred) {
+  guess = std::min(std::max(guess, lo), K_END - 1);
+  uint64_t a, b;  // pred(a) false (or a = lo - 1), pred(b) true (or b = K_END)
+  if (pred(guess)) {
+    b = guess;
+    uint64_t step = 1;
+    for (;;) {
+      if (b - lo < step) {
+        a = lo;
+        if (pred(a)) return a;
+        break;
+      }
+      const uint64_t c = b - step;
+      if (!pred(c)) {
+        a = c;
+        break;
+      }
+      b = c;
+      step *= 2;
+    }
+  } else {
+    a = guess;
+    uint64_t step = 1;
+    for (;;) {
+      if (K_END - 1 - a < step) {
+        b = K_END - 1;
+        if (!pred(b)) return K_END;
+        break;
+      }
+      const uint64_t c = a + step;
+      if (pred(c)) {
+        b = c;
+        break;
+      }
+      a = c;
+      step *= 2;
+    }
+  }
+  while (b - a > 1) {
+    const uint64_t m = a + (b - a) / 2;
+    if (pred(m)) b = m;
+    else a = m;
+  }
+  return b;
+}
+
+constexpr uint64_t CHECK_SIDE = 3;  // k checked on each side of every step
+
+std::shared_ptr<const SkipTable> build_skip(double p) {
+  auto t = std::make_shared<SkipTable>();
+  t->l = std::log(1.0 - p);
+  const double l = t->l;
+  t->thr.assign(BATCH + 1, K_END);
+  t->thr[0] = 0;
+  for (uint32_t g = 1; g <= BATCH; ++g) {
+    const uint64_t lo = t->thr[g - 1];
+    if (lo >= K_END) break;
+    const double approx = -std::expm1(double(g) * l) * 0x1.0p53;
+    const uint64_t guess = approx >= 0x1.0p53 ? K_END - 1 : uint64_t(approx);
+    const uint64_t k = least_true(lo, guess, [&](uint64_t x) { return skip_of(x, l) >= double(g); });
+    t->thr[g] = k;
+    if (k >= K_END) break;
+    for (uint64_t j = 1; j <= CHECK_SIDE; ++j) {
+      if (k >= j && k - j >= lo && skip_of(k - j, l) >= double(g)) return nullptr;
+      if (k + j - 1 < K_END && skip_of(k + j - 1, l) < double(g)) return nullptr;
+    }
+  }
+  t->bucket.resize(size_t(1) << 16);
+  uint32_t g = 0;
+  for (uint64_t b = 0; b < t->bucket.size(); ++b) {
+    const uint64_t k = b << 37;
+    while (g < BATCH && t->thr[g + 1] <= k) ++g;
+    t->bucket[b] = uint16_t(g);
+  }
+  return t;
+}
+
+std::shared_ptr<const PickTable> build_pick(const NoiseChannel& ch) {
+  auto t = std::make_shared<PickTable>();
+  uint64_t lo = 0;
+  for (uint32_t i = 0; i + 1 < ch.p.size(); ++i) {
+    const uint64_t k = least_true(lo, lo, [&](uint64_t x) { return pick_of(x, ch) > i; });
+    for (uint64_t j = 1; j <= CHECK_SIDE; ++j) {
+      if (k >= j && k - j >= lo && pick_of(k - j, ch) > i) return nullptr;
+      if (k + j - 1 < K_END && pick_of(k + j - 1, ch) <= i) return nullptr;
+    }
+    t->thr.push_back(k);
+    lo = std::min(k, K_END - 1);
+  }
+  return t;
+}
+
+// tables for the channels used often enough to repay them (one per distinct
+// probability list, shared by the channel's ops)
+void attach_tables(std::vector<NoiseChannel>& noise) {
+  std::map<std::vector<double>, std::pair<size_t, std::vector<size_t>>> uses;
+  for (size_t i = 0; i < noise.size(); ++i) {
+    auto& u = uses[noise[i].p];
+    u.second.push_back(i);
+  }
+  for (auto& kv : uses) {
+    const auto& idx = kv.second.second;
+    if (idx.size() < 64) continue;
+    const NoiseChannel& ch = noise[idx[0]];
+    if (!(ch.total > 0.0)) continue;
+    std::shared_ptr<const SkipTable> skip = ch.total < 0.25 ? build_skip(ch.total) : nullptr;
+    std::shared_ptr<const PickTable> pick = build_pick(ch);
+    for (size_t i : idx) {
+      noise[i].skip = skip;
+      noise[i].pick = pick;
+    }
+  }
+}
+
 }  // namespace
 
 Program compile(const ncsim_circuit& c, const std::vector<uint8_t>& reference) {
@@ -524,6 +656,7 @@ Program compile(const ncsim_circuit& c, const std::vector<uint8_t>& reference) {
     }
   }
   P.num_masks = mask;
+  attach_tables(P.noise);
   auto flip_of = [&](const std::vector<uint64_t>& idx) {
     uint32_t f = 0;
     for (uint64_t j : idx) f ^= reference[j];
@@ -558,10 +691,75 @@ void key_of_seed(uint64_t seed, uint32_t key[8]) {
   for (int i = 0; i < 8; ++i) key[i] = r.key[i];
 }
 
+namespace {
+
+// Random access into a StdRng key stream: ChaCha12 blocks (the same block
+// function as the host generator, host/rng.hpp) computed four at a time in
+// the lanes of 128-bit vectors, starting at the block a read needs.  A noise
+// channel's draws sit between masks the scan skips, so the stream is read in
+// short runs at scattered positions.
+struct KeyStream {
+  typedef uint32_t v4 __attribute__((vector_size(16)));
+  uint32_t key[8];
+  uint64_t first = ~uint64_t(0) - 3;  // block index of buf[0..15] (none loaded yet: above every index)
+  uint32_t buf[64];
+  uint64_t pos = 0;                // u32 index of the next draw
+
+  static inline v4 rl(v4 v, int s) { return (v << s) | (v >> (32 - s)); }
+  void load(uint64_t b) {
+    v4 x[16], in[16];
+    const uint32_t c[4] = {0x61707865u, 0x3320646eu, 0x79622d32u, 0x6b206574u};
+    for (int i = 0; i < 4; ++i) in[i] = v4{c[i], c[i], c[i], c[i]};
+    for (int i = 0; i < 8; ++i) in[4 + i] = v4{key[i], key[i], key[i], key[i]};
+    for (int l = 0; l < 4; ++l) {
+      in[12][l] = uint32_t(b + l);
+      in[13][l] = uint32_t((b + l) >> 32);
+      in[14][l] = 0;
+      in[15][l] = 0;
+    }
+    for (int i = 0; i < 16; ++i) x[i] = in[i];
+#define NCSIM_VQR(a, b, c, d)                  \
+  x[a] += x[b], x[d] = rl(x[d] ^ x[a], 16);    \
+  x[c] += x[d], x[b] = rl(x[b] ^ x[c], 12);    \
+  x[a] += x[b], x[d] = rl(x[d] ^ x[a], 8);     \
+  x[c] += x[d], x[b] = rl(x[b] ^ x[c], 7)
+    for (int dr = 0; dr < 6; ++dr) {
+      NCSIM_VQR(0, 4, 8, 12);
+      NCSIM_VQR(1, 5, 9, 13);
+      NCSIM_VQR(2, 6, 10, 14);
+      NCSIM_VQR(3, 7, 11, 15);
+      NCSIM_VQR(0, 5, 10, 15);
+      NCSIM_VQR(1, 6, 11, 12);
+      NCSIM_VQR(2, 7, 8, 13);
+      NCSIM_VQR(3, 4, 9, 14);
+    }
+#undef NCSIM_VQR
+    for (int i = 0; i < 16; ++i) {
+      const v4 o = x[i] + in[i];
+      for (int l = 0; l < 4; ++l) buf[16 * l + i] = o[l];
+    }
+    first = b;
+  }
+  // next_u64 and gen::<f64>() at the current position: a u64 draw reads two
+  // consecutive words, and every draw of a frame batch is a u64 (masks and
+  // gen::<f64>()), so positions stay even and a draw never straddles a block
+  inline uint64_t u64() {
+    const uint64_t b = pos >> 4;
+    if (b < first || b >= first + 4) load(b);
+    const uint32_t* w = buf + 16 * (b - first) + (pos & 15);
+    pos += 2;
+    return uint64_t(w[0]) | (uint64_t(w[1]) << 32);
+  }
+  inline double f64() { return double(u64() >> 11) * 0x1.0p-53; }
+};
+
+}  // namespace
+
 void scan_batch(const Program& p, uint64_t seed, uint32_t shots, BatchScan& out) {
   const uint64_t words = (uint64_t(shots) + 63) / 64;
-  ncsim_rng rng(seed);
-  uint64_t pos = 0;  // u32 position of the next draw
+  KeyStream rng;
+  key_of_seed(seed, rng.key);
+  uint64_t& pos = rng.pos;  // u32 position of the next draw
   out.mask_pos.assign(p.num_masks, 0);
   out.ev_off.assign(p.noise.size() + 1, 0);
   out.events.clear();
@@ -577,10 +775,20 @@ void scan_batch(const Program& p, uint64_t seed, uint32_t shots, BatchScan& out)
     // hits (frame.rs:241-266)
     hits.clear();
     if (total > 0.0) {
-      rng.seek(pos);
       if (total >= 0.25) {
         for (uint32_t s = 0; s < shots; ++s)
           if (rng.f64() < total) hits.push_back(s);
+      } else if (ch.skip) {
+        const SkipTable& t = *ch.skip;
+        uint32_t s = 0;
+        for (;;) {
+          const uint32_t gap = t.at(rng.u64() >> 11);
+          if (gap >= shots - s) break;
+          s += gap;
+          hits.push_back(s);
+          s += 1;
+          if (s >= shots) break;
+        }
       } else {
         const double l = std::log(1.0 - total);
         uint64_t s = 0;
@@ -596,18 +804,10 @@ void scan_batch(const Program& p, uint64_t seed, uint32_t shots, BatchScan& out)
       }
       // which error, given that one happened (frame.rs:270-280)
       for (uint32_t s : hits) {
-        double u = rng.f64() * total;
-        size_t pick = ch.p.size() - 1;
-        for (size_t i = 0; i < ch.p.size(); ++i) {
-          if (u < ch.p[i]) {
-            pick = i;
-            break;
-          }
-          u -= ch.p[i];
-        }
+        const uint64_t k = rng.u64() >> 11;
+        const uint32_t pick = ch.pick ? ch.pick->at(k) : pick_of(k, ch);
         out.events.push_back(s | (uint32_t(ch.x[pick]) << 16) | (uint32_t(ch.z[pick]) << 20));
       }
-      pos = rng.position();
     }
     out.ev_off[d.second + 1] = uint32_t(out.events.size());
   }

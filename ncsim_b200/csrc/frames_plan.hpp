@@ -6,6 +6,7 @@
 #pragma once
 
 #include <cstdint>
+#include <memory>
 #include <vector>
 
 #include "host/ir.hpp"
@@ -64,10 +65,43 @@ struct FrameOp {
   uint32_t off;   // into the pool
 };
 
+// The two decisions a noise channel takes from a draw u = k 2^-53 (k the
+// draw's top 53 bits) as step tables over k.  Each decision is a monotone
+// function of k: the geometric skip floor(ln(1 - u) / ln(1 - p)) (frame.rs:252)
+// and the error picked by subtracting the probabilities from u * total in
+// order (frame.rs:273-282).  A table lists the least k at which the decision
+// steps up, found with the same floating-point expressions the reference
+// evaluates (so the same log), and checked for monotonicity a few k on each
+// side of every step; a channel whose check fails keeps the direct evaluation.
+struct SkipTable {
+  double l = 0.0;                 // ln(1 - p)
+  std::vector<uint64_t> thr;      // thr[g]: least k with skip >= g (g = 0..BATCH; 2^53 when none)
+  std::vector<uint16_t> bucket;   // the skip at k = b << 37 for each of the 2^16 buckets b
+  uint32_t at(uint64_t k) const {
+    uint32_t g = bucket[k >> 37];
+    while (g < BATCH && thr[g + 1] <= k) ++g;
+    return g;
+  }
+};
+struct PickTable {
+  std::vector<uint64_t> thr;      // thr[i]: least k with pick > i
+  // starts from the pick of equal probabilities and walks to the step that holds k
+  uint32_t at(uint64_t k) const {
+    const uint32_t e = uint32_t(thr.size());
+    uint32_t i = uint32_t((unsigned __int128)k * (e + 1) >> 53);
+    if (i > e) i = e;
+    while (i > 0 && thr[i - 1] > k) --i;
+    while (i < e && thr[i] <= k) ++i;
+    return i;
+  }
+};
+
 struct NoiseChannel {
   std::vector<double> p;       // errors(): probabilities in order (circuit.rs:119-128)
   std::vector<uint8_t> x, z;   // local error bits
   double total = 0.0;          // their sum, left to right
+  std::shared_ptr<const SkipTable> skip;  // null: evaluate the skips directly
+  std::shared_ptr<const PickTable> pick;  // null: evaluate the picks directly
 };
 
 struct Program {

@@ -57,6 +57,26 @@ def test_per_shot_records_and_detectors_match_oracle(nb, oracle):
         assert np.array_equal(det, wd) and np.array_equal(obs, wo), text
 
 
+def test_channels_used_often_match_oracle(nb, oracle):
+    """Channels used on 64 or more ops draw their skips and picks from exact step
+    tables (zero probabilities, p >= 0.25 and the two-qubit channel included)."""
+    r = random.Random(8)
+    n = 24
+    chans1 = ["X_ERROR(0.1)", "DEPOLARIZE1(0.05)", "PAULI_CHANNEL_1(0.02,0,0.07)", "Z_ERROR(0.4)", "Y_ERROR(0.001)"]
+    lines = [f"QUBITS {n}"] + [f"H {q}" for q in range(0, n, 3)]
+    for _ in range(900):
+        a, b = r.sample(range(n), 2)
+        lines.append(f"CX {a} {b}")
+        lines.append(f"{r.choice(chans1)} {a}")
+        lines.append(f"DEPOLARIZE2({r.choice([0.003, 0.3])}) {a} {b}")
+        if r.random() < 0.2:
+            lines.append(f"M {r.randrange(n)}")
+    text = "\n".join(lines) + "\n"
+    for shots in (5000, 40000):
+        _, got, want = _both(nb, oracle, text, shots, 2, 3 + shots)
+        assert np.array_equal(got, want)
+
+
 def test_tables_in_global_memory_match_oracle(nb, oracle):
     """13 000 qubits: 16 n bytes per shot-word exceed the shared-memory budget."""
     n = 13000
