@@ -221,6 +221,11 @@ typedef struct ncsim_kernel_stat {
   double milliseconds;
   double bytes;
 } ncsim_kernel_stat;
+/* Runs of 16 or more consecutive gates in ncsim_sv_run go through tiled passes
+ * (on by default): a pass applies a run's gates to 4096-amplitude tiles in
+ * shared memory, one HBM read and write for many gates, each gate with the
+ * arithmetic of its own kernel (the amplitudes equal the gate-by-gate ones). */
+ncsim_status ncsim_sv_set_tile_passes(ncsim_state* s, int32_t enable);
 ncsim_status ncsim_sv_profile_enable(ncsim_state* s, int32_t enable);
 ncsim_status ncsim_sv_profile_read(ncsim_state* s, ncsim_kernel_stat* out, uint32_t cap, uint32_t* count);
 

@@ -172,6 +172,7 @@ _SIGNATURES = {
     "ncsim_sparse_synchronize": (_i32, [_vp]),
     "ncsim_sparse_timer_start": (_i32, [_vp]),
     "ncsim_sparse_timer_stop": (_i32, [_vp, _P(_dbl)]),
+    "ncsim_sv_set_tile_passes": (_i32, [_vp, _i32]),
     "ncsim_frames_new": (_i32, [_vp, _u64, _P(_vp)]),
     "ncsim_frames_with_reference": (_i32, [_vp, _P(C.c_uint8), _u64, _P(_vp)]),
     "ncsim_frames_free": (_i32, [_vp]),
@@ -750,6 +751,10 @@ class GpuStateVector:
         }
 
     # ---- launch profiler (CUDA events on the state's stream) ----
+    def set_tile_passes(self, enable: bool = True) -> None:
+        """Runs of gates through tiled passes (default) or gate by gate."""
+        _check(lib().ncsim_sv_set_tile_passes(self._h, int(enable)))
+
     def profile(self, enable: bool = True) -> None:
         """Start (clearing earlier records) or stop per-launch event timing."""
         _check(lib().ncsim_sv_profile_enable(self._h, int(enable)))

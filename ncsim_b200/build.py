@@ -19,6 +19,7 @@ SOURCES = [
     "csrc/capi_state.cu",
     "csrc/kernels_plain.cu",
     "csrc/wide.cu",
+    "csrc/plain_pass.cu",
     "csrc/fused.cu",
     "csrc/fused_plan.cpp",
     "csrc/batch.cu",

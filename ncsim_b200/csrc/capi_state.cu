@@ -115,7 +115,7 @@ const char* kernel_class_name(int c) {
   static const char* names[K_NUM_CLASSES] = {"dense1", "dense2", "dense_fiber", "diag", "pairswap", "perm_tile",
                                              "phasepoly", "pauli", "norm", "expect", "inner", "project", "scale",
                                              "sample", "fused_gemm", "fused_remap", "other", "dense_wide",
-                                             "perm_wide"};
+                                             "perm_wide", "plain_pass"};
   return (c >= 0 && c < K_NUM_CLASSES) ? names[c] : "other";
 }
 
@@ -821,6 +821,14 @@ ncsim_status ncsim_sv_compare(const ncsim_state* a, const ncsim_state* b, double
     if (na) *na = v[2];
     if (nb) *nb = v[3];
     if (maxdiff) *maxdiff = *std::max_element(mx.begin(), mx.end());
+  });
+}
+
+ncsim_status ncsim_sv_set_tile_passes(ncsim_state* s, int32_t enable) {
+  return guarded([&] {
+    if (!s) throw Error(NCSIM_ERR_INVALID, "null state");
+    std::lock_guard<std::recursive_mutex> lk(s->mu);
+    s->tile_passes = enable != 0;
   });
 }
 

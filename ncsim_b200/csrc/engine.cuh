@@ -105,7 +105,7 @@ namespace ncsim {
 enum KernelClass : int {
   K_DENSE1, K_DENSE2, K_DENSE_FIBER, K_DIAG, K_PAIRSWAP, K_PERM_TILE, K_PHASEPOLY, K_PAULI, K_NORM, K_EXPECT,
   K_INNER, K_PROJECT, K_SCALE, K_SAMPLE, K_FUSED_GEMM, K_FUSED_REMAP, K_OTHER, K_DENSE_WIDE, K_PERM_WIDE,
-  K_NUM_CLASSES
+  K_PLAIN_PASS, K_NUM_CLASSES
 };
 const char* kernel_class_name(int c);
 struct ProfRecord {
@@ -132,6 +132,7 @@ struct ncsim_state {
   mutable std::vector<cudaEvent_t> prof_pool;
   cudaEvent_t timer0 = nullptr, timer1 = nullptr;
   uint64_t uid = 0;  // unique over the process: keys the circuits' captured gate graphs
+  bool tile_passes = true;  // runs of gates go through tiled passes (plain_pass.cu)
 
   size_t elem_bytes() const { return precision == NCSIM_C128 ? 16 : 8; }
   size_t bytes() const { return size_t(len) * elem_bytes(); }
@@ -158,11 +159,30 @@ template <class R> struct VecOf;
 template <> struct VecOf<double> { using T = double2; };
 template <> struct VecOf<float> { using T = float2; };
 
+// Products and sums with a fixed rounding sequence (no contraction left to the
+// compiler): every kernel that applies a gate computes the same bits for it,
+// whichever kernel that is (the gate-by-gate kernels and the tiled passes).
+#ifdef __CUDA_ARCH__
+__device__ __forceinline__ double mul_rn(double a, double b) { return __dmul_rn(a, b); }
+__device__ __forceinline__ float mul_rn(float a, float b) { return __fmul_rn(a, b); }
+__device__ __forceinline__ double fma_rn(double a, double b, double c) { return __fma_rn(a, b, c); }
+__device__ __forceinline__ float fma_rn(float a, float b, float c) { return __fmaf_rn(a, b, c); }
+__device__ __forceinline__ double add_rn(double a, double b) { return __dadd_rn(a, b); }
+__device__ __forceinline__ float add_rn(float a, float b) { return __fadd_rn(a, b); }
+#else
+inline double mul_rn(double a, double b) { return a * b; }
+inline float mul_rn(float a, float b) { return a * b; }
+inline double fma_rn(double a, double b, double c) { return __builtin_fma(a, b, c); }
+inline float fma_rn(float a, float b, float c) { return __builtin_fmaf(a, b, c); }
+inline double add_rn(double a, double b) { return a + b; }
+inline float add_rn(float a, float b) { return a + b; }
+#endif
+
 template <class V>
 __host__ __device__ __forceinline__ V cmul(V a, V b) {
   V r;
-  r.x = a.x * b.x - a.y * b.y;
-  r.y = a.x * b.y + a.y * b.x;
+  r.x = fma_rn(a.x, b.x, -mul_rn(a.y, b.y));
+  r.y = fma_rn(a.x, b.y, mul_rn(a.y, b.x));
   return r;
 }
 template <class V>
@@ -175,8 +195,8 @@ __host__ __device__ __forceinline__ V cadd(V a, V b) {
 template <class V>
 __host__ __device__ __forceinline__ V cfma(V m, V x, V acc) {  // acc + m*x
   V r;
-  r.x = acc.x + (m.x * x.x - m.y * x.y);
-  r.y = acc.y + (m.x * x.y + m.y * x.x);
+  r.x = add_rn(acc.x, fma_rn(m.x, x.x, -mul_rn(m.y, x.y)));
+  r.y = add_rn(acc.y, fma_rn(m.x, x.y, mul_rn(m.y, x.x)));
   return r;
 }
 template <class V>

@@ -15,6 +15,12 @@ namespace ncsim {
 
 PolyTerms build_poly_terms(const PhasePolyIR& p, const std::vector<uint32_t>& qubits, const Phase& scalar);
 
+struct PlainPlan;
+std::shared_ptr<PlainPlan> plan_plain_passes(uint32_t n, int precision, const std::vector<const LoweredOp*>& gates);
+void run_plain_plan(ncsim_state* s, PlainPlan& P);
+size_t plain_plan_passes(const PlainPlan& P);
+size_t plain_plan_pass_gates(const PlainPlan& P);
+
 void apply_lowered(ncsim_state* s, const LoweredOp& op) {
   switch (op.kind) {
     case LoweredKind::Nothing: return;
@@ -296,8 +302,11 @@ namespace {
 // noisy trajectory drawn for one run) launches its kernels directly and pays
 // no capture.  Measurements, resets and
 // noise stay outside the graphs (their draws and decisions are made on the
-// host).  Not used while the launch profiler records per-launch events, nor
-// when the environment sets NCSIM_NO_GATE_GRAPHS (kernel-by-kernel launches).
+// host).  A run's gates go through tiled passes (plain_pass.cu) unless the
+// state turns them off or the environment sets NCSIM_NO_TILE_PASSES.  No graph
+// is captured while the launch profiler records per-launch events; the
+// environment variable NCSIM_NO_GATE_GRAPHS turns runs off altogether
+// (kernel-by-kernel launches).
 constexpr size_t MIN_GRAPH_GATES = 16;
 
 struct GateGraphs {
@@ -307,6 +316,9 @@ struct GateGraphs {
   std::vector<cudaGraphExec_t> exec;            // null until captured
   std::vector<char> seen;                       // the run has been launched directly once
   std::vector<char> failed;                     // capture did not succeed: launch directly
+  std::vector<std::shared_ptr<PlainPlan>> plans;  // tiled passes of each run (null: gate by gate)
+  std::vector<char> planned;
+  std::vector<char> plan_on;                    // the state's pass setting the plan was made under
   ~GateGraphs() {
     for (auto e : exec)
       if (e) cudaGraphExecDestroy(e);
@@ -340,20 +352,57 @@ std::shared_ptr<GateGraphs> gate_graphs_for(const ncsim_circuit* c, const ncsim_
   g->exec.assign(g->runs.size(), nullptr);
   g->seen.assign(g->runs.size(), 0);
   g->failed.assign(g->runs.size(), 0);
+  g->plans.assign(g->runs.size(), nullptr);
+  g->planned.assign(g->runs.size(), 0);
+  g->plan_on.assign(g->runs.size(), 0);
   c->gate_graphs = g;
   return g;
+}
+
+// the gates of run k: through its tiled passes when the state uses them
+void launch_run(ncsim_state* s, const ncsim_circuit* c, GateGraphs& g, size_t k) {
+  const auto [first, end] = g.runs[k];
+  if (g.plans[k]) {
+    run_plain_plan(s, *g.plans[k]);
+    return;
+  }
+  for (size_t i = first; i < end; ++i)
+    if (c->ops[i].kind == OpKind::Gate) apply_lowered(s, c->ops[i].lowered);
 }
 
 // Launches the gates of ops[first, end) on the state's stream, as a graph when it can.
 void run_gates(ncsim_state* s, const ncsim_circuit* c, GateGraphs& g, size_t k) {
   const auto [first, end] = g.runs[k];
+  static const bool passes_off = std::getenv("NCSIM_NO_TILE_PASSES") != nullptr;
+  const bool want = s->tile_passes && !passes_off;
+  if (!g.planned[k] || bool(g.plan_on[k]) != want) {
+    // a new plan drops the graph captured under the other setting
+    if (g.exec[k]) {
+      cudaGraphExecDestroy(g.exec[k]);
+      g.exec[k] = nullptr;
+    }
+    g.plans[k] = nullptr;
+    if (want) {
+      std::vector<const LoweredOp*> gates;
+      for (size_t i = first; i < end; ++i)
+        if (c->ops[i].kind == OpKind::Gate) gates.push_back(&c->ops[i].lowered);
+      g.plans[k] = plan_plain_passes(s->n, s->precision, gates);
+    }
+    g.planned[k] = 1;
+    g.plan_on[k] = want ? 1 : 0;
+    g.seen[k] = 0;
+    g.failed[k] = 0;
+  }
+  if (s->prof) {  // the launch profiler times every launch: no graph
+    launch_run(s, c, g, k);
+    return;
+  }
   if (!g.exec[k] && !g.failed[k] && g.seen[k]) {
     cudaGraph_t graph = nullptr;
     bool ok = cudaStreamBeginCapture(s->stream, cudaStreamCaptureModeThreadLocal) == cudaSuccess;
     if (ok) {
       try {
-        for (size_t i = first; i < end; ++i)
-          if (c->ops[i].kind == OpKind::Gate) apply_lowered(s, c->ops[i].lowered);
+        launch_run(s, c, g, k);
       } catch (...) {
         ok = false;
       }
@@ -372,8 +421,7 @@ void run_gates(ncsim_state* s, const ncsim_circuit* c, GateGraphs& g, size_t k) 
   if (g.exec[k]) {
     NCSIM_CUDA(cudaGraphLaunch(g.exec[k], s->stream));
   } else {
-    for (size_t i = first; i < end; ++i)
-      if (c->ops[i].kind == OpKind::Gate) apply_lowered(s, c->ops[i].lowered);
+    launch_run(s, c, g, k);
   }
 }
 
@@ -393,7 +441,7 @@ ncsim_status ncsim_sv_run(ncsim_state* s, const ncsim_circuit* c, ncsim_rng* rng
     std::lock_guard<std::recursive_mutex> lk(s->mu);
     static const bool graphs_off = std::getenv("NCSIM_NO_GATE_GRAPHS") != nullptr;
     std::shared_ptr<GateGraphs> g;
-    if (!s->prof && !graphs_off) g = gate_graphs_for(c, s);
+    if (!graphs_off) g = gate_graphs_for(c, s);
     size_t m = 0, k = 0;
     for (size_t i = 0; i < c->ops.size();) {
       if (g && k < g->runs.size() && g->runs[k].first == i) {

@@ -141,6 +141,7 @@ extern "C" {
     pub fn ncsim_sv_timer_start(s: *mut ncsim_state) -> ncsim_status;
     pub fn ncsim_sv_timer_stop(s: *mut ncsim_state, milliseconds: *mut f64) -> ncsim_status;
     pub fn ncsim_sv_compare(a: *const ncsim_state, b: *const ncsim_state, inner_re_im: *mut f64, norm_a: *mut f64, norm_b: *mut f64, max_abs_diff: *mut f64) -> ncsim_status;
+    pub fn ncsim_sv_set_tile_passes(s: *mut ncsim_state, enable: i32) -> ncsim_status;
     pub fn ncsim_sv_profile_enable(s: *mut ncsim_state, enable: i32) -> ncsim_status;
     pub fn ncsim_sv_profile_read(s: *mut ncsim_state, out: *mut ncsim_kernel_stat, cap: u32, count: *mut u32) -> ncsim_status;
     pub fn ncsim_measure_stats_noalloc(amps: *const c_void, n: u32, precision: i32, x: u64, z: u64, phase: u32, stream: *mut c_void, expectation_re_im: *mut f64, norm_sq: *mut f64) -> ncsim_status;
