@@ -193,15 +193,48 @@ __host__ __device__ __forceinline__ V cadd(V a, V b) {
   return r;
 }
 template <class V>
-__host__ __device__ __forceinline__ V cfma(V m, V x, V acc) {  // acc + m*x
+__host__ __device__ __forceinline__ V cfma(V m, V x, V acc) {  // acc + m*x, two fused steps per part
   V r;
-  r.x = add_rn(acc.x, fma_rn(m.x, x.x, -mul_rn(m.y, x.y)));
-  r.y = add_rn(acc.y, fma_rn(m.x, x.y, mul_rn(m.y, x.x)));
+  r.x = fma_rn(m.x, x.x, fma_rn(-m.y, x.y, acc.x));
+  r.y = fma_rn(m.x, x.y, fma_rn(m.y, x.x, acc.y));
   return r;
 }
+// Both parts +-0.  On the device an integer test of the bits (the floating-point
+// compare would occupy the FP64 pipe next to the products).
 template <class V>
 __host__ __device__ __forceinline__ bool is_zero(V a) {
   return a.x == 0 && a.y == 0;
+}
+template <>
+__host__ __device__ __forceinline__ bool is_zero<double2>(double2 a) {
+#ifdef __CUDA_ARCH__
+  return ((uint64_t(__double_as_longlong(a.x)) | uint64_t(__double_as_longlong(a.y))) << 1) == 0;
+#else
+  return a.x == 0 && a.y == 0;
+#endif
+}
+template <>
+__host__ __device__ __forceinline__ bool is_zero<float2>(float2 a) {
+#ifdef __CUDA_ARCH__
+  return ((__float_as_uint(a.x) | __float_as_uint(a.y)) << 1) == 0;
+#else
+  return a.x == 0 && a.y == 0;
+#endif
+}
+// exactly 1 + 0i (either sign of the zero)
+__host__ __device__ __forceinline__ bool is_one_v(double2 c) {
+#ifdef __CUDA_ARCH__
+  return uint64_t(__double_as_longlong(c.x)) == 0x3FF0000000000000ull && (uint64_t(__double_as_longlong(c.y)) << 1) == 0;
+#else
+  return c.x == 1.0 && c.y == 0.0;
+#endif
+}
+__host__ __device__ __forceinline__ bool is_one_v(float2 c) {
+#ifdef __CUDA_ARCH__
+  return __float_as_uint(c.x) == 0x3F800000u && (__float_as_uint(c.y) << 1) == 0;
+#else
+  return c.x == 1.0f && c.y == 0.0f;
+#endif
 }
 // i^k * a for k mod 4
 template <class V>

@@ -461,7 +461,7 @@ __global__ void __launch_bounds__(THREADS) k_phasepoly(V<R>* __restrict__ a, uin
     V<R> c;
     if (use_table) {
       c = table[f];
-      if (c.x == R(1) && c.y == R(0)) continue;
+      if (is_one_v(c)) continue;
     } else {
       if (f == 0 && s_one) continue;
       double2 r = device_root(f, bits);
@@ -554,7 +554,7 @@ __global__ void __launch_bounds__(THREADS) k_phasepoly_sliced(V<R>* __restrict__
         for (int k = 0; k < B; ++k) f |= ((F[k] >> j) & 1u) << k;
         if (is_zero(v[u])) continue;
         const V<R> c = table[f];
-        if (c.x == R(1) && c.y == R(0)) continue;
+        if (is_one_v(c)) continue;
         p[j << 5] = cmul(c, v[u]);
       }
     }

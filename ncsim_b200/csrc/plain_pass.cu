@@ -18,8 +18,10 @@
 // qubits, permutation tables other than pair swaps, phase polynomials of more
 // than 64 terms) run as their own kernels between passes.
 #include <algorithm>
+#include <cmath>
 #include <cstring>
 #include <memory>
+#include <string>
 
 #include "engine.cuh"
 #include "host/ir.hpp"
@@ -32,8 +34,11 @@ constexpr int PASS_THREADS = 512;
 constexpr int MAX_TILE_BITS = 12;
 constexpr int MAX_FIBER_K = 3;  // 4- and 5-qubit matrices run as their own kernels (registers)
 constexpr int MAX_TABLE_K = 10;
-constexpr int MAX_PASS_TERMS = 64;
-constexpr int MAX_PASS_PARITIES = 256;
+// longer phase polynomials run as the bit-sliced kernel: evaluated per element
+// in a tile they cost a popcount per parity per amplitude
+constexpr int MAX_PASS_TERMS = 4;
+constexpr int MAX_PASS_PARITIES = 8;
+constexpr int MAX_PASS_OPS = 192;  // ops of one pass (chain heads included)
 
 template <class R>
 using V = typename VecOf<R>::T;
@@ -66,7 +71,8 @@ struct TileOp {
   uint32_t phase;
   uint32_t cp;       // complex pool offset
   uint32_t up;       // word pool offset
-  uint32_t reg;      // in a chain: the op's bits among the cube's three (see tile_chain)
+  uint32_t reg;      // in a chain: the op's bits among the cube's three, or its cube elements (see chainify)
+  uint32_t gml, gvl; // in a chain: fixed local bits outside the cube, and their values
 };
 
 struct PassGeom {
@@ -102,21 +108,40 @@ __device__ __forceinline__ uint32_t insert_zeros32(uint32_t v, const uint8_t* po
 }
 __device__ __forceinline__ int parity64(uint64_t v) { return __popcll(v) & 1; }
 
+// A tile in shared memory, element e stored at e ^ ((e >> 3) & 7): the XOR of
+// the low three index bits with the next three spreads the 16-byte elements of
+// a warp's access over the banks whichever tile bits an op pairs (a thread
+// holding a cube of three low bits reads eight consecutive elements; without
+// the swizzle every thread of the warp would hit the same four banks).
+template <class R>
+struct SwTile {
+  V<R>* p;
+  __device__ __forceinline__ V<R>& operator[](uint32_t e) const { return p[e ^ ((e >> 3) & 7u)]; }
+};
+
+// The pass's ops travel in the kernel parameters (constant bank): every thread
+// reads the same op at the same time, a broadcast the constant cache serves.
 template <class R>
 struct PassParams {
   V<R>* amp;
   uint64_t ntiles;
   PassGeom g;
-  const TileOp* ops;
   uint32_t nops;
   const V<R>* cpool;
   const uint32_t* upool;
   const uint64_t* ppool;  // phase polynomial parities (global masks)
+  TileOp ops[MAX_PASS_OPS];
 };
+
+// constant i of the pass's pool
+template <class R>
+__device__ __forceinline__ V<R> pconst(const PassParams<R>& P, uint32_t i) {
+  return P.cpool[i];
+}
 
 // -------- the gates on a tile (all threads of the CTA; `t` in shared memory) --------
 template <class R>
-__device__ void tile_dense1(V<R>* t, uint32_t tsz, const TileOp& op, const V<R>* cp) {
+__device__ void tile_dense1(SwTile<R> t, uint32_t tsz, const TileOp& op, const V<R>* cp) {
   const V<R> m00 = cp[op.cp], m01 = cp[op.cp + 1], m10 = cp[op.cp + 2], m11 = cp[op.cp + 3];
   const uint32_t lo = (1u << op.l0) - 1;
   for (uint32_t p = threadIdx.x; p < (tsz >> 1); p += blockDim.x) {
@@ -128,7 +153,7 @@ __device__ void tile_dense1(V<R>* t, uint32_t tsz, const TileOp& op, const V<R>*
 }
 
 template <class R>
-__device__ void tile_dense2(V<R>* t, uint32_t tsz, const TileOp& op, const V<R>* cp) {
+__device__ void tile_dense2(SwTile<R> t, uint32_t tsz, const TileOp& op, const V<R>* cp) {
   const uint32_t ba = 1u << op.l0, bb = 1u << op.l1;
   uint8_t pos[2] = {uint8_t(min(op.l0, op.l1)), uint8_t(max(op.l0, op.l1))};
   for (uint32_t p = threadIdx.x; p < (tsz >> 2); p += blockDim.x) {
@@ -149,7 +174,7 @@ __device__ void tile_dense2(V<R>* t, uint32_t tsz, const TileOp& op, const V<R>*
 }
 
 template <class R, int K>
-__device__ void tile_fiber(V<R>* t, uint32_t tsz, const TileOp& op, const V<R>* cp, const uint32_t* up) {
+__device__ void tile_fiber(SwTile<R> t, uint32_t tsz, const TileOp& op, const V<R>* cp, const uint32_t* up) {
   constexpr int D = 1 << K;
   uint8_t pos[K];
 #pragma unroll
@@ -175,7 +200,7 @@ __device__ void tile_fiber(V<R>* t, uint32_t tsz, const TileOp& op, const V<R>* 
 
 // the elements with every local fixed bit set to its value: p with zeros inserted, ORed with the values
 template <class R>
-__device__ void tile_diag_const(V<R>* t, uint32_t tsz, const TileOp& op, const V<R>* cp, const uint32_t* up) {
+__device__ void tile_diag_const(SwTile<R> t, uint32_t tsz, const TileOp& op, const V<R>* cp, const uint32_t* up) {
   const int nf = __popc(op.lfix);
   uint8_t pos[MAX_TILE_BITS];
   for (int i = 0; i < nf; ++i) pos[i] = uint8_t(up[op.up + i]);
@@ -188,7 +213,7 @@ __device__ void tile_diag_const(V<R>* t, uint32_t tsz, const TileOp& op, const V
 }
 
 template <class R>
-__device__ void tile_diag_1q(V<R>* t, uint32_t tsz, const TileOp& op, const V<R>* cp, uint64_t base) {
+__device__ void tile_diag_1q(SwTile<R> t, uint32_t tsz, const TileOp& op, const V<R>* cp, uint64_t base) {
   const V<R> c0 = cp[op.cp], c1 = cp[op.cp + 1];
   const bool outside = op.flags & 1;
   const bool obit = (base >> op.l1) & 1;  // the qubit's global position when it lies outside
@@ -200,7 +225,7 @@ __device__ void tile_diag_1q(V<R>* t, uint32_t tsz, const TileOp& op, const V<R>
 }
 
 template <class R>
-__device__ void tile_diag_table(V<R>* t, uint32_t tsz, const TileOp& op, const V<R>* cp, const uint32_t* up,
+__device__ void tile_diag_table(SwTile<R> t, uint32_t tsz, const TileOp& op, const V<R>* cp, const uint32_t* up,
                                 uint64_t base) {
   // up: [k] local position of qubit j (or 255 + its global position when outside), then the
   // local fixed positions (ascending), then the unit flags as bytes
@@ -233,7 +258,7 @@ __device__ void tile_diag_table(V<R>* t, uint32_t tsz, const TileOp& op, const V
 }
 
 template <class R>
-__device__ void tile_pairswap(V<R>* t, uint32_t tsz, const TileOp& op, const V<R>* cp, const uint32_t* up) {
+__device__ void tile_pairswap(SwTile<R> t, uint32_t tsz, const TileOp& op, const V<R>* cp, const uint32_t* up) {
   const int nf = __popc(op.lfix);
   uint8_t pos[MAX_TILE_BITS];
   for (int i = 0; i < nf; ++i) pos[i] = uint8_t(up[op.up + i]);
@@ -275,7 +300,7 @@ __device__ __forceinline__ double2 pass_root(uint64_t f, uint32_t bits) {
 
 // up: bits, use_table, scalar_is_one, constant lo, constant hi, start[k+1], coeff[k]; cp: scalar, table[2^bits]
 template <class R>
-__device__ void tile_phasepoly(V<R>* t, uint32_t tsz, const TileOp& op, const V<R>* cp, const uint32_t* up,
+__device__ void tile_phasepoly(SwTile<R> t, uint32_t tsz, const TileOp& op, const V<R>* cp, const uint32_t* up,
                                const uint64_t* pp, uint64_t base, uint64_t dthread, const uint64_t* dround) {
   const uint32_t* u = up + op.up;
   const uint32_t bits = u[0];
@@ -304,7 +329,7 @@ __device__ void tile_phasepoly(V<R>* t, uint32_t tsz, const TileOp& op, const V<
     V<R> c;
     if (use_table) {
       c = table[f];
-      if (c.x == R(1) && c.y == R(0)) continue;
+      if (is_one_v(c)) continue;
     } else {
       if (f == 0 && s_one) continue;
       const double2 rr = pass_root(f, bits);
@@ -323,7 +348,7 @@ __device__ void tile_phasepoly(V<R>* t, uint32_t tsz, const TileOp& op, const V<
 // its ops in circuit order with each op's own arithmetic.  Register indices
 // are compile-time: the op's cube bits (`reg`) select a template instance.
 template <class R, int J>
-__device__ __forceinline__ void chain_dense1(V<R> (&v)[8], const V<R>* m) {
+__device__ __forceinline__ void chain_dense1(V<R> (&v)[8], const V<R> (&m)[4]) {
   const V<R> m00 = m[0], m01 = m[1], m10 = m[2], m11 = m[3];
 #pragma unroll
   for (int b = 0; b < 8; ++b)
@@ -335,7 +360,10 @@ __device__ __forceinline__ void chain_dense1(V<R> (&v)[8], const V<R>* m) {
 }
 
 template <class R, int JA, int JB>
-__device__ __forceinline__ void chain_dense2(V<R> (&v)[8], const V<R>* m) {
+__device__ __forceinline__ void chain_dense2(V<R> (&v)[8], const PassParams<R>& P, uint32_t c0) {
+  V<R> m[16];
+#pragma unroll
+  for (int i = 0; i < 16; ++i) m[i] = pconst(P, c0 + i);
 #pragma unroll
   for (int b = 0; b < 8; ++b)
     if (!((b >> JA) & 1) && !((b >> JB) & 1)) {
@@ -356,26 +384,27 @@ __device__ __forceinline__ void chain_dense2(V<R> (&v)[8], const V<R>* m) {
 
 // a 3-qubit matrix whose qubit j sits on cube bit PJ (the permutation P0 P1 P2)
 template <class R, int P0, int P1, int P2>
-__device__ __forceinline__ void chain_fiber(V<R> (&v)[8], const V<R>* m) {
+__device__ __forceinline__ void chain_fiber(V<R> (&v)[8], const PassParams<R>& P, uint32_t c0) {
+  const V<R>* m = P.cpool + c0;
+  auto mat = [&](int i) { return m[i]; };
   V<R> x[8];
 #pragma unroll
   for (int b = 0; b < 8; ++b) x[b] = v[((b & 1) << P0) | (((b >> 1) & 1) << P1) | (((b >> 2) & 1) << P2)];
 #pragma unroll
   for (int r = 0; r < 8; ++r) {
-    V<R> acc = cmul(m[r * 8], x[0]);
+    V<R> acc = cmul(mat(r * 8), x[0]);
 #pragma unroll
-    for (int b = 1; b < 8; ++b) acc = cfma(m[r * 8 + b], x[b], acc);
+    for (int b = 1; b < 8; ++b) acc = cfma(mat(r * 8 + b), x[b], acc);
     v[((r & 1) << P0) | (((r >> 1) & 1) << P1) | (((r >> 2) & 1) << P2)] = acc;
   }
 }
 
 template <class R, int X>
-__device__ __forceinline__ void chain_pairswap(V<R> (&v)[8], const uint32_t (&e)[8], const TileOp& op, V<R> ci,
-                                               V<R> cj) {
-  const bool ui = op.flags & 1, uj = (op.flags >> 1) & 1;
+__device__ __forceinline__ void chain_pairswap(V<R> (&v)[8], uint32_t em, uint32_t flags, V<R> ci, V<R> cj) {
+  const bool ui = flags & 1, uj = (flags >> 1) & 1;
 #pragma unroll
   for (int b = 0; b < 8; ++b)
-    if ((e[b] & op.lfix) == op.lones) {
+    if ((em >> b) & 1) {
       const V<R> vi = v[b], vj = v[b ^ X];
       v[b] = ui ? vj : cmul(ci, vj);
       v[b ^ X] = uj ? vi : cmul(cj, vi);
@@ -404,7 +433,7 @@ __device__ __forceinline__ V<R> phasepoly_elem(V<R> v, uint64_t i, const TileOp&
   V<R> c;
   if (use_table) {
     c = cp[op.cp + 1 + f];
-    if (c.x == R(1) && c.y == R(0)) return v;
+    if (is_one_v(c)) return v;
   } else {
     if (f == 0 && s_one) return v;
     const double2 rr = pass_root(f, bits);
@@ -417,14 +446,13 @@ __device__ __forceinline__ V<R> phasepoly_elem(V<R> v, uint64_t i, const TileOp&
 }
 
 template <class R>
-__device__ void tile_chain(V<R>* t, uint32_t tsz, const TileOp& head, const TileOp* sub, const PassParams<R>& P,
-                           uint64_t base) {
+__device__ void tile_chain(SwTile<R> t, uint32_t tsz, const TileOp* ops, const PassParams<R>& P, uint64_t base) {
+  const TileOp& head = ops[0];
   const uint32_t nsub = head.k;
   const uint8_t cpos[3] = {uint8_t(head.l0 & 0xff), uint8_t((head.l0 >> 8) & 0xff), uint8_t((head.l0 >> 16) & 0xff)};
   uint32_t loff[8];
 #pragma unroll
   for (int b = 0; b < 8; ++b) loff[b] = ((b & 1u) << cpos[0]) | (((b >> 1) & 1u) << cpos[1]) | (((b >> 2) & 1u) << cpos[2]);
-  const V<R>* cp = P.cpool;
   for (uint32_t grp = threadIdx.x; grp < (tsz >> 3); grp += blockDim.x) {
     const uint32_t gb = insert_zeros32(grp, cpos, 3);
     uint32_t e[8];
@@ -435,63 +463,71 @@ __device__ void tile_chain(V<R>* t, uint32_t tsz, const TileOp& head, const Tile
       v[b] = t[e[b]];
     }
     for (uint32_t s = 0; s < nsub; ++s) {
-      const TileOp& op = sub[s];
+      const TileOp& op = ops[1 + s];
       if ((base & op.gfix) != op.gval) continue;
+      // the op's constants (at most 64 of them: a 3-qubit matrix)
+      V<R> m[4];
       switch (op.kind) {
         case TK_DENSE1:
-          if (op.reg == 0) chain_dense1<R, 0>(v, cp + op.cp);
-          else if (op.reg == 1) chain_dense1<R, 1>(v, cp + op.cp);
-          else chain_dense1<R, 2>(v, cp + op.cp);
+#pragma unroll
+          for (int i = 0; i < 4; ++i) m[i] = pconst(P, op.cp + i);
+          if (op.reg == 0) chain_dense1<R, 0>(v, m);
+          else if (op.reg == 1) chain_dense1<R, 1>(v, m);
+          else chain_dense1<R, 2>(v, m);
           break;
         case TK_DENSE2:
           switch (op.reg) {  // ja | jb << 4
-            case 0x10: chain_dense2<R, 0, 1>(v, cp + op.cp); break;
-            case 0x20: chain_dense2<R, 0, 2>(v, cp + op.cp); break;
-            case 0x01: chain_dense2<R, 1, 0>(v, cp + op.cp); break;
-            case 0x21: chain_dense2<R, 1, 2>(v, cp + op.cp); break;
-            case 0x02: chain_dense2<R, 2, 0>(v, cp + op.cp); break;
-            default: chain_dense2<R, 2, 1>(v, cp + op.cp); break;
+            case 0x10: chain_dense2<R, 0, 1>(v, P, op.cp); break;
+            case 0x20: chain_dense2<R, 0, 2>(v, P, op.cp); break;
+            case 0x01: chain_dense2<R, 1, 0>(v, P, op.cp); break;
+            case 0x21: chain_dense2<R, 1, 2>(v, P, op.cp); break;
+            case 0x02: chain_dense2<R, 2, 0>(v, P, op.cp); break;
+            default: chain_dense2<R, 2, 1>(v, P, op.cp); break;
           }
           break;
         case TK_FIBER:
           switch (op.reg) {  // p0 | p1 << 4 | p2 << 8
-            case 0x210: chain_fiber<R, 0, 1, 2>(v, cp + op.cp); break;
-            case 0x120: chain_fiber<R, 0, 2, 1>(v, cp + op.cp); break;
-            case 0x201: chain_fiber<R, 1, 0, 2>(v, cp + op.cp); break;
-            case 0x021: chain_fiber<R, 1, 2, 0>(v, cp + op.cp); break;
-            case 0x102: chain_fiber<R, 2, 0, 1>(v, cp + op.cp); break;
-            default: chain_fiber<R, 2, 1, 0>(v, cp + op.cp); break;
+            case 0x210: chain_fiber<R, 0, 1, 2>(v, P, op.cp); break;
+            case 0x120: chain_fiber<R, 0, 2, 1>(v, P, op.cp); break;
+            case 0x201: chain_fiber<R, 1, 0, 2>(v, P, op.cp); break;
+            case 0x021: chain_fiber<R, 1, 2, 0>(v, P, op.cp); break;
+            case 0x102: chain_fiber<R, 2, 0, 1>(v, P, op.cp); break;
+            default: chain_fiber<R, 2, 1, 0>(v, P, op.cp); break;
           }
           break;
         case TK_PAIRSWAP: {
-          const V<R> ci = cp[op.cp], cj = cp[op.cp + 1];
-          switch (op.reg) {
-            case 1: chain_pairswap<R, 1>(v, e, op, ci, cj); break;
-            case 2: chain_pairswap<R, 2>(v, e, op, ci, cj); break;
-            case 3: chain_pairswap<R, 3>(v, e, op, ci, cj); break;
-            case 4: chain_pairswap<R, 4>(v, e, op, ci, cj); break;
-            case 5: chain_pairswap<R, 5>(v, e, op, ci, cj); break;
-            case 6: chain_pairswap<R, 6>(v, e, op, ci, cj); break;
-            default: chain_pairswap<R, 7>(v, e, op, ci, cj); break;
+          if ((gb & op.gml) != op.gvl) break;
+          const V<R> ci = pconst(P, op.cp), cj = pconst(P, op.cp + 1);
+          const uint32_t em = op.reg >> 8;
+          switch (op.reg & 7) {
+            case 1: chain_pairswap<R, 1>(v, em, op.flags, ci, cj); break;
+            case 2: chain_pairswap<R, 2>(v, em, op.flags, ci, cj); break;
+            case 3: chain_pairswap<R, 3>(v, em, op.flags, ci, cj); break;
+            case 4: chain_pairswap<R, 4>(v, em, op.flags, ci, cj); break;
+            case 5: chain_pairswap<R, 5>(v, em, op.flags, ci, cj); break;
+            case 6: chain_pairswap<R, 6>(v, em, op.flags, ci, cj); break;
+            default: chain_pairswap<R, 7>(v, em, op.flags, ci, cj); break;
           }
           break;
         }
         case TK_DIAG_CONST: {
-          const V<R> c = cp[op.cp];
+          if ((gb & op.gml) != op.gvl) break;
+          const V<R> c = pconst(P, op.cp);
+          const uint32_t em = op.reg;  // the cube elements with the fixed pattern
 #pragma unroll
           for (int b = 0; b < 8; ++b)
-            if ((e[b] & op.lfix) == op.lones && !is_zero(v[b])) v[b] = cmul(c, v[b]);
+            if (((em >> b) & 1) && !is_zero(v[b])) v[b] = cmul(c, v[b]);
           break;
         }
         case TK_DIAG_1Q: {
-          const V<R> c0 = cp[op.cp], c1 = cp[op.cp + 1];
-          const bool outside = op.flags & 1;
-          const bool obit = (base >> op.l1) & 1;
+          const V<R> c0 = pconst(P, op.cp), c1 = pconst(P, op.cp + 1);
+          // the cube elements whose qubit bit is 1: from the cube, the group or the tile base
+          const uint32_t ones = (op.flags & 4) ? op.reg
+                              : (op.flags & 1) ? (((base >> op.l1) & 1) ? 0xffu : 0u)
+                                               : (((gb >> op.l0) & 1) ? 0xffu : 0u);
 #pragma unroll
-          for (int b = 0; b < 8; ++b) {
-            const bool bit = outside ? obit : ((e[b] >> op.l0) & 1u);
-            if (!is_zero(v[b])) v[b] = cmul(bit ? c1 : c0, v[b]);
-          }
+          for (int b = 0; b < 8; ++b)
+            if (!is_zero(v[b])) v[b] = cmul(((ones >> b) & 1) ? c1 : c0, v[b]);
           break;
         }
         case TK_DIAG_TABLE: {
@@ -509,7 +545,7 @@ __device__ void tile_chain(V<R>* t, uint32_t tsz, const TileOp& head, const Tile
             for (int j = 0; j < k; ++j)
               if (qp[j] < 256) x |= ((e[b] >> qp[j]) & 1u) << j;
             if (unit[x]) continue;
-            if (!is_zero(v[b])) v[b] = cmul(cp[op.cp + x], v[b]);
+            if (!is_zero(v[b])) v[b] = cmul(pconst(P, op.cp + x), v[b]);
           }
           break;
         }
@@ -517,7 +553,7 @@ __device__ void tile_chain(V<R>* t, uint32_t tsz, const TileOp& head, const Tile
 #pragma unroll
           for (int b = 0; b < 8; ++b) {
             bool ch;
-            v[b] = phasepoly_elem<R>(v[b], base | deposit(e[b], P.g), op, cp, P.upool, P.ppool, ch);
+            v[b] = phasepoly_elem<R>(v[b], base | deposit(e[b], P.g), op, P.cpool, P.upool, P.ppool, ch);
           }
           break;
         }
@@ -536,8 +572,15 @@ __global__ void __launch_bounds__(PASS_THREADS) k_plain_pass(const __grid_consta
   const uint32_t tsz = 1u << g.T;
   V<R>* buf[2] = {reinterpret_cast<V<R>*>(pass_smem), reinterpret_cast<V<R>*>(pass_smem) + tsz};
   __shared__ uint64_t dround[MAX_TILE_BITS > 9 ? (1 << MAX_TILE_BITS) / 32 : 32];
+  __shared__ TileOp s_ops[MAX_PASS_OPS];  // the ops, read from shared memory in the tile loop
   const uint32_t nr = (tsz + blockDim.x - 1) / blockDim.x;  // element rounds per thread
   for (uint32_t r = threadIdx.x; r < nr; r += blockDim.x) dround[r] = deposit(r * blockDim.x, g);
+  {
+    const uint32_t words = P.nops * uint32_t(sizeof(TileOp) / 4);
+    const uint32_t* src = reinterpret_cast<const uint32_t*>(P.ops);
+    uint32_t* dst = reinterpret_cast<uint32_t*>(s_ops);
+    for (uint32_t i = threadIdx.x; i < words; i += blockDim.x) dst[i] = src[i];
+  }
   const uint64_t dthread = deposit(threadIdx.x, g);
   __syncthreads();
   auto load = [&](uint64_t tile, V<R>* dst) {
@@ -545,7 +588,7 @@ __global__ void __launch_bounds__(PASS_THREADS) k_plain_pass(const __grid_consta
     for (uint32_t r = 0; r < nr; ++r) {
       const uint32_t e = threadIdx.x + r * blockDim.x;
       if (e >= tsz) break;
-      const uint32_t d = static_cast<uint32_t>(__cvta_generic_to_shared(dst + e));
+      const uint32_t d = static_cast<uint32_t>(__cvta_generic_to_shared(&SwTile<R>{dst}[e]));
       if constexpr (sizeof(V<R>) == 16)
         asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(d), "l"(src + dround[r]) : "memory");
       else
@@ -556,7 +599,7 @@ __global__ void __launch_bounds__(PASS_THREADS) k_plain_pass(const __grid_consta
   uint64_t tile = blockIdx.x;
   if (tile < P.ntiles) load(tile, buf[0]);
   for (uint32_t it = 0; tile < P.ntiles; ++it, tile += gridDim.x) {
-    V<R>* t = buf[it & 1];
+    const SwTile<R> t{buf[it & 1]};
     const uint64_t next = tile + gridDim.x;
     if (next < P.ntiles) {
       load(next, buf[(it & 1) ^ 1]);
@@ -567,9 +610,9 @@ __global__ void __launch_bounds__(PASS_THREADS) k_plain_pass(const __grid_consta
     __syncthreads();
     const uint64_t base = tile_base_of(tile, g);
     for (uint32_t o = 0; o < P.nops; ++o) {
-      const TileOp& op = P.ops[o];
+      const TileOp& op = s_ops[o];
       if (op.kind == TK_CHAIN) {
-        tile_chain<R>(t, tsz, op, P.ops + o + 1, P, base);
+        tile_chain<R>(t, tsz, s_ops + o, P, base);
         o += op.k;
         __syncthreads();
         continue;
@@ -654,6 +697,21 @@ GateForm form_diag_table(const std::vector<uint32_t>& qubits, const std::vector<
   f.unit.resize(gd);
   for (int x = 0; x < gd; ++x) f.unit[x] = one_c(diag[x]) ? 1 : 0;
   return f;
+}
+
+// the share of the register the gate's own kernel reads and writes (its
+// algorithmic bytes over a full pass: the sectors that hold an amplitude it changes)
+double touched_share(const GateForm& f, int precision) {
+  const uint64_t below = precision == NCSIM_C128 ? 1 : 3;  // index bits inside a 32-byte sector
+  auto share = [&](uint64_t fixed) { return std::ldexp(1.0, -__builtin_popcountll(fixed & ~below)); };
+  switch (f.kind) {
+    case TK_DIAG_CONST: case TK_DIAG_TABLE: return share(f.fixmask);
+    case TK_PAIRSWAP: {
+      const uint64_t ctrl = f.fixmask & ~f.xmask;
+      return std::min(1.0, share(ctrl) * 2.0 / double(uint64_t(1) << __builtin_popcountll(f.xmask)));
+    }
+    default: return 1.0;
+  }
 }
 
 GateForm form_of(const LoweredOp& op) {
@@ -801,17 +859,15 @@ struct PlainPlan {
     size_t gate = 0;              // direct: index into `gates`
     Window win;
     std::vector<TileOp> ops;
-    uint32_t op_off = 0;          // into the device op array
+    uint32_t cbeg = 0, cend = 0;  // the pass's range of the constant pool
   };
   int precision = NCSIM_C128;
   std::vector<const LoweredOp*> gates;
   std::vector<Item> items;
-  std::vector<TileOp> all_ops;
   std::vector<double> cpool;      // complex values, interleaved
   std::vector<uint32_t> upool;
   std::vector<uint64_t> ppool;
   int device = -1;
-  void* d_ops = nullptr;
   void* d_cpool = nullptr;
   uint32_t* d_upool = nullptr;
   uint64_t* d_ppool = nullptr;
@@ -821,7 +877,6 @@ struct PlainPlan {
       int cur = 0;
       cudaGetDevice(&cur);
       cudaSetDevice(device);
-      cudaFree(d_ops);
       cudaFree(d_cpool);
       cudaFree(d_upool);
       cudaFree(d_ppool);
@@ -973,6 +1028,17 @@ std::vector<TileOp> chainify(const std::vector<TileOp>& ops, const std::vector<u
         if (cpos[q] == int(l)) return uint32_t(q);
       return 0u;
     };
+    const uint32_t cmask = (1u << cpos[0]) | (1u << cpos[1]) | (1u << cpos[2]);
+    uint32_t loff[8];
+    for (int b = 0; b < 8; ++b)
+      loff[b] = ((b & 1u) << cpos[0]) | (((b >> 1) & 1u) << cpos[1]) | (((b >> 2) & 1u) << cpos[2]);
+    // the cube elements b whose cube bits match the op's fixed pattern there
+    auto elements = [&](uint32_t lfix, uint32_t lones) {
+      uint32_t em = 0;
+      for (int b = 0; b < 8; ++b)
+        if ((loff[b] & lfix) == (lones & cmask)) em |= 1u << b;
+      return em;
+    };
     TileOp head{};
     head.kind = TK_CHAIN;
     head.k = uint32_t(j - i);
@@ -993,9 +1059,22 @@ std::vector<TileOp> chainify(const std::vector<TileOp>& ops, const std::vector<u
           uint32_t r = 0;
           for (int b = 0; b < T; ++b)
             if ((op.lx >> b) & 1) r |= 1u << cube(uint32_t(b));
-          op.reg = r;
+          op.reg = r | (elements(op.lfix, op.lones) << 8);
+          op.gml = op.lfix & ~cmask;
+          op.gvl = op.lones & ~cmask;
           break;
         }
+        case TK_DIAG_CONST:
+          op.reg = elements(op.lfix, op.lones);
+          op.gml = op.lfix & ~cmask;
+          op.gvl = op.lones & ~cmask;
+          break;
+        case TK_DIAG_1Q:
+          if (!(op.flags & 1) && ((cmask >> op.l0) & 1)) {
+            op.flags |= 4;
+            op.reg = elements(1u << op.l0, 1u << op.l0);
+          }
+          break;
         default: break;
       }
       out.push_back(op);
@@ -1021,17 +1100,26 @@ std::shared_ptr<PlainPlan> plan_plain_passes(uint32_t n, int precision, const st
   uint64_t moving = 0;
   auto flush = [&] {
     if (cur.empty()) return;
-    if (cur.size() == 1) {
-      PlainPlan::Item it;
-      it.gate = cur[0];
-      P->items.push_back(it);
+    // a pass reads and writes the whole register once; gates whose own kernels
+    // touch less than that between them stay gate by gate
+    double shares = 0.0;
+    for (size_t i : cur) shares += touched_share(forms[i], precision);
+    if (cur.size() == 1 || shares < 1.25) {
+      for (size_t i : cur) {
+        PlainPlan::Item it;
+        it.gate = i;
+        P->items.push_back(it);
+      }
     } else {
       PlainPlan::Item it;
       it.pass = true;
       it.win = make_window(n, T, moving);
       std::vector<TileOp> ops;
+      it.cbeg = uint32_t(P->cpool.size() / 2);
       for (size_t i : cur) ops.push_back(encode(forms[i], it.win, *P));
+      it.cend = uint32_t(P->cpool.size() / 2);
       it.ops = chainify(ops, P->upool, it.win.g.T);
+      if (it.ops.size() > size_t(MAX_PASS_OPS)) throw Error(NCSIM_ERR_INVALID, "tiled pass: too many ops");
       P->passes += 1;
       P->pass_gates += cur.size();
       P->items.push_back(std::move(it));
@@ -1049,18 +1137,29 @@ std::shared_ptr<PlainPlan> plan_plain_passes(uint32_t n, int precision, const st
       P->items.push_back(it);
       continue;
     }
-    if (__builtin_popcountll(moving | f.moving) > T) flush();
+    // chains add at most one head per op: a pass of MAX_PASS_OPS / 2 gates fits in shared memory
+    if (__builtin_popcountll(moving | f.moving) > T || cur.size() >= size_t(MAX_PASS_OPS / 2)) flush();
     cur.push_back(i);
     moving |= f.moving;
   }
   flush();
   if (P->passes == 0) return nullptr;
-  for (auto& it : P->items)
-    if (it.pass) {
-      it.op_off = uint32_t(P->all_ops.size());
-      P->all_ops.insert(P->all_ops.end(), it.ops.begin(), it.ops.end());
-    }
   return P;
+}
+
+// passes, gates in passes, chains and ops in chains, and gates left to their own kernels
+std::string plain_plan_summary(const PlainPlan& P) {
+  size_t chains = 0, chained = 0, direct = 0;
+  for (const auto& it : P.items) {
+    if (!it.pass) {
+      ++direct;
+      continue;
+    }
+    for (const auto& op : it.ops)
+      if (op.kind == TK_CHAIN) ++chains, chained += op.k;
+  }
+  return "passes " + std::to_string(P.passes) + ", gates in passes " + std::to_string(P.pass_gates) + ", chains " +
+         std::to_string(chains) + " holding " + std::to_string(chained) + " ops, own kernels " + std::to_string(direct);
 }
 
 size_t plain_plan_passes(const PlainPlan& P) { return P.passes; }
@@ -1074,8 +1173,9 @@ void launch_pass(ncsim_state* s, const PlainPlan& P, const PlainPlan::Item& it) 
   pp.amp = reinterpret_cast<V<R>*>(s->amp);
   pp.g = it.win.g;
   pp.ntiles = s->len >> it.win.g.T;
-  pp.ops = reinterpret_cast<const TileOp*>(P.d_ops) + it.op_off;
   pp.nops = uint32_t(it.ops.size());
+  std::copy(it.ops.begin(), it.ops.end(), pp.ops);
+
   pp.upool = P.d_upool;
   pp.ppool = P.d_ppool;
   // the complex pool as this precision's values
@@ -1097,8 +1197,6 @@ void run_plain_plan(ncsim_state* s, PlainPlan& P) {
   if (P.device < 0) {
     P.device = s->device;
     const bool dbl = s->precision == NCSIM_C128;
-    NCSIM_CUDA(cudaMalloc(&P.d_ops, std::max<size_t>(P.all_ops.size(), 1) * sizeof(TileOp)));
-    NCSIM_CUDA(cudaMemcpy(P.d_ops, P.all_ops.data(), P.all_ops.size() * sizeof(TileOp), cudaMemcpyHostToDevice));
     const size_t nc = P.cpool.size() / 2;
     if (dbl) {
       NCSIM_CUDA(cudaMalloc(&P.d_cpool, std::max<size_t>(nc, 1) * sizeof(double2)));

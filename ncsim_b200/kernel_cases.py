@@ -18,7 +18,7 @@ import os
 
 import numpy as np
 
-from . import C128, Gate, GpuStateVector, Pauli, StdRng
+from . import C128, Circuit, Gate, GpuStateVector, Pauli, StdRng
 
 
 def _unitary(k: int, seed: int) -> np.ndarray:
@@ -32,6 +32,7 @@ def cases(n: int):
     """(name, action) pairs; each action launches one kernel of its class on the state."""
     h, cx, cz, rz = Gate.parse("H"), Gate.parse("CX"), Gate.parse("CZ"), Gate.parse("RZ(0.3)")
     ccx = Gate.parse("CCX")
+    layers = Circuit.random_layers(n, 4, 1)
     u2, u3, u6 = _unitary(2, 1), _unitary(3, 2), _unitary(6, 3)
     u4, u5 = _unitary(4, 4), _unitary(5, 6)
     r = np.random.default_rng(5)
@@ -64,6 +65,8 @@ def cases(n: int):
         ("project_diag", lambda s: (s.project(Pauli(n, 0, 1 << (n - 4), 0), False), s.apply_gate(h, [n - 4]))),
         ("project_pair", lambda s: s.project(Pauli(n, 1 << (n - 5), 0, 0), False)),
         ("sample", lambda s: s.sample(StdRng(3), 1024)),
+        # a run of gates through tiled passes (one layer of the random layer family per pass or so)
+        ("run_layers", lambda s: s.run(layers, StdRng(0))),
     ]
 
 
