@@ -197,6 +197,78 @@ uint64_t qubit_mask(const std::vector<uint32_t>& qs) {
   return m;
 }
 
+// How the pass kernel can apply a term next to a unitary on the qubits gm:
+// 0 as a phase of the whole column (no gate qubit in its mask), 1 as a sign
+// on the rows of one gate qubit (a -1 conditioned on that qubit and column
+// bits), 2 neither (a sweep of its own).
+int term_relation(const Term& t, uint64_t gm) {
+  const uint64_t gp = t.mask & gm;
+  if (!gp) return 0;
+  if (__builtin_popcountll(gp) == 1 && t.c.re == -1.0 && t.c.im == 0.0) return 1;
+  return 2;
+}
+
+// Places a pass's elementwise terms.  Diagonal terms commute with each other
+// and with every unitary whose qubits they do not share, so each term moves
+// right to the gap before the first unitary that touches its qubits (or to the
+// end of the pass); one whose qubits all lie in that unitary is multiplied
+// into it (U <- U D, FP64), the rest gather in fewer gaps.  Each gap then holds
+// up to three term ops in this order: the terms the previous unitary's
+// read-back can apply, the ones that need a sweep of their own, and the ones
+// the next unitary's split can apply.  Every gap with terms costs the kernel a
+// per-amplitude phase or sign step, so fewer gaps mean fewer of them.
+void place_terms(Pass& pass) {
+  std::vector<FusedOp> us;
+  std::vector<std::vector<Term>> gaps(1);  // gaps[i]: terms before unitary i; the last: after all
+  for (FusedOp& op : pass.ops) {
+    if (op.kind == 0) {
+      us.push_back(std::move(op));
+      gaps.emplace_back();
+    } else {
+      for (const Term& t : op.terms) gaps.back().push_back(t);
+    }
+  }
+  const size_t nu = us.size();
+  std::vector<uint64_t> gm(nu);
+  for (size_t i = 0; i < nu; ++i) gm[i] = qubit_mask(us[i].qubits);
+  std::vector<std::vector<Term>> placed(nu + 1);
+  for (size_t i = 0; i <= nu; ++i)
+    for (const Term& t : gaps[i]) {
+      size_t j = i;
+      while (j < nu && !(t.mask & gm[j])) ++j;
+      if (j < nu && (t.mask & ~gm[j]) == 0) {
+        // U <- U D: column c of U takes the phase when its local index holds every bit of the mask
+        const std::vector<uint32_t>& q = us[j].qubits;
+        uint32_t lm = 0;
+        for (size_t b = 0; b < q.size(); ++b)
+          if ((t.mask >> q[b]) & 1) lm |= 1u << b;
+        const size_t d = size_t(1) << q.size();
+        for (size_t c = 0; c < d; ++c)
+          if ((uint32_t(c) & lm) == lm)
+            for (size_t r = 0; r < d; ++r) us[j].u[r * d + c] = mul(us[j].u[r * d + c], t.c);
+        continue;
+      }
+      placed[j].push_back(t);
+    }
+  pass.ops.clear();
+  for (size_t i = 0; i <= nu; ++i) {
+    std::vector<Term> post, sweep, pre;
+    for (const Term& t : merge_terms(placed[i])) {
+      if (i < nu && term_relation(t, gm[i]) < 2) pre.push_back(t);
+      else if (i > 0 && term_relation(t, gm[i - 1]) < 2) post.push_back(t);
+      else sweep.push_back(t);
+    }
+    for (std::vector<Term>* ts : {&post, &sweep, &pre}) {
+      if (ts->empty()) continue;
+      FusedOp op;
+      op.kind = 1;
+      op.terms = std::move(*ts);
+      pass.ops.push_back(std::move(op));
+    }
+    if (i < nu) pass.ops.push_back(std::move(us[i]));
+  }
+}
+
 // Builds one pass's program.  Diagonal gates are folded into a unitary on
 // their qubits whenever the order allows: into the most recent unitary that
 // touches them (everything applied to those qubits after it is diagonal, and
@@ -331,6 +403,7 @@ struct PassBuilder {
         ++term_count;
       }
     }
+    place_terms(pass);
     // window: exactly TILE_BITS qubits, ascending
     uint64_t w = window;
     for (uint32_t b = 0; b < n && __builtin_popcountll(w) < TILE_BITS; ++b) w |= uint64_t(1) << b;
