@@ -679,6 +679,58 @@ def config_rates(nb, peak, peak_kind):
                         "note": "GpuSparseVector from |0>: device time of the run on its stream (the host waits "
                                 "for entry counts after every normalisation); wall includes state creation"}
     del sp
+    out["sparse_published_n1000"] = sparse_published_workload(nb)
+    return out
+
+
+def ripple_texts(n: int = 1000, inputs: int = 10):
+    """The reference's published SparseVector workload (examples/bench.rs:245-262):
+    H on `inputs` qubits of an n-qubit register, then for q in 0..n-2 CCX (q, q+1, q+2)
+    and CX (q, q+2); the reference times the 2(n-2) ripple gates."""
+    head = "\n".join([f"QUBITS {n}"] + [f"H {q}" for q in range(inputs)]) + "\n"
+    body = "".join(f"CCX {q} {q + 1} {q + 2}\nCX {q} {q + 2}\n" for q in range(n - 2))
+    return head, f"QUBITS {n}\n" + body
+
+
+def sparse_published_workload(nb, reps: int = 5):
+    """n = 1000 sparse register, 1024 superposed inputs, the 1996-gate CCX/CX ripple
+    (README.md:214: 7 ms on a 16-thread desktop): device time of the ripple through
+    GpuSparseVector.run (one launch per run of one-to-one gates), wall time of the same
+    call, and the oracle's CPU restatement of the whole circuit on one host thread."""
+    head, ripple = ripple_texts()
+    ch, cr = nb.Circuit.parse(head), nb.Circuit.parse(ripple)
+    pz = nb.Pauli.from_string(1000, "Z0*Z999")
+    dev, wall, exp_ms = [], [], []
+    for _ in range(reps + 1):
+        sp = nb.GpuSparseVector(1000)
+        sp.run(ch, nb.StdRng(1))
+        sp.synchronize()
+        t0 = time.perf_counter()
+        sp.timer_start()
+        sp.run(cr, nb.StdRng(1))
+        dev.append(sp.timer_stop())
+        wall.append((time.perf_counter() - t0) * 1e3)
+        t1 = time.perf_counter()
+        z = sp.expectation(pz)
+        exp_ms.append((time.perf_counter() - t1) * 1e3)
+    dev, wall, exp_ms = dev[1:], wall[1:], exp_ms[1:]  # the first run warms the pools
+    out = {"workload": "n=1000 SparseVector: H on qubits 0..9, then CCX(q,q+1,q+2), CX(q,q+2) for q in 0..998 "
+                       "(1996 timed gates, 1024 entries of 16 words)",
+           "gates": cr.num_gates, "entries": sp.num_entries(),
+           "ms_device": statistics.median(dev), "ms_wall": statistics.median(wall),
+           "expectation_z0z999_ms_wall": statistics.median(exp_ms), "z0z999": z.real,
+           "published": {"ripple_s": 0.007, "hardware": "16-thread desktop (README.md:202, :214)"},
+           "vs_published_wall": 7.0 / statistics.median(wall)}
+    try:
+        from oracle import oracle as O
+
+        O.build()
+        t0 = time.perf_counter()
+        O.WideSparse(head + ripple.split("\n", 1)[1], 1)
+        out["cpu_oracle"] = {"s": time.perf_counter() - t0, "cores": 1, "kind": "port",
+                             "sample": "the whole circuit (H's, ripple) on the oracle's restatement, parse included"}
+    except Exception as e:  # the oracle is the baseline's checker only; its absence does not stop the bench
+        out["cpu_oracle"] = {"unavailable": str(e)[:200]}
     return out
 
 

@@ -288,6 +288,10 @@ ncsim_status ncsim_gate_lowered_matrix(const ncsim_gate* g, double* out, size_t 
 
 /* Pauli::from_string(n, text) (pauli/mod.rs:349-414) as (x, z, phase). */
 ncsim_status ncsim_pauli_parse(const char* text, uint32_t n, uint64_t* x, uint64_t* z, uint32_t* phase);
+/* The same on registers of any width: x and z as `words` 64-bit words each
+ * (qubit q: bit q % 64 of word q / 64), words * 64 >= n. */
+ncsim_status ncsim_pauli_parse_words(const char* text, uint32_t n, uint64_t* x, uint64_t* z, uint32_t words,
+                                     uint32_t* phase);
 
 /* QuantumState::apply_gate through the gate's views (vector.rs:364-395). */
 ncsim_status ncsim_sv_apply_gate(ncsim_state* s, const ncsim_gate* g, const uint32_t* qubits, uint32_t k);
@@ -415,8 +419,14 @@ ncsim_status ncsim_batch_results(ncsim_batch* b, uint32_t* n, uint64_t* records,
 ncsim_status ncsim_batch_emulate(const ncsim_batch* b, uint32_t t, uint64_t* record, double* z0, double* norm);
 
 /* ---- sparse form: SparseVector<C64> (src/state/sparse.rs) on the device ----
- * The nonzero amplitudes of a register of 1..64 qubits as (basis index,
- * complex128) entries in device memory (at most 2^31 entries).  Operations
+ * The nonzero amplitudes of a register of 1..1024 qubits as (basis index,
+ * complex128) entries in device memory (at most 2^31 entries).  A basis index
+ * is W = ncsim_sparse_num_words() 64-bit words (1 up to 64 qubits, 4 up to
+ * 256, 16 up to 1024), qubit q being bit q % 64 of word q / 64, the layout of
+ * ncsim's Bits (bits.rs:1-17); every key array below holds W words per entry,
+ * and keys order lexicographically from word 0, as Vec<u64> does.  The
+ * functions taking one uint64_t mask or index address qubits 0..63 of any
+ * register; the _words variants take W words.  Operations
  * that move each entry to one entry (monomial gates, permutations with
  * phases, Paulis, diagonals) keep the entry order and leave it unsorted when
  * a key changed; operations that create entries (dense gates, projections)
@@ -457,9 +467,10 @@ ncsim_status ncsim_sparse_project(ncsim_sparse* s, uint64_t x, uint64_t z, uint3
                                   double* weight_re_im);
 /* scale (sparse.rs:382-386). */
 ncsim_status ncsim_sparse_scale(ncsim_sparse* s, double re, double im);
-/* tensor (sparse.rs:388-405): a on the low qubits, b above them (n_a + n_b <= 64). */
+/* tensor (sparse.rs:388-405): a on the low qubits, b above them (n_a + n_b <= 1024). */
 ncsim_status ncsim_sparse_tensor(const ncsim_sparse* a, const ncsim_sparse* b, ncsim_sparse** out);
-/* sample (sparse.rs:407-424): cumulative weights in entry order, one rng.gen::<f64>() per shot. */
+/* sample (sparse.rs:407-424): cumulative weights in entry order, one rng.gen::<f64>() per shot;
+ * out holds W words per shot. */
 ncsim_status ncsim_sparse_sample(const ncsim_sparse* s, ncsim_rng* rng, uint64_t shots, uint64_t* out);
 /* to_vector (sparse.rs:426-434), n <= 26. */
 ncsim_status ncsim_sparse_to_vector(const ncsim_sparse* s, double* amps, uint64_t len);
@@ -468,6 +479,21 @@ ncsim_status ncsim_sparse_measure(ncsim_sparse* s, uint64_t x, uint64_t z, uint3
                                   int32_t* outcome);
 ncsim_status ncsim_sparse_run(ncsim_sparse* s, const ncsim_circuit* c, ncsim_rng* rng, uint8_t* rec, size_t cap,
                               size_t* len);
+/* Words per basis key: Bits' nwords(n) rounded up to 1, 4 or 16 (bits.rs:14-17). */
+ncsim_status ncsim_sparse_num_words(const ncsim_sparse* s, uint32_t* words);
+/* apply_pauli, amplitude, expectation, project and measure with W-word masks
+ * and indices (words must equal ncsim_sparse_num_words; sparse.rs:216-380,
+ * mod.rs:113-131). */
+ncsim_status ncsim_sparse_apply_pauli_words(ncsim_sparse* s, const uint64_t* x, const uint64_t* z, uint32_t words,
+                                            uint32_t phase);
+ncsim_status ncsim_sparse_amplitude_words(const ncsim_sparse* s, const uint64_t* index, uint32_t words,
+                                          double* re_im);
+ncsim_status ncsim_sparse_expectation_words(const ncsim_sparse* s, const uint64_t* x, const uint64_t* z,
+                                            uint32_t words, uint32_t phase, double* re_im);
+ncsim_status ncsim_sparse_project_words(ncsim_sparse* s, const uint64_t* x, const uint64_t* z, uint32_t words,
+                                        uint32_t phase, int32_t outcome, double* weight_re_im);
+ncsim_status ncsim_sparse_measure_words(ncsim_sparse* s, const uint64_t* x, const uint64_t* z, uint32_t words,
+                                        uint32_t phase, ncsim_rng* rng, int32_t* outcome);
 /* Waits for the state's queued device work; device-time events on its stream. */
 ncsim_status ncsim_sparse_synchronize(const ncsim_sparse* s);
 ncsim_status ncsim_sparse_timer_start(ncsim_sparse* s);

@@ -119,6 +119,7 @@ _SIGNATURES = {
     "ncsim_gate_free": (_i32, [_vp]),
     "ncsim_gate_lowered_matrix": (_i32, [_vp, _P(_dbl), C.c_size_t, _P(_u32)]),
     "ncsim_pauli_parse": (_i32, [C.c_char_p, _u32, _P(_u64), _P(_u64), _P(_u32)]),
+    "ncsim_pauli_parse_words": (_i32, [C.c_char_p, _u32, _P(_u64), _P(_u64), _u32, _P(_u32)]),
     "ncsim_sv_apply_gate": (_i32, [_vp, _vp, _P(_u32), _u32]),
     "ncsim_sv_measure": (_i32, [_vp, _u64, _u64, _u32, _vp, _P(_i32)]),
     "ncsim_sv_run": (_i32, [_vp, _vp, _vp, _P(C.c_uint8), C.c_size_t, _P(C.c_size_t)]),
@@ -172,6 +173,12 @@ _SIGNATURES = {
     "ncsim_sparse_synchronize": (_i32, [_vp]),
     "ncsim_sparse_timer_start": (_i32, [_vp]),
     "ncsim_sparse_timer_stop": (_i32, [_vp, _P(_dbl)]),
+    "ncsim_sparse_num_words": (_i32, [_vp, _P(_u32)]),
+    "ncsim_sparse_apply_pauli_words": (_i32, [_vp, _P(_u64), _P(_u64), _u32, _u32]),
+    "ncsim_sparse_amplitude_words": (_i32, [_vp, _P(_u64), _u32, _P(_dbl)]),
+    "ncsim_sparse_expectation_words": (_i32, [_vp, _P(_u64), _P(_u64), _u32, _u32, _P(_dbl)]),
+    "ncsim_sparse_project_words": (_i32, [_vp, _P(_u64), _P(_u64), _u32, _u32, _i32, _P(_dbl)]),
+    "ncsim_sparse_measure_words": (_i32, [_vp, _P(_u64), _P(_u64), _u32, _u32, _vp, _P(_i32)]),
     "ncsim_sv_set_tile_passes": (_i32, [_vp, _i32]),
     "ncsim_frames_new": (_i32, [_vp, _u64, _P(_vp)]),
     "ncsim_frames_with_reference": (_i32, [_vp, _P(C.c_uint8), _u64, _P(_vp)]),
@@ -272,7 +279,13 @@ class Pauli:
 
     @classmethod
     def from_string(cls, n: int, text: str) -> "Pauli":
-        """``Pauli::from_string`` (src/pauli/mod.rs:349-351)."""
+        """``Pauli::from_string`` (src/pauli/mod.rs:349-351); x and z are Python
+        integers of n bits, so registers wider than 64 qubits work too."""
+        if n > 64:
+            words = (n + 63) // 64
+            xw, zw, ph = (_u64 * words)(), (_u64 * words)(), _u32()
+            _check(lib().ncsim_pauli_parse_words(text.encode(), n, xw, zw, words, C.byref(ph)))
+            return cls(n, words_to_int(xw), words_to_int(zw), ph.value)
         x, z, ph = _u64(), _u64(), _u32()
         _check(lib().ncsim_pauli_parse(text.encode(), n, C.byref(x), C.byref(z), C.byref(ph)))
         return cls(n, x.value, z.value, ph.value)
@@ -286,6 +299,15 @@ class Pauli:
 
     def __repr__(self) -> str:
         return f"Pauli(n={self.n}, x={self.x:#x}, z={self.z:#x}, phase={self.phase})"
+
+
+def int_to_words(v: int, words: int):
+    """A basis index or Pauli mask as `words` little-endian 64-bit words (ncsim's Bits)."""
+    return (_u64 * words)(*[(v >> (64 * w)) & 0xFFFFFFFFFFFFFFFF for w in range(words)])
+
+
+def words_to_int(ws) -> int:
+    return sum(int(w) << (64 * i) for i, w in enumerate(ws))
 
 
 # ---------------------------------------------------------------------------
@@ -902,8 +924,12 @@ class TrajectoryBatch:
 
 
 class GpuSparseVector:
-    """The nonzero amplitudes of a register of up to 64 qubits in B200 memory:
+    """The nonzero amplitudes of a register of up to 1024 qubits in B200 memory:
     the drop-in for ``SparseVector<C64>`` (``src/state/sparse.rs``).
+
+    Basis indices are Python integers; on the device they are ``words`` 64-bit
+    words (1 up to 64 qubits, 4 up to 256, 16 up to 1024), ordered as ncsim's
+    ``Bits`` (``Vec<u64>``) order them.
 
     Entries are (basis index, complex128) pairs.  Gates that move each entry to
     one entry (monomials, permutations with phases, Paulis, diagonals) keep the
@@ -920,6 +946,12 @@ class GpuSparseVector:
             _handle = h
         self._h = _handle
         self.n = n
+        w = _u32()
+        _check(lib().ncsim_sparse_num_words(self._h, C.byref(w)))
+        self.words = w.value
+
+    def _w(self, v: int):
+        return int_to_words(v, self.words)
 
     @classmethod
     def zero_state(cls, n: int) -> "GpuSparseVector":
@@ -928,10 +960,18 @@ class GpuSparseVector:
     @classmethod
     def from_entries(cls, n: int, keys: Sequence[int], amps: Sequence[complex]) -> "GpuSparseVector":
         """``SparseVector::from_entries`` (sparse.rs:54-72): duplicates are added."""
-        k = np.ascontiguousarray(np.asarray(list(keys), dtype=np.uint64))
+        words = 1 if n <= 64 else 4 if n <= 256 else 16
+        if words == 1:
+            k = np.ascontiguousarray(np.asarray(list(keys), dtype=np.uint64))
+        else:
+            ks = [int(v) for v in keys]
+            k = np.zeros((len(ks), words), dtype=np.uint64)
+            for i, v in enumerate(ks):
+                for w in range(words):
+                    k[i, w] = (v >> (64 * w)) & 0xFFFFFFFFFFFFFFFF
         a = np.ascontiguousarray(np.asarray(list(amps), dtype=np.complex128))
         h = _vp()
-        _check(lib().ncsim_sparse_from_entries(n, k.ctypes.data_as(_P(_u64)), _dp(a.view(np.float64)), k.size,
+        _check(lib().ncsim_sparse_from_entries(n, k.ctypes.data_as(_P(_u64)), _dp(a.view(np.float64)), a.size,
                                                C.byref(h)))
         return cls(n, h)
 
@@ -959,12 +999,15 @@ class GpuSparseVector:
         return m.value
 
     def entries(self):
-        """(indices, amplitudes) in the current entry order."""
+        """(indices, amplitudes) in the current entry order: indices as a uint64
+        array (one word per entry) up to 64 qubits, as Python integers beyond."""
         m = self.num_entries()
-        k = np.empty(m, dtype=np.uint64)
+        k = np.empty((m, self.words), dtype=np.uint64)
         a = np.empty(2 * m, dtype=np.float64)
         _check(lib().ncsim_sparse_get_entries(self._h, k.ctypes.data_as(_P(_u64)), _dp(a), m))
-        return k, a.view(np.complex128)
+        if self.words == 1:
+            return k[:, 0].copy(), a.view(np.complex128)
+        return [words_to_int(row) for row in k], a.view(np.complex128)
 
     def sort(self) -> None:
         _check(lib().ncsim_sparse_sort(self._h))
@@ -973,6 +1016,9 @@ class GpuSparseVector:
         _check(lib().ncsim_sparse_apply_gate(self._h, gate._h, _u32s(qubits), len(qubits)))
 
     def apply_pauli(self, p: Pauli) -> None:
+        if self.words > 1:
+            _check(lib().ncsim_sparse_apply_pauli_words(self._h, self._w(p.x), self._w(p.z), self.words, p.phase))
+            return
         _check(lib().ncsim_sparse_apply_pauli(self._h, p.x, p.z, p.phase))
 
     def norm_sq(self) -> complex:
@@ -982,14 +1028,20 @@ class GpuSparseVector:
 
     def amplitude(self, index: int) -> complex:
         o = (_dbl * 2)()
-        _check(lib().ncsim_sparse_amplitude(self._h, index, o))
+        if self.words > 1:
+            _check(lib().ncsim_sparse_amplitude_words(self._h, self._w(index), self.words, o))
+        else:
+            _check(lib().ncsim_sparse_amplitude(self._h, index, o))
         return _complex(o)
 
     def expectation(self, p: Pauli) -> complex:
         if p.n != self.n:
             raise SimError(8, "expectation: operator on the wrong register")
         o = (_dbl * 2)()
-        _check(lib().ncsim_sparse_expectation(self._h, p.x, p.z, p.phase, o))
+        if self.words > 1:
+            _check(lib().ncsim_sparse_expectation_words(self._h, self._w(p.x), self._w(p.z), self.words, p.phase, o))
+        else:
+            _check(lib().ncsim_sparse_expectation(self._h, p.x, p.z, p.phase, o))
         return _complex(o)
 
     def inner(self, other: "GpuSparseVector") -> complex:
@@ -999,7 +1051,11 @@ class GpuSparseVector:
 
     def project(self, p: Pauli, outcome: bool) -> complex:
         o = (_dbl * 2)()
-        _check(lib().ncsim_sparse_project(self._h, p.x, p.z, p.phase, int(bool(outcome)), o))
+        if self.words > 1:
+            _check(lib().ncsim_sparse_project_words(self._h, self._w(p.x), self._w(p.z), self.words, p.phase,
+                                                    int(bool(outcome)), o))
+        else:
+            _check(lib().ncsim_sparse_project(self._h, p.x, p.z, p.phase, int(bool(outcome)), o))
         return _complex(o)
 
     def scale(self, c: complex) -> None:
@@ -1011,10 +1067,13 @@ class GpuSparseVector:
         _check(lib().ncsim_sparse_tensor(self._h, other._h, C.byref(h)))
         return GpuSparseVector(self.n + other.n, h)
 
-    def sample(self, rng: StdRng, shots: int) -> np.ndarray:
-        out = np.empty(shots, dtype=np.uint64)
+    def sample(self, rng: StdRng, shots: int):
+        """Shots as a uint64 array up to 64 qubits, as Python integers beyond."""
+        out = np.empty((shots, self.words), dtype=np.uint64)
         _check(lib().ncsim_sparse_sample(self._h, rng._h, shots, out.ctypes.data_as(_P(_u64))))
-        return out
+        if self.words == 1:
+            return out[:, 0].copy()
+        return [words_to_int(row) for row in out]
 
     def to_vector(self) -> np.ndarray:
         b = np.empty(2 << self.n, dtype=np.float64)
@@ -1023,7 +1082,11 @@ class GpuSparseVector:
 
     def measure(self, p: Pauli, rng: StdRng) -> bool:
         o = _i32()
-        _check(lib().ncsim_sparse_measure(self._h, p.x, p.z, p.phase, rng._h, C.byref(o)))
+        if self.words > 1:
+            _check(lib().ncsim_sparse_measure_words(self._h, self._w(p.x), self._w(p.z), self.words, p.phase, rng._h,
+                                                    C.byref(o)))
+        else:
+            _check(lib().ncsim_sparse_measure(self._h, p.x, p.z, p.phase, rng._h, C.byref(o)))
         return bool(o.value)
 
     def run(self, circuit: Circuit, rng: StdRng) -> list[bool]:

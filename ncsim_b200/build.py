@@ -25,6 +25,7 @@ SOURCES = [
     "csrc/batch.cu",
     "csrc/batch_plan.cpp",
     "csrc/sparse.cu",
+    "csrc/sparse_wide.cu",
     "csrc/frames.cu",
     "csrc/frames_plan.cpp",
     "csrc/host/ir.cpp",
@@ -35,6 +36,7 @@ SOURCES = [
 WORKLOAD_SOURCES = ["csrc/workloads/workloads.cpp"]
 HEADERS = [
     "csrc/engine.cuh",
+    "csrc/sparse_common.cuh",
     "csrc/host_math.hpp",
     "csrc/fused_plan.hpp",
     "csrc/batch_plan.hpp",

@@ -799,7 +799,8 @@ ncsim_circuit parse_circuit(const std::string& text) {
       if (c.n <= 64) {
         o.lowered = lower_gate(g, qs, c.n);
       } else {
-        // wider than any state form: the same checks, the gate lowered on its own qubits only
+        // wider than 64 qubits: the same checks, the gate lowered on its own qubits (local
+        // qubit j is qs[j]; the wide sparse form maps them back)
         std::vector<uint32_t> local(qs.size());
         for (size_t i = 0; i < qs.size(); ++i) {
           if (qs[i] >= c.n) throw qubit_out_of_range(qs[i], c.n);
@@ -807,7 +808,7 @@ ncsim_circuit parse_circuit(const std::string& text) {
             if (qs[j] == qs[i]) throw duplicate_qubit(qs[i]);
           local[i] = uint32_t(i);
         }
-        if (qs.size() <= 64) lower_gate(g, local, uint32_t(qs.size()));
+        if (qs.size() <= 64) o.lowered = lower_gate(g, local, uint32_t(qs.size()));
         else if (qs.size() != g.arity()) throw arity_error(g.text(), g.arity(), qs.size());
       }
     } catch (const Error& e) {

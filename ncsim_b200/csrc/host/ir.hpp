@@ -118,7 +118,7 @@ struct OpIR {
   OpKind kind = OpKind::Tick;
   GateIR gate;
   std::vector<uint32_t> qubits;
-  LoweredOp lowered;  // registers of at most 64 qubits (the state forms' limit)
+  LoweredOp lowered;  // on the register's qubits (n <= 64); wider: on local qubits 0..k-1 (= qubits[j])
   PauliOp pauli;      // measured Pauli, registers of at most 64 qubits
   PauliSites sites;   // measured Pauli, any register
   NoiseIR noise;

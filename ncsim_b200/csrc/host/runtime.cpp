@@ -263,6 +263,27 @@ ncsim_status ncsim_pauli_parse(const char* text, uint32_t n, uint64_t* x, uint64
   });
 }
 
+ncsim_status ncsim_pauli_parse_words(const char* text, uint32_t n, uint64_t* x, uint64_t* z, uint32_t words,
+                                     uint32_t* phase) {
+  return guarded([&] {
+    need(text, "text");
+    const PauliSites ps = parse_pauli_sites(text, int64_t(n));
+    if (uint64_t(words) * 64 < ps.n) throw Error(NCSIM_ERR_INVALID, "too few words for the Pauli's register");
+    uint32_t ys = 0;
+    for (uint32_t w = 0; w < words; ++w) {
+      if (x) x[w] = 0;
+      if (z) z[w] = 0;
+    }
+    for (const auto& st : ps.sites) {  // Y = i X Z: a Y site adds one to the phase
+      const uint32_t q = st.first;
+      if ((st.second & 1) && x) x[q >> 6] |= uint64_t(1) << (q & 63);
+      if ((st.second & 2) && z) z[q >> 6] |= uint64_t(1) << (q & 63);
+      ys += st.second == 3;
+    }
+    if (phase) *phase = (ps.phase + ys) & 3u;
+  });
+}
+
 // ---- trait methods on the device state ----
 ncsim_status ncsim_sv_apply_gate(ncsim_state* s, const ncsim_gate* g, const uint32_t* qubits, uint32_t k) {
   return guarded([&] {

@@ -12,75 +12,11 @@
 // Sums over entries (norm, expectation, inner product) are FP64 block partials
 // added on the host in a fixed order; Born sampling takes the cumulative
 // weights in entry order on the host, as sparse.rs:407-424 does.
-#include <cub/cub.cuh>
-
-#include <algorithm>
-#include <cmath>
-#include <memory>
-#include <mutex>
-#include <vector>
-
-#include "engine.cuh"
-#include "host/ir.hpp"
-#include "host/rng.hpp"
+#include "sparse_common.cuh"
 
 using namespace ncsim;
 
-struct ncsim_sparse {
-  uint32_t n = 0;
-  uint64_t m = 0;    // entries
-  uint64_t cap = 0;  // capacity of key/amp
-  uint64_t* key = nullptr;
-  double2* amp = nullptr;
-  bool sorted = true;
-  double cutoff = 0.0;
-  cudaStream_t stream = nullptr;
-  int device = 0;
-  double* partials = nullptr;       // device: SP_BLOCKS * 2 doubles
-  double* host_partials = nullptr;  // pinned mirror
-  cudaEvent_t timer0 = nullptr, timer1 = nullptr;
-  mutable std::recursive_mutex mu;
-};
-
 namespace {
-
-constexpr int SP_THREADS = 256;
-constexpr int SP_BLOCKS = 1024;  // reduction blocks (partials)
-constexpr uint32_t SP_MAX_K = 10;
-
-unsigned sp_grid(uint64_t items) {
-  uint64_t b = (items + SP_THREADS - 1) / SP_THREADS;
-  const uint64_t cap = uint64_t(sm_count()) * 16;
-  return unsigned(std::max<uint64_t>(1, std::min(b, cap)));
-}
-
-__device__ __forceinline__ double2 zmul(double2 a, double2 b) {
-  return make_double2(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x);
-}
-__device__ __forceinline__ double2 ipow(double2 v, uint32_t k) {  // i^k v
-  switch (k & 3u) {
-    case 0: return v;
-    case 1: return make_double2(-v.y, v.x);
-    case 2: return make_double2(-v.x, -v.y);
-    default: return make_double2(v.y, -v.x);
-  }
-}
-
-// the qubits of a gate and the local index of a key on them (sparse.rs:243-258)
-struct Qubits {
-  uint32_t k;
-  uint8_t q[SP_MAX_K];
-};
-__device__ __forceinline__ uint32_t local_of(uint64_t key, const Qubits& qs) {
-  uint32_t x = 0;
-  for (uint32_t j = 0; j < qs.k; ++j) x |= uint32_t((key >> qs.q[j]) & 1u) << j;
-  return x;
-}
-__device__ __forceinline__ uint64_t with_local(uint64_t key, const Qubits& qs, uint32_t y) {
-  for (uint32_t j = 0; j < qs.k; ++j)
-    key = (key & ~(uint64_t(1) << qs.q[j])) | (uint64_t((y >> j) & 1u) << qs.q[j]);
-  return key;
-}
 
 // ---- kernels that move each entry to one entry (order kept) ----
 // monomial: entry with local pattern x goes to image[x] with phase[x]
@@ -124,33 +60,6 @@ __global__ void k_sp_pauli(uint64_t* key, double2* amp, uint64_t m, uint64_t x, 
   }
 }
 
-// exp(2 pi i f / 2^bits) with exact quarter and eighth turns
-__device__ double2 turn_root(uint64_t f, uint32_t bits) {
-  const uint64_t mk = bits >= 64 ? ~uint64_t(0) : (uint64_t(1) << bits) - 1;
-  f &= mk;
-  if (bits >= 2 && (f & (mk >> 2)) == 0) {
-    switch ((f >> (bits - 2)) & 3u) {
-      case 0: return make_double2(1.0, 0.0);
-      case 1: return make_double2(0.0, 1.0);
-      case 2: return make_double2(-1.0, 0.0);
-      default: return make_double2(0.0, -1.0);
-    }
-  }
-  if (bits >= 3 && (f & (mk >> 3)) == 0) {
-    const double h = 0.70710678118654752440;
-    switch ((f >> (bits - 3)) & 7u) {
-      case 1: return make_double2(h, h);
-      case 3: return make_double2(-h, h);
-      case 5: return make_double2(-h, -h);
-      default: return make_double2(h, -h);
-    }
-  }
-  if (bits == 1) return f ? make_double2(-1.0, 0.0) : make_double2(1.0, 0.0);
-  double s, c;
-  sincospi(2.0 * double(f) / double(uint64_t(1) << std::min<uint32_t>(bits, 63)), &s, &c);
-  return make_double2(c, s);
-}
-
 // diagonal phase polynomial over global index parities (Diagonal(PhasePoly))
 struct SpPoly {
   uint32_t bits, nterms, scalar_is_one, use_table;
@@ -161,38 +70,6 @@ struct SpPoly {
   const uint64_t* coeff;
   const double2* table;
 };
-// amp *= scalar * zeta^f(key), f = constant + sum_t coeff_t prod_l [par_l . key] mod 2^bits
-// (and_mask, when given: a term whose parities are all single bits is the AND of
-// those bits, one compare instead of a popcount per parity; 0 for other terms)
-template <class Start>
-__device__ __forceinline__ void poly_apply(uint64_t kk, double2& amp, uint32_t bits, uint32_t nterms, uint64_t constant,
-                                           bool scalar_is_one, double2 scalar, bool use_table, const Start* start,
-                                           const uint64_t* par, const uint64_t* coeff, const double2* table,
-                                           const uint64_t* and_mask = nullptr) {
-  const uint64_t mk = bits >= 64 ? ~uint64_t(0) : (uint64_t(1) << bits) - 1;
-  uint64_t f = constant;
-  for (uint32_t t = 0; t < nterms; ++t) {
-    uint32_t all = 1;
-    const uint64_t am = and_mask ? and_mask[t] : 0;
-    if (am) {
-      all = (kk & am) == am;
-    } else {
-      for (uint32_t l = start[t]; l < start[t + 1]; ++l) all &= uint32_t(__popcll(par[l] & kk)) & 1u;
-    }
-    if (all) f += coeff[t];
-  }
-  f &= mk;
-  double2 c;
-  if (use_table) {
-    c = table[f];
-  } else {
-    if (f == 0 && scalar_is_one) return;
-    c = turn_root(f, bits);
-    if (!scalar_is_one) c = zmul(scalar, c);
-  }
-  if (c.x == 1.0 && c.y == 0.0) return;
-  amp = zmul(c, amp);
-}
 __global__ void k_sp_phasepoly(const uint64_t* key, double2* amp, uint64_t m, SpPoly P) {
   for (uint64_t i = uint64_t(blockIdx.x) * blockDim.x + threadIdx.x; i < m; i += uint64_t(gridDim.x) * blockDim.x)
     poly_apply(key[i], amp[i], P.bits, P.nterms, P.constant, P.scalar_is_one, P.scalar, P.use_table, P.start, P.par,
@@ -214,11 +91,6 @@ __global__ void k_sp_phasepoly_p(const uint64_t* key, double2* amp, uint64_t m, 
   for (uint64_t i = uint64_t(blockIdx.x) * blockDim.x + threadIdx.x; i < m; i += uint64_t(gridDim.x) * blockDim.x)
     poly_apply(key[i], amp[i], P.bits, P.nterms, P.constant, P.scalar_is_one, P.scalar, P.use_table, P.start, P.par,
                P.coeff, P.table);
-}
-
-__global__ void k_sp_scale(double2* amp, uint64_t m, double2 c) {
-  for (uint64_t i = uint64_t(blockIdx.x) * blockDim.x + threadIdx.x; i < m; i += uint64_t(gridDim.x) * blockDim.x)
-    amp[i] = zmul(c, amp[i]);
 }
 
 // ---- expansions (new entries, normalised afterwards) ----
@@ -327,45 +199,6 @@ __global__ void k_sp_run(uint64_t* key, double2* amp, uint64_t m, RunData d) {
   }
 }
 
-// ---- normalisation helpers ----
-struct ZAdd {
-  __device__ __forceinline__ double2 operator()(const double2& a, const double2& b) const {
-    return make_double2(a.x + b.x, a.y + b.y);
-  }
-};
-__global__ void k_sp_keep(const double2* amp, uint64_t m, double cut2, uint8_t* flag) {
-  for (uint64_t i = uint64_t(blockIdx.x) * blockDim.x + threadIdx.x; i < m; i += uint64_t(gridDim.x) * blockDim.x) {
-    const double2 a = amp[i];
-    const bool zero = a.x == 0.0 && a.y == 0.0;
-    flag[i] = !zero && (cut2 == 0.0 || a.x * a.x + a.y * a.y >= cut2);
-  }
-}
-
-// ---- sums (block partials, FP64) ----
-__device__ __forceinline__ void block_add2(double a, double b, double* out) {
-  __shared__ double red[SP_THREADS / 32][2];
-  for (int o = 16; o; o >>= 1) {
-    a += __shfl_down_sync(0xffffffffu, a, o);
-    b += __shfl_down_sync(0xffffffffu, b, o);
-  }
-  const int w = threadIdx.x >> 5, l = threadIdx.x & 31;
-  if (l == 0) red[w][0] = a, red[w][1] = b;
-  __syncthreads();
-  if (threadIdx.x == 0) {
-    double s0 = 0, s1 = 0;
-    for (int i = 0; i < SP_THREADS / 32; ++i) s0 += red[i][0], s1 += red[i][1];
-    out[2 * blockIdx.x] = s0;
-    out[2 * blockIdx.x + 1] = s1;
-  }
-}
-__global__ void k_sp_norm(const double2* amp, uint64_t m, double* part) {
-  double s = 0;
-  for (uint64_t i = uint64_t(blockIdx.x) * blockDim.x + threadIdx.x; i < m; i += uint64_t(gridDim.x) * blockDim.x) {
-    const double2 a = amp[i];
-    s += a.x * a.x + a.y * a.y;
-  }
-  block_add2(s, 0.0, part);
-}
 __device__ __forceinline__ int64_t find_key(const uint64_t* sk, uint64_t m, uint64_t x) {
   uint64_t lo = 0, hi = m;
   while (lo < hi) {
@@ -404,12 +237,6 @@ __global__ void k_sp_inner(const uint64_t* ka, const double2* va, uint64_t ma, c
   }
   block_add2(re, im, part);
 }
-__global__ void k_sp_abs2(const double2* amp, uint64_t m, double* out) {
-  for (uint64_t i = uint64_t(blockIdx.x) * blockDim.x + threadIdx.x; i < m; i += uint64_t(gridDim.x) * blockDim.x) {
-    const double2 a = amp[i];
-    out[i] = a.x * a.x + a.y * a.y;
-  }
-}
 __global__ void k_sp_find(const uint64_t* key, const double2* amp, uint64_t m, uint64_t x, int sorted, double2* out) {
   if (blockIdx.x == 0 && threadIdx.x == 0) {
     double2 r = make_double2(0.0, 0.0);
@@ -430,44 +257,13 @@ __global__ void k_sp_find(const uint64_t* key, const double2* amp, uint64_t m, u
 // ---------------------------------------------------------------------------
 // host side
 // ---------------------------------------------------------------------------
-struct Lock {
-  std::lock_guard<std::recursive_mutex> g;
-  explicit Lock(const ncsim_sparse* s) : g(s->mu) { NCSIM_CUDA(cudaSetDevice(s->device)); }
-};
-// two states locked together without an order between them (no deadlock when
-// other threads lock the same pair the other way round); a's device current
-struct PairLock {
-  std::unique_lock<std::recursive_mutex> la, lb;
-  PairLock(const ncsim_sparse* a, const ncsim_sparse* b) : la(a->mu, std::defer_lock), lb(b->mu, std::defer_lock) {
-    if (a == b) la.lock();
-    else std::lock(la, lb);
-    NCSIM_CUDA(cudaSetDevice(a->device));
-  }
-};
-
-template <class T>
-T* dalloc(size_t count, cudaStream_t st) {
-  void* p = nullptr;
-  NCSIM_CUDA(pool_alloc(&p, std::max<size_t>(1, count) * sizeof(T), st));
-  return static_cast<T*>(p);
-}
-void dfree(void* p, cudaStream_t st) {
-  if (p) cudaFreeAsync(p, st);
-}
-template <class T>
-T* upload(const std::vector<T>& v, cudaStream_t st) {
-  T* d = dalloc<T>(v.size(), st);
-  if (!v.empty()) NCSIM_CUDA(cudaMemcpyAsync(d, v.data(), v.size() * sizeof(T), cudaMemcpyHostToDevice, st));
-  return d;
-}
-
 void sp_reserve(ncsim_sparse* s, uint64_t need) {
   if (need <= s->cap) return;
   const uint64_t cap = std::max<uint64_t>(need, std::max<uint64_t>(1024, 2 * s->cap));
-  uint64_t* k = dalloc<uint64_t>(cap, s->stream);
+  uint64_t* k = dalloc<uint64_t>(cap * s->words, s->stream);
   double2* a = dalloc<double2>(cap, s->stream);
   if (s->m) {
-    NCSIM_CUDA(cudaMemcpyAsync(k, s->key, s->m * 8, cudaMemcpyDeviceToDevice, s->stream));
+    NCSIM_CUDA(cudaMemcpyAsync(k, s->key, s->m * 8 * s->words, cudaMemcpyDeviceToDevice, s->stream));
     NCSIM_CUDA(cudaMemcpyAsync(a, s->amp, s->m * 16, cudaMemcpyDeviceToDevice, s->stream));
   }
   dfree(s->key, s->stream);
@@ -530,6 +326,7 @@ void sp_normalize_from(ncsim_sparse* s, uint64_t* key, double2* amp, uint64_t cn
 }
 
 void sp_normalize(ncsim_sparse* s) {
+  if (s->words > 1) return spw::normalize(s);
   cudaStream_t st = s->stream;
   uint64_t* k = dalloc<uint64_t>(s->m, st);
   double2* a = dalloc<double2>(s->m, st);
@@ -561,6 +358,7 @@ void sp_sorted_copy(const ncsim_sparse* s, uint64_t*& k, double2*& a) {
 
 void sp_sort(ncsim_sparse* s) {
   if (s->sorted) return;
+  if (s->words > 1) return spw::sort(s);
   uint64_t* k;
   double2* a;
   sp_sorted_copy(s, k, a);
@@ -572,26 +370,6 @@ void sp_sort(ncsim_sparse* s) {
   s->sorted = true;
 }
 
-// the host sum of the block partials (fixed order)
-void sp_sum(const ncsim_sparse* s, unsigned blocks, double* out2) {
-  NCSIM_CUDA(cudaMemcpyAsync(s->host_partials, s->partials, size_t(blocks) * 2 * sizeof(double),
-                             cudaMemcpyDeviceToHost, s->stream));
-  NCSIM_CUDA(cudaStreamSynchronize(s->stream));
-  double a = 0, b = 0;
-  for (unsigned i = 0; i < blocks; ++i) a += s->host_partials[2 * i], b += s->host_partials[2 * i + 1];
-  out2[0] = a;
-  out2[1] = b;
-}
-unsigned red_grid(uint64_t m) { return unsigned(std::min<uint64_t>(SP_BLOCKS, std::max<uint64_t>(1, (m + SP_THREADS - 1) / SP_THREADS))); }
-
-double sp_norm(const ncsim_sparse* s) {
-  const unsigned g = red_grid(s->m);
-  k_sp_norm<<<g, SP_THREADS, 0, s->stream>>>(s->amp, s->m, s->partials);
-  NCSIM_LAUNCHED("sparse norm");
-  double r[2];
-  sp_sum(s, g, r);
-  return r[0];
-}
 
 void sp_expect(const ncsim_sparse* s, uint64_t x, uint64_t z, uint32_t phase, double* out) {
   const uint64_t* k = s->key;
@@ -661,27 +439,6 @@ void sp_monomial(ncsim_sparse* s, const std::vector<uint32_t>& qubits, const std
 }
 
 // a dense matrix (row-major 2^k x 2^k): permutations with phases in place, others by expansion
-// A dense view with one nonzero per column on distinct rows (a permutation with
-// phases, as CCX): every entry moves to one entry (sparse.rs:176-199).
-bool permutation_view(const std::vector<CplxD>& mat, size_t gd, std::vector<uint32_t>& image, std::vector<CplxD>& ph) {
-  image.assign(gd, 0);
-  ph.assign(gd, CplxD{0, 0});
-  std::vector<uint8_t> hit(gd, 0);
-  for (size_t b = 0; b < gd; ++b) {
-    int found = 0;
-    for (size_t a = 0; a < gd; ++a) {
-      const CplxD e = mat[a * gd + b];
-      if (e.re == 0.0 && e.im == 0.0) continue;
-      if (++found > 1 || hit[a]) return false;
-      hit[a] = 1;
-      image[b] = uint32_t(a);
-      ph[b] = e;
-    }
-    if (found != 1) return false;
-  }
-  return true;
-}
-
 void sp_matrix(ncsim_sparse* s, const std::vector<uint32_t>& qubits, const std::vector<CplxD>& mat) {
   const uint32_t k = uint32_t(qubits.size());
   if (k > SP_MAX_K) throw Error(NCSIM_ERR_UNSUPPORTED, "sparse dense gate on more than 10 qubits");
@@ -972,9 +729,10 @@ int sp_apply_op(ncsim_sparse* s, const OpIR& op, ncsim_rng& rng) {
 }
 
 ncsim_sparse* sp_new(uint32_t n) {
-  if (n == 0 || n > 64) throw Error(NCSIM_ERR_INVALID, "sparse register of " + std::to_string(n) + " qubits (1..64)");
+  const uint32_t words = spw::words_for(n);  // checks 1 <= n <= 1024
   auto s = std::make_unique<ncsim_sparse>();
   s->n = n;
+  s->words = words;
   NCSIM_CUDA(cudaGetDevice(&s->device));
   NCSIM_CUDA(cudaStreamCreateWithFlags(&s->stream, cudaStreamNonBlocking));
   NCSIM_CUDA(cudaMalloc(&s->partials, SP_BLOCKS * 2 * sizeof(double)));
@@ -999,6 +757,7 @@ void sp_release(ncsim_sparse* s) {
 }
 
 void set_entries(ncsim_sparse* s, const uint64_t* keys, const double* amps, uint64_t count) {
+  if (s->words > 1) return spw::set_entries(s, keys, amps, count);
   const uint64_t mask = s->n >= 64 ? ~uint64_t(0) : (uint64_t(1) << s->n) - 1;
   std::vector<uint64_t> k(count);
   for (uint64_t i = 0; i < count; ++i) k[i] = keys[i] & mask;
@@ -1008,8 +767,26 @@ void set_entries(ncsim_sparse* s, const uint64_t* keys, const double* amps, uint
   sp_normalize_from(s, dk, da, count);
 }
 
-void need(const void* p, const char* what) {
-  if (!p) throw Error(NCSIM_ERR_INVALID, std::string(what) + " is null");
+
+// a one-word mask on a register of any width (qubits 0..63)
+std::vector<uint64_t> word0(const ncsim_sparse* s, uint64_t v) {
+  std::vector<uint64_t> w(s->words, 0);
+  w[0] = v;
+  return w;
+}
+// checks a caller's word arrays: their count is the register's and no bit lies outside it
+void check_words(const ncsim_sparse* s, uint32_t words, std::initializer_list<const uint64_t*> masks) {
+  if (words != s->words)
+    throw Error(NCSIM_ERR_INVALID, "masks of " + std::to_string(words) + " words on a register keyed by " +
+                                       std::to_string(s->words));
+  for (const uint64_t* m : masks) {
+    need(m, "mask");
+    for (uint32_t w = 0; w < words; ++w) {
+      const uint32_t lo = 64 * w;
+      const uint64_t keep = s->n >= lo + 64 ? ~uint64_t(0) : s->n <= lo ? 0 : (uint64_t(1) << (s->n - lo)) - 1;
+      if (m[w] & ~keep) throw Error(NCSIM_ERR_INVALID, "Pauli on qubits outside the register");
+    }
+  }
 }
 
 }  // namespace
@@ -1021,9 +798,9 @@ ncsim_status ncsim_sparse_create(uint32_t n, ncsim_sparse** out) {
     need(out, "out");
     ncsim_sparse* s = sp_new(n);
     try {
-      const uint64_t zero = 0;
+      const std::vector<uint64_t> zero(s->words, 0);
       const double one[2] = {1.0, 0.0};
-      set_entries(s, &zero, one, 1);
+      set_entries(s, zero.data(), one, 1);
     } catch (...) {
       sp_release(s);
       throw;
@@ -1066,7 +843,7 @@ ncsim_status ncsim_sparse_clone(const ncsim_sparse* s, ncsim_sparse** out) {
       NCSIM_CUDA(cudaStreamSynchronize(s->stream));
       sp_reserve(c, s->m);
       if (s->m) {
-        NCSIM_CUDA(cudaMemcpyAsync(c->key, s->key, s->m * 8, cudaMemcpyDeviceToDevice, c->stream));
+        NCSIM_CUDA(cudaMemcpyAsync(c->key, s->key, s->m * 8 * s->words, cudaMemcpyDeviceToDevice, c->stream));
         NCSIM_CUDA(cudaMemcpyAsync(c->amp, s->amp, s->m * 16, cudaMemcpyDeviceToDevice, c->stream));
       }
       c->m = s->m;
@@ -1114,7 +891,7 @@ ncsim_status ncsim_sparse_get_entries(const ncsim_sparse* s, uint64_t* keys, dou
     if (s->m) {
       need(keys, "keys");
       need(amps, "amps");
-      NCSIM_CUDA(cudaMemcpyAsync(keys, s->key, s->m * 8, cudaMemcpyDeviceToHost, s->stream));
+      NCSIM_CUDA(cudaMemcpyAsync(keys, s->key, s->m * 8 * s->words, cudaMemcpyDeviceToHost, s->stream));
       NCSIM_CUDA(cudaMemcpyAsync(amps, s->amp, s->m * 16, cudaMemcpyDeviceToHost, s->stream));
     }
     NCSIM_CUDA(cudaStreamSynchronize(s->stream));
@@ -1135,6 +912,7 @@ ncsim_status ncsim_sparse_apply_gate(ncsim_sparse* s, const ncsim_gate* g, const
     need(g, "gate");
     if (k) need(qubits, "qubits");
     Lock lk(s);
+    if (s->words > 1) return spw::apply_gate(s, g->g, std::vector<uint32_t>(qubits, qubits + k));
     const LoweredOp op = lower_gate(g->g, std::vector<uint32_t>(qubits, qubits + k), s->n);
     sp_apply_lowered(s, op);
   });
@@ -1146,6 +924,7 @@ ncsim_status ncsim_sparse_apply_pauli(ncsim_sparse* s, uint64_t x, uint64_t z, u
     const uint64_t mask = s->n >= 64 ? ~uint64_t(0) : (uint64_t(1) << s->n) - 1;
     if ((x | z) & ~mask) throw Error(NCSIM_ERR_INVALID, "Pauli on qubits outside the register");
     Lock lk(s);
+    if (s->words > 1) return spw::pauli(s, word0(s, x).data(), word0(s, z).data(), phase);
     sp_pauli(s, x, z, phase);
   });
 }
@@ -1165,6 +944,7 @@ ncsim_status ncsim_sparse_amplitude(const ncsim_sparse* s, uint64_t index, doubl
     need(s, "state");
     need(re_im, "out");
     Lock lk(s);
+    if (s->words > 1) return spw::amplitude(s, word0(s, index).data(), re_im);
     const uint64_t mask = s->n >= 64 ? ~uint64_t(0) : (uint64_t(1) << s->n) - 1;
     double2* d = dalloc<double2>(1, s->stream);
     k_sp_find<<<1, 32, 0, s->stream>>>(s->key, s->amp, s->m, index & mask, s->sorted ? 1 : 0, d);
@@ -1185,6 +965,7 @@ ncsim_status ncsim_sparse_expectation(const ncsim_sparse* s, uint64_t x, uint64_
     const uint64_t mask = s->n >= 64 ? ~uint64_t(0) : (uint64_t(1) << s->n) - 1;
     if ((x | z) & ~mask) throw Error(NCSIM_ERR_INVALID, "expectation: operator on the wrong register");
     Lock lk(s);
+    if (s->words > 1) return spw::expectation(s, word0(s, x).data(), word0(s, z).data(), phase & 3u, re_im);
     sp_expect(s, x, z, phase & 3u, re_im);
   });
 }
@@ -1197,6 +978,7 @@ ncsim_status ncsim_sparse_inner(const ncsim_sparse* a, const ncsim_sparse* b, do
     if (a->n != b->n) throw Error(NCSIM_ERR_INVALID, "inner: register sizes differ");
     PairLock lk(a, b);
     NCSIM_CUDA(cudaStreamSynchronize(b->stream));
+    if (a->words > 1) return spw::inner(a, b, re_im);
     uint64_t* kb = b->key;
     double2* vb = b->amp;
     uint64_t* kc = nullptr;
@@ -1226,7 +1008,8 @@ ncsim_status ncsim_sparse_project(ncsim_sparse* s, uint64_t x, uint64_t z, uint3
     p.phase = phase & 3u;
     if (!p.hermitian()) throw Error(NCSIM_ERR_INVALID, "projector of a non-Hermitian Pauli");
     Lock lk(s);
-    const double w = sp_project(s, x, z, phase, outcome != 0);
+    const double w = s->words > 1 ? spw::project(s, word0(s, x).data(), word0(s, z).data(), phase, outcome != 0)
+                                  : sp_project(s, x, z, phase, outcome != 0);
     if (weight_re_im) weight_re_im[0] = w, weight_re_im[1] = 0.0;
   });
 }
@@ -1248,10 +1031,24 @@ ncsim_status ncsim_sparse_tensor(const ncsim_sparse* a, const ncsim_sparse* b, n
     need(a, "a");
     need(b, "b");
     need(out, "out");
-    if (a->n + b->n > 64) throw Error(NCSIM_ERR_UNSUPPORTED, "sparse tensor product of more than 64 qubits");
+    if (a->n + b->n > spw::MAX_QUBITS)
+      throw Error(NCSIM_ERR_UNSUPPORTED, "sparse tensor product of more than " + std::to_string(spw::MAX_QUBITS) + " qubits");
     PairLock lk(a, b);
     NCSIM_CUDA(cudaStreamSynchronize(a->stream));
     NCSIM_CUDA(cudaStreamSynchronize(b->stream));
+    if (a->n + b->n > 64) {  // keys of several words
+      ncsim_sparse* c = sp_new(a->n + b->n);
+      try {
+        c->cutoff = a->cutoff;
+        spw::tensor(a, b, c);
+        NCSIM_CUDA(cudaStreamSynchronize(c->stream));
+      } catch (...) {
+        sp_release(c);
+        throw;
+      }
+      *out = c;
+      return;
+    }
     const uint64_t tot = a->m * b->m;
     if (tot > uint64_t(INT32_MAX)) throw Error(NCSIM_ERR_UNSUPPORTED, "sparse state of more than 2^31 entries");
     ncsim_sparse* c = sp_new(a->n + b->n);
@@ -1280,6 +1077,7 @@ ncsim_status ncsim_sparse_sample(const ncsim_sparse* s, ncsim_rng* rng, uint64_t
     need(rng, "rng");
     if (shots) need(out, "out");
     Lock lk(s);
+    if (s->words > 1) return spw::sample(s, *rng, shots, out);
     std::vector<double> w(s->m);
     std::vector<uint64_t> keys(s->m);
     if (s->m) {
@@ -1337,7 +1135,8 @@ ncsim_status ncsim_sparse_measure(ncsim_sparse* s, uint64_t x, uint64_t z, uint3
     p.x = x;
     p.z = z;
     p.phase = phase & 3u;
-    const bool o = sp_measure(s, p, *rng);
+    const bool o = s->words > 1 ? spw::measure(s, word0(s, x).data(), word0(s, z).data(), phase & 3u, *rng)
+                                : sp_measure(s, p, *rng);
     if (outcome) *outcome = o ? 1 : 0;
   });
 }
@@ -1353,6 +1152,12 @@ ncsim_status ncsim_sparse_run(ncsim_sparse* s, const ncsim_circuit* c, ncsim_rng
     if (c->num_measurements()) need(rec, "record");
     Lock lk(s);
     size_t m = 0;
+    if (s->words > 1) {
+      spw::run(s, *c, *rng, rec, m);
+      NCSIM_CUDA(cudaStreamSynchronize(s->stream));
+      if (len) *len = m;
+      return;
+    }
     // runs of one-to-one ops (gates with a monomial, diagonal or Pauli view, and the
     // Paulis of sampled noise) go to the device as one pass each; a measurement, a
     // reset or a gate that creates entries ends a run
@@ -1401,6 +1206,94 @@ ncsim_status ncsim_sparse_run(ncsim_sparse* s, const ncsim_circuit* c, ncsim_rng
     run.launch(s);
     NCSIM_CUDA(cudaStreamSynchronize(s->stream));
     if (len) *len = m;
+  });
+}
+
+ncsim_status ncsim_sparse_num_words(const ncsim_sparse* s, uint32_t* words) {
+  return guarded([&] {
+    need(s, "state");
+    need(words, "words");
+    *words = s->words;
+  });
+}
+
+ncsim_status ncsim_sparse_apply_pauli_words(ncsim_sparse* s, const uint64_t* x, const uint64_t* z, uint32_t words,
+                                            uint32_t phase) {
+  return guarded([&] {
+    need(s, "state");
+    check_words(s, words, {x, z});
+    Lock lk(s);
+    if (s->words > 1) return spw::pauli(s, x, z, phase);
+    sp_pauli(s, x[0], z[0], phase);
+  });
+}
+
+ncsim_status ncsim_sparse_amplitude_words(const ncsim_sparse* s, const uint64_t* index, uint32_t words,
+                                          double* re_im) {
+  return guarded([&] {
+    need(s, "state");
+    need(re_im, "out");
+    need(index, "index");
+    if (words != s->words) throw Error(NCSIM_ERR_INVALID, "index of the wrong word count");
+    if (s->words == 1) {
+      const ncsim_status r = ncsim_sparse_amplitude(s, index[0], re_im);
+      if (r) throw Error(r, ncsim_last_error());
+      return;
+    }
+    std::vector<uint64_t> idx(index, index + words);
+    const uint32_t top = s->n - 64 * (words - 1);  // bits of the register in the last word
+    if (top < 64) idx[words - 1] &= (uint64_t(1) << top) - 1;
+    Lock lk(s);
+    spw::amplitude(s, idx.data(), re_im);
+  });
+}
+
+ncsim_status ncsim_sparse_expectation_words(const ncsim_sparse* s, const uint64_t* x, const uint64_t* z,
+                                            uint32_t words, uint32_t phase, double* re_im) {
+  return guarded([&] {
+    need(s, "state");
+    need(re_im, "out");
+    check_words(s, words, {x, z});
+    Lock lk(s);
+    if (s->words > 1) return spw::expectation(s, x, z, phase & 3u, re_im);
+    sp_expect(s, x[0], z[0], phase & 3u, re_im);
+  });
+}
+
+ncsim_status ncsim_sparse_project_words(ncsim_sparse* s, const uint64_t* x, const uint64_t* z, uint32_t words,
+                                        uint32_t phase, int32_t outcome, double* weight_re_im) {
+  return guarded([&] {
+    need(s, "state");
+    check_words(s, words, {x, z});
+    uint32_t c = 0;
+    for (uint32_t w = 0; w < words; ++w) c += uint32_t(__builtin_popcountll(x[w] & z[w]));
+    if (((phase & 1u) == 1u) != bool(c & 1u)) throw Error(NCSIM_ERR_INVALID, "projector of a non-Hermitian Pauli");
+    Lock lk(s);
+    const double w = s->words > 1 ? spw::project(s, x, z, phase, outcome != 0)
+                                  : sp_project(s, x[0], z[0], phase, outcome != 0);
+    if (weight_re_im) weight_re_im[0] = w, weight_re_im[1] = 0.0;
+  });
+}
+
+ncsim_status ncsim_sparse_measure_words(ncsim_sparse* s, const uint64_t* x, const uint64_t* z, uint32_t words,
+                                        uint32_t phase, ncsim_rng* rng, int32_t* outcome) {
+  return guarded([&] {
+    need(s, "state");
+    need(rng, "rng");
+    check_words(s, words, {x, z});
+    Lock lk(s);
+    bool o;
+    if (s->words > 1) {
+      o = spw::measure(s, x, z, phase & 3u, *rng);
+    } else {
+      PauliOp p;
+      p.n = s->n;
+      p.x = x[0];
+      p.z = z[0];
+      p.phase = phase & 3u;
+      o = sp_measure(s, p, *rng);
+    }
+    if (outcome) *outcome = o ? 1 : 0;
   });
 }
 

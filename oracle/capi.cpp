@@ -5,6 +5,7 @@
 // leave a message in oracle_last_error().
 #include "frames_ref.hpp"
 #include "ncsim_ref.hpp"
+#include "sparse_wide_ref.hpp"
 #include "workloads_ref.hpp"
 
 #include <chrono>
@@ -333,6 +334,57 @@ void oracle_sparse_get(void* h, uint64_t* idx, double* amp) {
 }
 void oracle_sparse_free(void* h) { delete (SparseState*)h; }
 
+
+// ---- sparse restatement on registers of any width (sparse.rs with Bits keys) ----
+// Runs the circuit from |0...0> with StdRng::seed_from_u64(seed); rec gets the record.
+void* oracle_wsparse_run(const char* text, uint64_t seed, uint8_t* rec, size_t cap, size_t* len) {
+  WideSparse* s = nullptr;
+  int st = guard([&] {
+    Circuit c = Circuit::parse(text);
+    auto w = std::make_unique<WideSparse>(WideSparse::zero_state(c.n));
+    StdRng rng = StdRng::seed_from_u64(seed);
+    auto r = w->run(c, rng);
+    if (r.size() > cap) throw SimError(ErrKind::Invalid, "record buffer too small");
+    for (size_t i = 0; i < r.size(); ++i) rec[i] = r[i];
+    *len = r.size();
+    s = w.release();
+  });
+  return st == 0 ? s : nullptr;
+}
+uint64_t oracle_wsparse_len(void* h) { return ((WideSparse*)h)->ent.size(); }
+uint32_t oracle_wsparse_words(void* h) { return uint32_t(nwords(((WideSparse*)h)->n)); }
+// entries in entry order: nwords(n) words per key
+void oracle_wsparse_get(void* h, uint64_t* keys, double* amps) {
+  auto* s = (WideSparse*)h;
+  const size_t W = nwords(s->n);
+  for (size_t i = 0; i < s->ent.size(); ++i) {
+    std::memcpy(keys + i * W, s->ent[i].first.data(), W * 8);
+    amps[2 * i] = s->ent[i].second.re;
+    amps[2 * i + 1] = s->ent[i].second.im;
+  }
+}
+int oracle_wsparse_expect(void* h, const char* pauli, double* re_im) {
+  return guard([&] {
+    auto* s = (WideSparse*)h;
+    WidePauli w = WidePauli::parse_with(pauli, s->n);
+    Bits x, z;
+    uint32_t ph = 0;
+    s->sites_words(w, x, z, ph);
+    C64 e = s->expectation(x, z, ph);
+    re_im[0] = e.re;
+    re_im[1] = e.im;
+  });
+}
+int oracle_wsparse_sample(void* h, uint64_t seed, uint64_t shots, uint64_t* out) {
+  return guard([&] {
+    auto* s = (WideSparse*)h;
+    StdRng rng = StdRng::seed_from_u64(seed);
+    auto v = s->sample(rng, shots);
+    const size_t W = nwords(s->n);
+    for (size_t i = 0; i < v.size(); ++i) std::memcpy(out + i * W, v[i].data(), W * 8);
+  });
+}
+void oracle_wsparse_free(void* h) { delete (WideSparse*)h; }
 
 // ---- frame sampler (frame.rs) ----
 // The reference record of FrameSampler::new; returns the number of measurements.

@@ -87,6 +87,13 @@ def lib():
             "oracle_sparse_len": (u64, [vp]),
             "oracle_sparse_get": (None, [vp, P(u64), P(dbl)]),
             "oracle_sparse_free": (None, [vp]),
+            "oracle_wsparse_run": (vp, [C.c_char_p, u64, P(C.c_uint8), C.c_size_t, P(C.c_size_t)]),
+            "oracle_wsparse_len": (u64, [vp]),
+            "oracle_wsparse_words": (u32, [vp]),
+            "oracle_wsparse_get": (None, [vp, P(u64), P(dbl)]),
+            "oracle_wsparse_expect": (i32, [vp, C.c_char_p, P(dbl)]),
+            "oracle_wsparse_sample": (i32, [vp, u64, u64, P(u64)]),
+            "oracle_wsparse_free": (None, [vp]),
             "oracle_frames_reference": (i32, [C.c_char_p, u64, P(C.c_uint8), C.c_size_t]),
             "oracle_frames_sample_packed": (i32, [C.c_char_p, P(C.c_uint8), C.c_size_t, u64, P(u64), C.c_size_t, i32,
                                                   P(u64)]),
@@ -346,6 +353,48 @@ def sparse_run(text: str):
         return idx, amp.view(np.complex128)
     finally:
         lib().oracle_sparse_free(h)
+
+
+class WideSparse:
+    """The sparse restatement on a register of any width after running a circuit
+    text from |0...0> with StdRng::seed_from_u64(seed): the record, the entries in
+    entry order (keys as Python integers), expectations and samples."""
+
+    def __init__(self, text: str, seed: int, max_record: int = 4096):
+        rec = (C.c_uint8 * max(1, max_record))()
+        ln = C.c_size_t()
+        h = lib().oracle_wsparse_run(text.encode(), seed, rec, max_record, C.byref(ln))
+        if not h:
+            raise OracleError(-8, lib().oracle_last_error().decode())
+        self._h = h
+        self.record = [bool(rec[i]) for i in range(ln.value)]
+        self.words = lib().oracle_wsparse_words(h)
+
+    def __del__(self):
+        h = getattr(self, "_h", None)
+        if h:
+            lib().oracle_wsparse_free(h)
+            self._h = None
+
+    def _ints(self, arr):
+        return [sum(int(w) << (64 * j) for j, w in enumerate(row)) for row in arr.reshape(-1, self.words)]
+
+    def entries(self):
+        m = lib().oracle_wsparse_len(self._h)
+        k = np.zeros(m * self.words, dtype=np.uint64)
+        a = np.zeros(2 * m, dtype=np.float64)
+        lib().oracle_wsparse_get(self._h, k.ctypes.data_as(C.POINTER(C.c_uint64)), _dp(a))
+        return self._ints(k), a.view(np.complex128)
+
+    def expectation(self, pauli: str) -> complex:
+        o = (C.c_double * 2)()
+        _check(lib().oracle_wsparse_expect(self._h, pauli.encode(), o))
+        return complex(o[0], o[1])
+
+    def sample(self, seed: int, shots: int):
+        out = np.zeros(shots * self.words, dtype=np.uint64)
+        _check(lib().oracle_wsparse_sample(self._h, seed, shots, out.ctypes.data_as(C.POINTER(C.c_uint64))))
+        return self._ints(out)
 
 
 FRAME_BATCH = 1 << 14

@@ -161,6 +161,7 @@ extern "C" {
     pub fn ncsim_gate_free(g: *mut ncsim_gate) -> ncsim_status;
     pub fn ncsim_gate_lowered_matrix(g: *const ncsim_gate, out: *mut f64, cap_doubles: usize, k: *mut u32) -> ncsim_status;
     pub fn ncsim_pauli_parse(text: *const c_char, n: u32, x: *mut u64, z: *mut u64, phase: *mut u32) -> ncsim_status;
+    pub fn ncsim_pauli_parse_words(text: *const c_char, n: u32, x: *mut u64, z: *mut u64, words: u32, phase: *mut u32) -> ncsim_status;
     pub fn ncsim_sv_apply_gate(s: *mut ncsim_state, g: *const ncsim_gate, qubits: *const u32, k: u32) -> ncsim_status;
     pub fn ncsim_sv_measure(s: *mut ncsim_state, x: u64, z: u64, phase: u32, rng: *mut ncsim_rng, outcome: *mut i32) -> ncsim_status;
     pub fn ncsim_sv_run(s: *mut ncsim_state, c: *const ncsim_circuit, rng: *mut ncsim_rng, rec: *mut u8, cap: usize, len: *mut usize) -> ncsim_status;
@@ -205,6 +206,12 @@ extern "C" {
     pub fn ncsim_sparse_to_vector(s: *const ncsim_sparse, amps: *mut f64, len: u64) -> ncsim_status;
     pub fn ncsim_sparse_measure(s: *mut ncsim_sparse, x: u64, z: u64, phase: u32, rng: *mut ncsim_rng, outcome: *mut i32) -> ncsim_status;
     pub fn ncsim_sparse_run(s: *mut ncsim_sparse, c: *const ncsim_circuit, rng: *mut ncsim_rng, rec: *mut u8, cap: usize, len: *mut usize) -> ncsim_status;
+    pub fn ncsim_sparse_num_words(s: *const ncsim_sparse, words: *mut u32) -> ncsim_status;
+    pub fn ncsim_sparse_apply_pauli_words(s: *mut ncsim_sparse, x: *const u64, z: *const u64, words: u32, phase: u32) -> ncsim_status;
+    pub fn ncsim_sparse_amplitude_words(s: *const ncsim_sparse, index: *const u64, words: u32, re_im: *mut f64) -> ncsim_status;
+    pub fn ncsim_sparse_expectation_words(s: *const ncsim_sparse, x: *const u64, z: *const u64, words: u32, phase: u32, re_im: *mut f64) -> ncsim_status;
+    pub fn ncsim_sparse_project_words(s: *mut ncsim_sparse, x: *const u64, z: *const u64, words: u32, phase: u32, outcome: i32, weight_re_im: *mut f64) -> ncsim_status;
+    pub fn ncsim_sparse_measure_words(s: *mut ncsim_sparse, x: *const u64, z: *const u64, words: u32, phase: u32, rng: *mut ncsim_rng, outcome: *mut i32) -> ncsim_status;
     pub fn ncsim_sparse_synchronize(s: *const ncsim_sparse) -> ncsim_status;
     pub fn ncsim_sparse_timer_start(s: *mut ncsim_sparse) -> ncsim_status;
     pub fn ncsim_sparse_timer_stop(s: *mut ncsim_sparse, milliseconds: *mut f64) -> ncsim_status;

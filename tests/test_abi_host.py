@@ -127,8 +127,8 @@ def test_state_argument_errors_need_no_device(nb):
     assert nb.lib().ncsim_sv_create(10, 7, ctypes.byref(h)) == 8
     assert nb.lib().ncsim_sv_norm_sq(None, (ctypes.c_double * 2)()) == 8
     assert "null" in nb.lib().ncsim_last_error().decode()
-    # the sparse form: register sizes 1..64 and null handles, checked before any device call
-    assert nb.lib().ncsim_sparse_create(65, ctypes.byref(h)) == 8
+    # the sparse form: register sizes 1..1024 and null handles, checked before any device call
+    assert nb.lib().ncsim_sparse_create(1025, ctypes.byref(h)) == 8
     assert nb.lib().ncsim_sparse_create(0, ctypes.byref(h)) == 8
     assert nb.lib().ncsim_sparse_norm_sq(None, (ctypes.c_double * 2)()) == 8
     assert nb.lib().ncsim_sparse_run(None, None, None, None, 0, None) == 8

@@ -156,7 +156,7 @@ def test_tensor_scale_and_cutoff(nb):
 
 def test_errors(nb):
     with pytest.raises(nb.SimError):
-        nb.GpuSparseVector(65)
+        nb.GpuSparseVector(1025)  # registers of 1..1024 qubits
     s = nb.GpuSparseVector(4)
     with pytest.raises(nb.SimError):
         s.expectation(nb.Pauli(5, 0, 1, 0))
