@@ -20,6 +20,7 @@
 // the chunk copies and the FP64 sums conflict-free.
 #include <algorithm>
 #include <array>
+#include <mutex>
 #include <atomic>
 #include <cstdlib>
 #include <fstream>
@@ -794,11 +795,13 @@ void ensure_device(ncsim_batch* b) {
   NCSIM_CUDA(cudaMallocHost(&b->h_z0, size_t(c) * 8));
   NCSIM_CUDA(cudaMallocHost(&b->h_norm, size_t(c) * 8));
   NCSIM_CUDA(cudaMallocHost(&b->h_err, sizeof(uint32_t)));
+  static std::mutex attr_mu;  // batches on several host threads may race here
   static bool attr_done[64] = {};
-  if (dev < 64 && !attr_done[dev]) {
+  std::lock_guard<std::mutex> lk(attr_mu);
+  if (dev < 0 || dev >= 64 || !attr_done[dev]) {
     NCSIM_CUDA(cudaFuncSetAttribute(k_batch<2>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(SMEM_NBUF2)));
     NCSIM_CUDA(cudaFuncSetAttribute(k_batch<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(SMEM_NBUF1)));
-    attr_done[dev] = true;
+    if (dev >= 0 && dev < 64) attr_done[dev] = true;
   }
 }
 

@@ -710,7 +710,7 @@ TermClass term_class(uint32_t tm, const CplxD& c) {
   return T_GENERIC;
 }
 
-std::unique_ptr<DevicePlan> build_device_plan(const ncsim_circuit& c, uint32_t max_fuse) {
+std::unique_ptr<DevicePlan> build_device_plan(const ncsim_circuit& c, uint32_t max_fuse, cudaStream_t stream) {
   auto dp = std::make_unique<DevicePlan>();
   dp->plan = make_plan(c, max_fuse);
   std::vector<uint8_t> images;
@@ -835,7 +835,10 @@ std::unique_ptr<DevicePlan> build_device_plan(const ncsim_circuit& c, uint32_t m
   }
   if (!images.empty()) {
     NCSIM_CUDA(cudaMalloc(&dp->rops, images.size()));
-    NCSIM_CUDA(cudaMemcpy(dp->rops, images.data(), images.size(), cudaMemcpyHostToDevice));
+    // on the state's stream, waited for: a pageable cudaMemcpy may return before its DMA lands,
+    // and the pass kernels' non-blocking stream does not wait for the legacy stream
+    NCSIM_CUDA(cudaMemcpyAsync(dp->rops, images.data(), images.size(), cudaMemcpyHostToDevice, stream));
+    NCSIM_CUDA(cudaStreamSynchronize(stream));
   }
   for (auto& P : dp->params) P.rops = reinterpret_cast<const uint4*>(dp->rops + uintptr_t(P.rops));
   NCSIM_CUDA(cudaGetDevice(&dp->device));
@@ -856,13 +859,13 @@ namespace {
 std::mutex g_fused_mu;
 
 // the circuit's device plan for this device and fusion width (built once)
-std::shared_ptr<fused::DevicePlan> device_plan_for(const ncsim_circuit* c, uint32_t max_fuse) {
+std::shared_ptr<fused::DevicePlan> device_plan_for(const ncsim_circuit* c, uint32_t max_fuse, cudaStream_t stream) {
   std::lock_guard<std::mutex> lk(g_fused_mu);
   int dev = 0;
   NCSIM_CUDA(cudaGetDevice(&dev));
   if (c->fused_plan && c->fused_plan_fuse == max_fuse && c->fused_plan_device == dev)
     return std::static_pointer_cast<fused::DevicePlan>(c->fused_plan);
-  std::shared_ptr<fused::DevicePlan> dp(fused::build_device_plan(*c, max_fuse).release());
+  std::shared_ptr<fused::DevicePlan> dp(fused::build_device_plan(*c, max_fuse, stream).release());
   c->fused_plan = dp;
   c->fused_plan_fuse = max_fuse;
   c->fused_plan_device = dev;
@@ -881,7 +884,7 @@ extern "C" ncsim_status ncsim_sv_run_fused(ncsim_state* s, const ncsim_circuit* 
       if (!rec) throw Error(NCSIM_ERR_INVALID, "record is null");
     }
     std::lock_guard<std::recursive_mutex> lk(s->mu);
-    std::shared_ptr<fused::DevicePlan> dp = device_plan_for(c, max_fuse ? max_fuse : 5);
+    std::shared_ptr<fused::DevicePlan> dp = device_plan_for(c, max_fuse ? max_fuse : 5, s->stream);
     int* d_err = s->dev_flag;  // the state's own word: no allocation per run
     NCSIM_CUDA(cudaMemsetAsync(d_err, 0, sizeof(int), s->stream));
     NCSIM_CUDA(cudaFuncSetAttribute(fused::k_fused_pass, cudaFuncAttributeMaxDynamicSharedMemorySize, fused::SM_DYNAMIC));

@@ -1410,7 +1410,10 @@ int launch_compare_partials(const ncsim_state* a, const ncsim_state* b, double* 
 
 int launch_project_partials(ncsim_state* s, uint64_t x, uint64_t z, uint32_t phase, bool outcome) {
   int g;
-  ProfScope ps(s, K_PROJECT, x ? full_bytes(s) : 0.75 * full_bytes(s));
+  // a diagonal projection reads every amplitude and writes only the nonzero ones of the other outcome, a
+  // share that depends on the state's support (half of a dense register, none of one already measured): the
+  // profiler counts the reads alone, a lower bound on its traffic
+  ProfScope ps(s, K_PROJECT, x ? full_bytes(s) : 0.5 * full_bytes(s));
   NCSIM_DISPATCH(s, {
     if (x == 0) {
       g = reduce_grid(s->len);

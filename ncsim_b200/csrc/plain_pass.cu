@@ -21,6 +21,7 @@
 #include <cmath>
 #include <cstring>
 #include <memory>
+#include <mutex>
 #include <string>
 
 #include "engine.cuh"
@@ -1181,11 +1182,17 @@ void launch_pass(ncsim_state* s, const PlainPlan& P, const PlainPlan::Item& it) 
   // the complex pool as this precision's values
   pp.cpool = reinterpret_cast<const V<R>*>(P.d_cpool);
   const size_t smem = 2 * (size_t(1) << it.win.g.T) * sizeof(V<R>);
-  static bool attr_set[2] = {false, false};
-  if (!attr_set[sizeof(R) == 8]) {
-    NCSIM_CUDA(cudaFuncSetAttribute(k_plain_pass<R>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                    int(2 * (size_t(1) << MAX_TILE_BITS) * sizeof(V<R>))));
-    attr_set[sizeof(R) == 8] = true;
+  {
+    // the kernel's shared-memory limit, set once per device and precision (host threads may race here)
+    static std::mutex mu;
+    static bool done[64][2] = {};
+    std::lock_guard<std::mutex> lk(mu);
+    const int dev = s->device;
+    if (dev < 0 || dev >= 64 || !done[dev][sizeof(R) == 8]) {
+      NCSIM_CUDA(cudaFuncSetAttribute(k_plain_pass<R>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                      int(2 * (size_t(1) << MAX_TILE_BITS) * sizeof(V<R>))));
+      if (dev >= 0 && dev < 64) done[dev][sizeof(R) == 8] = true;
+    }
   }
   const uint64_t grid = std::min<uint64_t>(pp.ntiles, uint64_t(sm_count()) * (sizeof(R) == 8 ? 1 : 2));
   ProfScope ps(s, K_PLAIN_PASS, 2.0 * double(s->len) * double(s->elem_bytes()));
@@ -1195,21 +1202,30 @@ void launch_pass(ncsim_state* s, const PlainPlan& P, const PlainPlan::Item& it) 
 
 void run_plain_plan(ncsim_state* s, PlainPlan& P) {
   if (P.device < 0) {
-    P.device = s->device;
+    // The pools go up on the state's own stream and are waited for: a cudaMemcpy from pageable
+    // memory runs on the legacy stream and may return before its DMA lands, and the pass
+    // kernels run on a non-blocking stream that does not wait for the legacy one.
+    cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
+    NCSIM_CUDA(cudaStreamIsCapturing(s->stream, &cap));
+    if (cap != cudaStreamCaptureStatusNone) throw Error(NCSIM_ERR_DEVICE, "a gate plan is uploaded outside stream capture");
     const bool dbl = s->precision == NCSIM_C128;
     const size_t nc = P.cpool.size() / 2;
-    if (dbl) {
-      NCSIM_CUDA(cudaMalloc(&P.d_cpool, std::max<size_t>(nc, 1) * sizeof(double2)));
-      NCSIM_CUDA(cudaMemcpy(P.d_cpool, P.cpool.data(), nc * sizeof(double2), cudaMemcpyHostToDevice));
-    } else {
-      std::vector<float> f(P.cpool.begin(), P.cpool.end());
-      NCSIM_CUDA(cudaMalloc(&P.d_cpool, std::max<size_t>(nc, 1) * sizeof(float2)));
-      NCSIM_CUDA(cudaMemcpy(P.d_cpool, f.data(), nc * sizeof(float2), cudaMemcpyHostToDevice));
-    }
+    std::vector<float> f;
+    if (!dbl) f.assign(P.cpool.begin(), P.cpool.end());
+    NCSIM_CUDA(cudaMalloc(&P.d_cpool, std::max<size_t>(nc, 1) * (dbl ? sizeof(double2) : sizeof(float2))));
     NCSIM_CUDA(cudaMalloc(&P.d_upool, std::max<size_t>(P.upool.size(), 1) * sizeof(uint32_t)));
-    NCSIM_CUDA(cudaMemcpy(P.d_upool, P.upool.data(), P.upool.size() * sizeof(uint32_t), cudaMemcpyHostToDevice));
     NCSIM_CUDA(cudaMalloc(&P.d_ppool, std::max<size_t>(P.ppool.size(), 1) * sizeof(uint64_t)));
-    NCSIM_CUDA(cudaMemcpy(P.d_ppool, P.ppool.data(), P.ppool.size() * sizeof(uint64_t), cudaMemcpyHostToDevice));
+    P.device = s->device;  // the destructor frees the pools from here on
+    if (nc)
+      NCSIM_CUDA(cudaMemcpyAsync(P.d_cpool, dbl ? static_cast<const void*>(P.cpool.data()) : f.data(),
+                                 nc * (dbl ? sizeof(double2) : sizeof(float2)), cudaMemcpyHostToDevice, s->stream));
+    if (!P.upool.empty())
+      NCSIM_CUDA(cudaMemcpyAsync(P.d_upool, P.upool.data(), P.upool.size() * sizeof(uint32_t), cudaMemcpyHostToDevice,
+                                 s->stream));
+    if (!P.ppool.empty())
+      NCSIM_CUDA(cudaMemcpyAsync(P.d_ppool, P.ppool.data(), P.ppool.size() * sizeof(uint64_t), cudaMemcpyHostToDevice,
+                                 s->stream));
+    NCSIM_CUDA(cudaStreamSynchronize(s->stream));
   }
   if (P.device != s->device) throw Error(NCSIM_ERR_DEVICE, "a gate plan stays on the device it was built for");
   for (const auto& it : P.items) {

@@ -850,7 +850,11 @@ struct RunBuilderW {
       WKey<W>* d_px = upload(px, st);
       WKey<W>* d_pz = upload(pz, st);
       RunDataW d{d_ops, uint32_t(ops.size()), d_img, d_ph, d_unit, d_tab, d_start, d_par, d_coeff, d_q, d_px, d_pz};
-      k_w_run<W><<<sp_grid(s->m), SP_THREADS, 0, st>>>(keys_of<W>(s), s->amp, s->m, d);
+      // a thread walks the whole run with its entry: with few entries, small blocks spread
+      // the walks over more SMs (the run is bound by each walk's dependent loads)
+      const unsigned threads = s->m < uint64_t(sm_count()) * SP_THREADS ? 32u : unsigned(SP_THREADS);
+      const unsigned grid = unsigned(std::min<uint64_t>((s->m + threads - 1) / threads, uint64_t(sm_count()) * 16));
+      k_w_run<W><<<grid, threads, 0, st>>>(keys_of<W>(s), s->amp, s->m, d);
       NCSIM_LAUNCHED("sparse run (wide)");
       dfree(d_ops, st);
       dfree(d_img, st);
