@@ -149,6 +149,9 @@ struct RunOpW {
   uint32_t nq, qoff;  // POLY: its qubits in RunDataW::qlist; PAULI: its masks (index into px/pz)
   uint64_t constant;  // POLY
   double2 scalar;     // POLY
+  // MONO on at most 3 qubits: the 8 images (16 bits each: patterns 0..3, 4..7) and unit flags
+  // (byte x: the phase of pattern x is exactly 1), packed on the host
+  uint64_t img_lo, img_hi, unit8;
 };
 struct RunDataW {
   const RunOpW* ops;
@@ -164,35 +167,93 @@ struct RunDataW {
   const void* px;  // WKey<W>[]: the runs' Pauli masks
   const void* pz;
 };
+// One warp per block, one entry per lane.  The run's op descriptors (monomials on at most 3
+// qubits carry their image and unit tables packed into words) are staged 32 at a time into
+// shared memory, one op per lane, so the walk reads them as broadcasts instead of a chain of
+// dependent global loads per op.
+constexpr int RW_STAGE = 32;
+// One lane's key held in shared memory, word w at col[w * RW_STAGE] (consecutive lanes in
+// consecutive words: conflict-free), so the walk's bit reads and writes stay on chip.
+struct SKeyCol {
+  uint64_t* col;
+  __device__ uint32_t bit(uint32_t q) const { return uint32_t(col[(q >> 6) * RW_STAGE] >> (q & 63)) & 1u; }
+  __device__ void set(uint32_t q, uint32_t v) const {
+    uint64_t& w = col[(q >> 6) * RW_STAGE];
+    const uint64_t b = uint64_t(1) << (q & 63);
+    w = v ? (w | b) : (w & ~b);
+  }
+};
 template <int W>
-__global__ void k_w_run(WKey<W>* key, double2* amp, uint64_t m, RunDataW d) {
+__global__ void __launch_bounds__(RW_STAGE) k_w_run(WKey<W>* key, double2* amp, uint64_t m, RunDataW d) {
+  __shared__ RunOpW s_op[RW_STAGE];
+  __shared__ uint64_t s_key[W * RW_STAGE];
   const WKey<W>* px = static_cast<const WKey<W>*>(d.px);
   const WKey<W>* pz = static_cast<const WKey<W>*>(d.pz);
-  NCSIM_GRID_LOOP(i, m) {
-    WKey<W> kk = key[i];
-    double2 a = amp[i];
-    for (uint32_t o = 0; o < d.nops; ++o) {
-      const RunOpW& op = d.ops[o];
-      if (op.type == RW_MONO) {
-        QubitsW qs;
-        qs.k = op.k;
-        for (uint32_t j = 0; j < op.k; ++j) qs.q[j] = op.q[j];
-        const uint32_t x = local_w(kk, qs);
-        if (!d.unit[op.off + x]) a = zmul(d.phase[op.off + x], a);
-        const uint32_t y = d.image[op.off + x];
-        if (y != x) set_local_w(kk, qs, y);
-      } else if (op.type == RW_POLY) {
-        const uint64_t x = local_w64(kk, d.qlist + op.qoff, op.nq);
-        poly_apply(x, a, op.bits, op.k, op.constant, op.flags & 1u, op.scalar, (op.flags >> 1) & 1u, d.start + op.off,
-                   d.par, d.coeff + op.off, d.table + op.toff);
-      } else {
-        const uint32_t k = (op.flags + 2u * and_popc(pz[op.qoff], kk)) & 3u;
-        if (k) a = ipow(a, k);
-        kxor(kk, px[op.qoff]);
+  const uint32_t lane = threadIdx.x;
+  const SKeyCol kk{s_key + lane};
+  for (uint64_t base = uint64_t(blockIdx.x) * RW_STAGE; base < m; base += uint64_t(gridDim.x) * RW_STAGE) {
+    const uint64_t i = base + lane;
+    const bool live = i < m;
+    double2 a = make_double2(0.0, 0.0);
+    {
+      WKey<W> k0{};
+      if (live) {
+        k0 = key[i];
+        a = amp[i];
+      }
+#pragma unroll
+      for (int w = 0; w < W; ++w) kk.col[w * RW_STAGE] = k0.w[w];
+    }
+    for (uint32_t o0 = 0; o0 < d.nops; o0 += RW_STAGE) {
+      const uint32_t cnt = min(uint32_t(RW_STAGE), d.nops - o0);
+      __syncwarp();
+      if (lane < cnt) s_op[lane] = d.ops[o0 + lane];
+      __syncwarp();
+      if (!live) continue;
+      for (uint32_t c = 0; c < cnt; ++c) {
+        const RunOpW& op = s_op[c];
+        if (op.type == RW_MONO) {
+          const uint32_t k = op.k;
+          uint32_t x = 0;
+          for (uint32_t j = 0; j < k; ++j) x |= kk.bit(op.q[j]) << j;
+          uint32_t y;
+          bool unit;
+          if (k <= 3) {
+            y = uint32_t((x < 4 ? op.img_lo : op.img_hi) >> (16 * (x & 3))) & 0xffffu;
+            unit = (op.unit8 >> (8 * x)) & 1u;
+          } else {
+            y = d.image[op.off + x];
+            unit = d.unit[op.off + x];
+          }
+          if (!unit) a = zmul(d.phase[op.off + x], a);
+          if (y != x)
+            for (uint32_t j = 0; j < k; ++j) kk.set(op.q[j], (y >> j) & 1u);
+        } else if (op.type == RW_POLY) {
+          uint64_t x = 0;
+          for (uint32_t j = 0; j < op.nq; ++j) x |= uint64_t(kk.bit(d.qlist[op.qoff + j])) << j;
+          poly_apply(x, a, op.bits, op.k, op.constant, op.flags & 1u, op.scalar, (op.flags >> 1) & 1u,
+                     d.start + op.off, d.par, d.coeff + op.off, d.table + op.toff);
+        } else {
+          const WKey<W>& zx = pz[op.qoff];
+          const WKey<W>& xx = px[op.qoff];
+          uint32_t cz = 0;
+#pragma unroll
+          for (int w = 0; w < W; ++w) {
+            cz += uint32_t(__popcll(zx.w[w] & kk.col[w * RW_STAGE]));
+            kk.col[w * RW_STAGE] ^= xx.w[w];
+          }
+          const uint32_t ph = (op.flags + 2u * cz) & 3u;
+          if (ph) a = ipow(a, ph);
+        }
       }
     }
-    key[i] = kk;
-    amp[i] = a;
+    if (live) {
+      WKey<W> k1;
+#pragma unroll
+      for (int w = 0; w < W; ++w) k1.w[w] = kk.col[w * RW_STAGE];
+      key[i] = k1;
+      amp[i] = a;
+    }
   }
 }
 
@@ -797,8 +858,13 @@ struct RunBuilderW {
     for (size_t x = 0; x < img.size(); ++x) {
       image.push_back(uint16_t(img[x]));
       phase.push_back(make_double2(ph[x].re, ph[x].im));
-      unit.push_back(ph[x].re == 1.0 && ph[x].im == 0.0);
+      const bool one = ph[x].re == 1.0 && ph[x].im == 0.0;
+      unit.push_back(one);
       moves |= img[x] != x;
+      if (qs.k <= 3) {
+        (x < 4 ? op.img_lo : op.img_hi) |= uint64_t(img[x]) << (16 * (x & 3));
+        op.unit8 |= uint64_t(one) << (8 * x);
+      }
     }
     ops.push_back(op);
   }
@@ -850,11 +916,10 @@ struct RunBuilderW {
       WKey<W>* d_px = upload(px, st);
       WKey<W>* d_pz = upload(pz, st);
       RunDataW d{d_ops, uint32_t(ops.size()), d_img, d_ph, d_unit, d_tab, d_start, d_par, d_coeff, d_q, d_px, d_pz};
-      // a thread walks the whole run with its entry: with few entries, small blocks spread
-      // the walks over more SMs (the run is bound by each walk's dependent loads)
-      const unsigned threads = s->m < uint64_t(sm_count()) * SP_THREADS ? 32u : unsigned(SP_THREADS);
-      const unsigned grid = unsigned(std::min<uint64_t>((s->m + threads - 1) / threads, uint64_t(sm_count()) * 16));
-      k_w_run<W><<<grid, threads, 0, st>>>(keys_of<W>(s), s->amp, s->m, d);
+      // one warp per block walks the run for 32 entries (up to 32 blocks per SM)
+      const unsigned grid =
+          unsigned(std::min<uint64_t>((s->m + RW_STAGE - 1) / RW_STAGE, uint64_t(sm_count()) * 32));
+      k_w_run<W><<<grid, RW_STAGE, 0, st>>>(keys_of<W>(s), s->amp, s->m, d);
       NCSIM_LAUNCHED("sparse run (wide)");
       dfree(d_ops, st);
       dfree(d_img, st);

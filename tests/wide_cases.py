@@ -64,6 +64,12 @@ def random_wide_text(n: int, gates: int, seed: int, dense_budget: int = 8, measu
         elif u < 0.88:
             a, b, c = qs(3)
             lines.append(f"{r.choice(['CCX', 'CCZ'])} {a} {b} {c}")
+        elif u < 0.895:
+            # diagonal phase polynomials: on 4 qubits (a monomial table) and on 11 (evaluated per entry)
+            if r.random() < 0.5:
+                lines.append(f"DIAG(3;1;1:1;3:2,4;5:1,2,8) {' '.join(map(str, qs(4)))}")
+            else:
+                lines.append(f"DIAG(4;3;5:1;3:6,1024;9:513,12,2) {' '.join(map(str, qs(11)))}")
         elif u < 0.93 and measure:
             lines.append(f"M {qs(1)[0]}")
         elif u < 0.95 and measure:
