@@ -23,7 +23,8 @@ struct PauliOp {
   bool hermitian() const { return ((phase & 1) == 1) == bool(__builtin_popcountll(x & z) & 1); }
 };
 // Circuits (and the Paulis they measure) may name up to this many qubits; the
-// state forms take registers of at most 64, the frame sampler any of these.
+// dense forms take registers of at most 64 (the sparse form 1024), the frame
+// sampler any of these.
 constexpr uint32_t MAX_CIRCUIT_QUBITS = 1u << 24;
 
 // A Pauli on any number of qubits as its non-identity sites (qubit ascending;
