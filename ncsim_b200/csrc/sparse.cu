@@ -103,13 +103,13 @@ __global__ void k_sp_count(const uint64_t* key, uint64_t m, Qubits qs, const uin
   }
 }
 __global__ void k_sp_expand(const uint64_t* key, const double2* amp, uint64_t m, Qubits qs, const uint32_t* col_start,
-                            const uint32_t* col_row, const double2* col_val, const uint32_t* off, uint64_t* okey,
-                            double2* oamp) {
+                            const uint32_t* col_row, const double2* col_val, const uint32_t* off, uint32_t per,
+                            uint64_t* okey, double2* oamp) {
   for (uint64_t i = uint64_t(blockIdx.x) * blockDim.x + threadIdx.x; i < m; i += uint64_t(gridDim.x) * blockDim.x) {
     const uint64_t kk = key[i];
     const double2 v = amp[i];
     const uint32_t b = local_of(kk, qs);
-    uint32_t o = off[i];
+    uint64_t o = off ? uint64_t(off[i]) : i * per;  // per: every column's count, when they are all equal
     for (uint32_t j = col_start[b]; j < col_start[b + 1]; ++j, ++o) {
       okey[o] = with_local(kk, qs, col_row[j]);
       oamp[o] = zmul(col_val[j], v);
@@ -158,6 +158,9 @@ struct RunOp {
   uint32_t toff;     // POLY: first entry of its phasor table in RunData::table
   uint64_t x, z;     // PAULI; POLY: x = constant
   double2 scalar;    // POLY
+  // MONO on at most 3 qubits: the 8 images (16 bits each: patterns 0..3, 4..7) and unit flags
+  // (byte x: the phase of pattern x is exactly 1), packed on the host
+  uint64_t img_lo, img_hi, unit8;
 };
 struct RunData {
   const RunOp* ops;
@@ -171,31 +174,63 @@ struct RunData {
   const uint64_t* coeff;
   const uint64_t* and_mask;  // per term (aligned with coeff): the AND of single-bit parities, or 0
 };
-__global__ void k_sp_run(uint64_t* key, double2* amp, uint64_t m, RunData d) {
-  for (uint64_t i = uint64_t(blockIdx.x) * blockDim.x + threadIdx.x; i < m; i += uint64_t(gridDim.x) * blockDim.x) {
-    uint64_t kk = key[i];
-    double2 a = amp[i];
-    for (uint32_t o = 0; o < d.nops; ++o) {
-      const RunOp& op = d.ops[o];
-      if (op.type == RUN_MONO) {
-        Qubits qs;
-        qs.k = op.k;
-        for (uint32_t j = 0; j < op.k; ++j) qs.q[j] = op.q[j];
-        const uint32_t x = local_of(kk, qs);
-        if (!d.unit[op.off + x]) a = zmul(d.phase[op.off + x], a);
-        const uint32_t y = d.image[op.off + x];
-        if (y != x) kk = with_local(kk, qs, y);
-      } else if (op.type == RUN_POLY) {
-        poly_apply(kk, a, op.bits, op.k, op.x, op.flags & 1u, op.scalar, (op.flags >> 1) & 1u, d.start + op.off, d.par,
-                   d.coeff + op.off, d.table + op.toff, d.and_mask + op.off);
-      } else {
-        const uint32_t k = (op.flags + 2u * uint32_t(__popcll(op.z & kk))) & 3u;
-        if (k) a = ipow(a, k);
-        kk ^= op.x;
+// The block stages the run's op descriptors RUN_STAGE at a time in shared
+// memory, so each thread's walk reads them as broadcasts instead of a chain of
+// dependent global loads per op; monomials on at most 3 qubits carry their image
+// and unit tables in the descriptor, a wider monomial's three table loads issue
+// together, and a phase polynomial's terms are loaded 32 at a time by the warp.
+// Every lane walks the ops (lanes past the last entry on a dummy entry) so that
+// the warp's shuffles see all 32 lanes.
+constexpr uint32_t RUN_STAGE = SP_THREADS;
+__global__ void __launch_bounds__(SP_THREADS) k_sp_run(uint64_t* key, double2* amp, uint64_t m, RunData d) {
+  __shared__ RunOp s_op[RUN_STAGE];
+  for (uint64_t base = uint64_t(blockIdx.x) * blockDim.x; base < m; base += uint64_t(gridDim.x) * blockDim.x) {
+    const uint64_t i = base + threadIdx.x;
+    const bool live = i < m;
+    uint64_t kk = live ? key[i] : 0;
+    double2 a = live ? amp[i] : make_double2(0.0, 0.0);
+    for (uint32_t o0 = 0; o0 < d.nops; o0 += RUN_STAGE) {
+      const uint32_t cnt = min(RUN_STAGE, d.nops - o0);
+      __syncthreads();
+      if (threadIdx.x < cnt) s_op[threadIdx.x] = d.ops[o0 + threadIdx.x];
+      __syncthreads();
+      for (uint32_t c = 0; c < cnt; ++c) {
+        const RunOp& op = s_op[c];
+        if (op.type == RUN_MONO) {
+          const uint32_t k = op.k;
+          uint32_t x = 0;
+          for (uint32_t j = 0; j < k; ++j) x |= uint32_t((kk >> op.q[j]) & 1u) << j;
+          uint32_t y;
+          bool unit;
+          double2 ph = make_double2(1.0, 0.0);
+          if (k <= 3) {
+            y = uint32_t((x < 4 ? op.img_lo : op.img_hi) >> (16 * (x & 3))) & 0xffffu;
+            unit = (op.unit8 >> (8 * x)) & 1u;
+            if (!unit) ph = d.phase[op.off + x];
+          } else {
+            y = d.image[op.off + x];
+            unit = d.unit[op.off + x];
+            ph = d.phase[op.off + x];
+          }
+          if (!unit) a = zmul(ph, a);
+          if (y != x)
+            for (uint32_t j = 0; j < k; ++j)
+              kk = (kk & ~(uint64_t(1) << op.q[j])) | (uint64_t((y >> j) & 1u) << op.q[j]);
+        } else if (op.type == RUN_POLY) {
+          const uint64_t f =
+              poly_sum_warp(kk, op.k, op.x, d.start + op.off, d.par, d.coeff + op.off, d.and_mask + op.off);
+          poly_finish(f, a, op.bits, op.flags & 1u, op.scalar, (op.flags >> 1) & 1u, d.table + op.toff);
+        } else {
+          const uint32_t ph = (op.flags + 2u * uint32_t(__popcll(op.z & kk))) & 3u;
+          if (ph) a = ipow(a, ph);
+          kk ^= op.x;
+        }
       }
     }
-    key[i] = kk;
-    amp[i] = a;
+    if (live) {
+      key[i] = kk;
+      amp[i] = a;
+    }
   }
 }
 
@@ -294,20 +329,17 @@ void sp_normalize_from(ncsim_sparse* s, uint64_t* key, double2* amp, uint64_t cn
   NCSIM_CUDA(cub::DeviceSelect::Flagged(nullptr, t4, a3, flag, amp, d_num + 1, num, st));
   const size_t tb = std::max(std::max(t1, t2), std::max(t3, t4));
   void* tmp = dalloc<uint8_t>(tb, st);
-  int runs = 0, kept = 0;
+  int kept = 0;
   if (num > 0) {
     NCSIM_CUDA(cub::DeviceRadixSort::SortPairs(tmp, t1, key, k2, amp, a2, num, 0, end_bit, st));
     NCSIM_CUDA(cub::DeviceReduce::ReduceByKey(tmp, t2, k2, k3, a2, a3, d_num, ZAdd(), num, st));
-    NCSIM_CUDA(cudaMemcpyAsync(&runs, d_num, sizeof(int), cudaMemcpyDeviceToHost, st));
+    // the run count stays on the device: the keep flags drop the positions past it
+    k_sp_keep<<<sp_grid(cnt), SP_THREADS, 0, st>>>(a3, d_num, cnt, s->cutoff * s->cutoff, flag);
+    NCSIM_LAUNCHED("sparse keep");
+    NCSIM_CUDA(cub::DeviceSelect::Flagged(tmp, t3, k3, flag, key, d_num + 1, num, st));
+    NCSIM_CUDA(cub::DeviceSelect::Flagged(tmp, t4, a3, flag, amp, d_num + 1, num, st));
+    NCSIM_CUDA(cudaMemcpyAsync(&kept, d_num + 1, sizeof(int), cudaMemcpyDeviceToHost, st));
     NCSIM_CUDA(cudaStreamSynchronize(st));
-    if (runs > 0) {
-      k_sp_keep<<<sp_grid(uint64_t(runs)), SP_THREADS, 0, st>>>(a3, uint64_t(runs), s->cutoff * s->cutoff, flag);
-      NCSIM_LAUNCHED("sparse keep");
-      NCSIM_CUDA(cub::DeviceSelect::Flagged(tmp, t3, k3, flag, key, d_num + 1, runs, st));
-      NCSIM_CUDA(cub::DeviceSelect::Flagged(tmp, t4, a3, flag, amp, d_num + 1, runs, st));
-      NCSIM_CUDA(cudaMemcpyAsync(&kept, d_num + 1, sizeof(int), cudaMemcpyDeviceToHost, st));
-      NCSIM_CUDA(cudaStreamSynchronize(st));
-    }
   }
   dfree(tmp, st);
   dfree(k2, st);
@@ -478,10 +510,15 @@ void sp_matrix(ncsim_sparse* s, const std::vector<uint32_t>& qubits, const std::
   uint32_t* dcs = upload(col_start, st);
   uint32_t* dcr = upload(col_row, st);
   double2* dcv = upload(col_val, st);
-  uint32_t* cnt = dalloc<uint32_t>(m + 1, st);
-  uint32_t* off = dalloc<uint32_t>(m + 1, st);
-  uint64_t total = 0;
-  if (m) {
+  // every column with the same count (H, SQRT_X, rotations): entry i's images start at i * per,
+  // so the counts, their scan and the host's wait for the total are not needed
+  const uint32_t per = col_start[1] - col_start[0];
+  bool uniform = true;
+  for (size_t b = 0; b < gd && uniform; ++b) uniform = col_start[b + 1] - col_start[b] == per;
+  uint32_t* cnt = uniform ? nullptr : dalloc<uint32_t>(m + 1, st);
+  uint32_t* off = uniform ? nullptr : dalloc<uint32_t>(m + 1, st);
+  uint64_t total = uniform ? m * per : 0;
+  if (m && !uniform) {
     k_sp_count<<<sp_grid(m), SP_THREADS, 0, st>>>(s->key, m, qs, dcs, cnt);
     NCSIM_LAUNCHED("sparse count");
     NCSIM_CUDA(cudaMemsetAsync(cnt + m, 0, sizeof(uint32_t), st));
@@ -495,10 +532,11 @@ void sp_matrix(ncsim_sparse* s, const std::vector<uint32_t>& qubits, const std::
     dfree(tmp, st);
     total = t32;
   }
+  if (total > uint64_t(INT32_MAX)) throw Error(NCSIM_ERR_UNSUPPORTED, "sparse state of more than 2^31 entries");
   uint64_t* okey = dalloc<uint64_t>(total, st);
   double2* oamp = dalloc<double2>(total, st);
   if (total) {
-    k_sp_expand<<<sp_grid(m), SP_THREADS, 0, st>>>(s->key, s->amp, m, qs, dcs, dcr, dcv, off, okey, oamp);
+    k_sp_expand<<<sp_grid(m), SP_THREADS, 0, st>>>(s->key, s->amp, m, qs, dcs, dcr, dcv, off, per, okey, oamp);
     NCSIM_LAUNCHED("sparse expand");
   }
   dfree(dcs, st);
@@ -521,6 +559,19 @@ struct RunBuilder {
   bool moves = false;
 
   bool empty() const { return ops.empty(); }
+  // empties the builder and keeps its buffers' capacity for the next run
+  void reset() {
+    ops.clear();
+    image.clear();
+    phase.clear();
+    unit.clear();
+    table.clear();
+    start.clear();
+    par.clear();
+    coeff.clear();
+    and_mask.clear();
+    moves = false;
+  }
   void add_mono(const std::vector<uint32_t>& qubits, const std::vector<uint32_t>& img, const std::vector<CplxD>& ph) {
     RunOp op{};
     op.type = RUN_MONO;
@@ -530,8 +581,13 @@ struct RunBuilder {
     for (size_t x = 0; x < img.size(); ++x) {
       image.push_back(uint16_t(img[x]));
       phase.push_back(make_double2(ph[x].re, ph[x].im));
-      unit.push_back(ph[x].re == 1.0 && ph[x].im == 0.0);
+      const bool one = ph[x].re == 1.0 && ph[x].im == 0.0;
+      unit.push_back(one);
       moves |= img[x] != x;
+      if (op.k <= 3) {
+        (x < 4 ? op.img_lo : op.img_hi) |= uint64_t(img[x]) << (16 * (x & 3));
+        op.unit8 |= uint64_t(one) << (8 * x);
+      }
     }
     ops.push_back(op);
   }
@@ -601,7 +657,7 @@ struct RunBuilder {
       dfree(d_and, st);
     }
     if (moves) s->sorted = false;
-    *this = RunBuilder();
+    reset();
   }
 };
 
@@ -1161,7 +1217,9 @@ ncsim_status ncsim_sparse_run(ncsim_sparse* s, const ncsim_circuit* c, ncsim_rng
     // runs of one-to-one ops (gates with a monomial, diagonal or Pauli view, and the
     // Paulis of sampled noise) go to the device as one pass each; a measurement, a
     // reset or a gate that creates entries ends a run
-    RunBuilder run;
+    // one builder per host thread, reused so that its tables keep their capacity across runs
+    static thread_local RunBuilder run;
+    run.reset();
     std::vector<uint32_t> img;
     std::vector<CplxD> ph;
     for (const OpIR& op : c->ops) {

@@ -105,26 +105,10 @@ __device__ double2 turn_root(uint64_t f, uint32_t bits) {
 }
 
 
-// amp *= scalar * zeta^f(key), f = constant + sum_t coeff_t prod_l [par_l . key] mod 2^bits
-// (and_mask, when given: a term whose parities are all single bits is the AND of
-// those bits, one compare instead of a popcount per parity; 0 for other terms)
-template <class Start>
-__device__ __forceinline__ void poly_apply(uint64_t kk, double2& amp, uint32_t bits, uint32_t nterms, uint64_t constant,
-                                           bool scalar_is_one, double2 scalar, bool use_table, const Start* start,
-                                           const uint64_t* par, const uint64_t* coeff, const double2* table,
-                                           const uint64_t* and_mask = nullptr) {
+// amp *= scalar * zeta^f for the polynomial's value f (reduced mod 2^bits here)
+__device__ __forceinline__ void poly_finish(uint64_t f, double2& amp, uint32_t bits, bool scalar_is_one,
+                                            double2 scalar, bool use_table, const double2* table) {
   const uint64_t mk = bits >= 64 ? ~uint64_t(0) : (uint64_t(1) << bits) - 1;
-  uint64_t f = constant;
-  for (uint32_t t = 0; t < nterms; ++t) {
-    uint32_t all = 1;
-    const uint64_t am = and_mask ? and_mask[t] : 0;
-    if (am) {
-      all = (kk & am) == am;
-    } else {
-      for (uint32_t l = start[t]; l < start[t + 1]; ++l) all &= uint32_t(__popcll(par[l] & kk)) & 1u;
-    }
-    if (all) f += coeff[t];
-  }
   f &= mk;
   double2 c;
   if (use_table) {
@@ -136,6 +120,67 @@ __device__ __forceinline__ void poly_apply(uint64_t kk, double2& amp, uint32_t b
   }
   if (c.x == 1.0 && c.y == 0.0) return;
   amp = zmul(c, amp);
+}
+
+// amp *= scalar * zeta^f(key), f = constant + sum_t coeff_t prod_l [par_l . key] mod 2^bits
+// (and_mask, when given: a term whose parities are all single bits is the AND of
+// those bits, one compare instead of a popcount per parity; 0 for other terms)
+template <class Start>
+__device__ __forceinline__ void poly_apply(uint64_t kk, double2& amp, uint32_t bits, uint32_t nterms, uint64_t constant,
+                                           bool scalar_is_one, double2 scalar, bool use_table, const Start* start,
+                                           const uint64_t* par, const uint64_t* coeff, const double2* table,
+                                           const uint64_t* and_mask = nullptr) {
+  uint64_t f = constant;
+#pragma unroll 4
+  for (uint32_t t = 0; t < nterms; ++t) {
+    uint32_t all = 1;
+    const uint64_t am = and_mask ? and_mask[t] : 0;
+    if (am) {
+      all = (kk & am) == am;
+    } else {
+      for (uint32_t l = start[t]; l < start[t + 1]; ++l) all &= uint32_t(__popcll(par[l] & kk)) & 1u;
+    }
+    if (all) f += coeff[t];
+  }
+  poly_finish(f, amp, bits, scalar_is_one, scalar, use_table, table);
+}
+
+// The sum of poly_apply with the warp sharing the term loads: lane j loads term
+// t0 + j of each group of 32 and the terms reach every lane by shuffles, so a
+// polynomial of many terms costs one round of dependent loads per 32 terms
+// instead of one per term (integer sums: the same f in any order).  All 32 lanes
+// of the warp call it with the same polynomial.
+__device__ __forceinline__ uint64_t poly_sum_warp(uint64_t kk, uint32_t nterms, uint64_t constant,
+                                                  const uint32_t* start, const uint64_t* par, const uint64_t* coeff,
+                                                  const uint64_t* and_mask) {
+  const uint32_t lane = threadIdx.x & 31u;
+  uint64_t f = constant;
+  for (uint32_t t0 = 0; t0 < nterms; t0 += 32) {
+    const uint32_t t = t0 + lane;
+    uint64_t am = 0, co = 0;
+    uint32_t s0 = 0, s1 = 0;
+    if (t < nterms) {
+      am = and_mask[t];
+      co = coeff[t];
+      s0 = start[t];
+      s1 = start[t + 1];
+    }
+    const uint32_t cnt = min(32u, nterms - t0);
+    for (uint32_t j = 0; j < cnt; ++j) {
+      const uint64_t amj = __shfl_sync(0xffffffffu, am, int(j));
+      const uint64_t coj = __shfl_sync(0xffffffffu, co, int(j));
+      uint32_t all = 1;
+      if (amj) {  // warp-uniform
+        all = (kk & amj) == amj;
+      } else {
+        const uint32_t a0 = __shfl_sync(0xffffffffu, s0, int(j));
+        const uint32_t a1 = __shfl_sync(0xffffffffu, s1, int(j));
+        for (uint32_t l = a0; l < a1; ++l) all &= uint32_t(__popcll(par[l] & kk)) & 1u;
+      }
+      if (all) f += coj;
+    }
+  }
+  return f;
 }
 
 __global__ void k_sp_scale(double2* amp, uint64_t m, double2 c) {
@@ -150,8 +195,17 @@ struct ZAdd {
     return make_double2(a.x + b.x, a.y + b.y);
   }
 };
-__global__ void k_sp_keep(const double2* amp, uint64_t m, double cut2, uint8_t* flag) {
-  for (uint64_t i = uint64_t(blockIdx.x) * blockDim.x + threadIdx.x; i < m; i += uint64_t(gridDim.x) * blockDim.x) {
+// Keep flags over a reduce-by-key output whose run count is still on the device:
+// an entry stays when its amplitude is nonzero and |a|^2 >= cutoff^2 (or the
+// cutoff is 0); positions at or past the count are dropped, so the selection can
+// run over the input's size without the host waiting for the count.
+__global__ void k_sp_keep(const double2* amp, const int* d_runs, uint64_t cap, double cut2, uint8_t* flag) {
+  const uint64_t runs = uint64_t(*d_runs);
+  for (uint64_t i = uint64_t(blockIdx.x) * blockDim.x + threadIdx.x; i < cap; i += uint64_t(gridDim.x) * blockDim.x) {
+    if (i >= runs) {
+      flag[i] = 0;
+      continue;
+    }
     const double2 a = amp[i];
     const bool zero = a.x == 0.0 && a.y == 0.0;
     flag[i] = !zero && (cut2 == 0.0 || a.x * a.x + a.y * a.y >= cut2);

@@ -267,13 +267,13 @@ __global__ void k_w_count(const WKey<W>* key, uint64_t m, QubitsW qs, const uint
 }
 template <int W>
 __global__ void k_w_expand(const WKey<W>* key, const double2* amp, uint64_t m, QubitsW qs, const uint32_t* col_start,
-                           const uint32_t* col_row, const double2* col_val, const uint32_t* off, WKey<W>* okey,
-                           double2* oamp) {
+                           const uint32_t* col_row, const double2* col_val, const uint32_t* off, uint32_t per,
+                           WKey<W>* okey, double2* oamp) {
   NCSIM_GRID_LOOP(i, m) {
     const WKey<W> kk = key[i];
     const double2 v = amp[i];
     const uint32_t b = local_w(kk, qs);
-    uint32_t o = off[i];
+    uint64_t o = off ? uint64_t(off[i]) : uint64_t(i) * per;  // per: every column's count, when they are all equal
     for (uint32_t j = col_start[b]; j < col_start[b + 1]; ++j, ++o) {
       WKey<W> nk = kk;
       set_local_w(nk, qs, col_row[j]);
@@ -527,7 +527,7 @@ void normalize_from(ncsim_sparse* s, WKey<W>* key, double2* amp, uint64_t cnt) {
   double2* a3 = dalloc<double2>(cnt, st);
   uint8_t* flag = dalloc<uint8_t>(cnt, st);
   int* d_num = dalloc<int>(2, st);
-  int runs = 0, kept = 0;
+  int kept = 0;
   if (num > 0) {
     sort_pairs<W>(key, amp, k2, a2, cnt, st);
     size_t t2 = 0, t3 = 0, t4 = 0;
@@ -536,16 +536,13 @@ void normalize_from(ncsim_sparse* s, WKey<W>* key, double2* amp, uint64_t cnt) {
     NCSIM_CUDA(cub::DeviceSelect::Flagged(nullptr, t4, a3, flag, amp, d_num + 1, num, st));
     void* tmp = dalloc<uint8_t>(std::max(t2, std::max(t3, t4)), st);
     NCSIM_CUDA(cub::DeviceReduce::ReduceByKey(tmp, t2, k2, k3, a2, a3, d_num, ZAdd(), num, st));
-    NCSIM_CUDA(cudaMemcpyAsync(&runs, d_num, sizeof(int), cudaMemcpyDeviceToHost, st));
+    // the run count stays on the device: the keep flags drop the positions past it
+    k_sp_keep<<<sp_grid(cnt), SP_THREADS, 0, st>>>(a3, d_num, cnt, s->cutoff * s->cutoff, flag);
+    NCSIM_LAUNCHED("sparse keep");
+    NCSIM_CUDA(cub::DeviceSelect::Flagged(tmp, t3, k3, flag, key, d_num + 1, num, st));
+    NCSIM_CUDA(cub::DeviceSelect::Flagged(tmp, t4, a3, flag, amp, d_num + 1, num, st));
+    NCSIM_CUDA(cudaMemcpyAsync(&kept, d_num + 1, sizeof(int), cudaMemcpyDeviceToHost, st));
     NCSIM_CUDA(cudaStreamSynchronize(st));
-    if (runs > 0) {
-      k_sp_keep<<<sp_grid(uint64_t(runs)), SP_THREADS, 0, st>>>(a3, uint64_t(runs), s->cutoff * s->cutoff, flag);
-      NCSIM_LAUNCHED("sparse keep");
-      NCSIM_CUDA(cub::DeviceSelect::Flagged(tmp, t3, k3, flag, key, d_num + 1, runs, st));
-      NCSIM_CUDA(cub::DeviceSelect::Flagged(tmp, t4, a3, flag, amp, d_num + 1, runs, st));
-      NCSIM_CUDA(cudaMemcpyAsync(&kept, d_num + 1, sizeof(int), cudaMemcpyDeviceToHost, st));
-      NCSIM_CUDA(cudaStreamSynchronize(st));
-    }
     dfree(tmp, st);
   }
   dfree(k2, st);
@@ -656,10 +653,14 @@ void matrix_w(ncsim_sparse* s, const QubitsW& qs, const std::vector<CplxD>& mat)
   uint32_t* dcs = upload(col_start, st);
   uint32_t* dcr = upload(col_row, st);
   double2* dcv = upload(col_val, st);
-  uint32_t* cnt = dalloc<uint32_t>(m + 1, st);
-  uint32_t* off = dalloc<uint32_t>(m + 1, st);
-  uint64_t total = 0;
-  if (m) {
+  // every column with the same count: entry i's images start at i * per (no counts, scan or wait)
+  const uint32_t per = col_start[1] - col_start[0];
+  bool uniform = true;
+  for (size_t b = 0; b < gd && uniform; ++b) uniform = col_start[b + 1] - col_start[b] == per;
+  uint32_t* cnt = uniform ? nullptr : dalloc<uint32_t>(m + 1, st);
+  uint32_t* off = uniform ? nullptr : dalloc<uint32_t>(m + 1, st);
+  uint64_t total = uniform ? m * per : 0;
+  if (m && !uniform) {
     k_w_count<W><<<sp_grid(m), SP_THREADS, 0, st>>>(keys_of<W>(s), m, qs, dcs, cnt);
     NCSIM_LAUNCHED("sparse count (wide)");
     NCSIM_CUDA(cudaMemsetAsync(cnt + m, 0, sizeof(uint32_t), st));
@@ -673,10 +674,12 @@ void matrix_w(ncsim_sparse* s, const QubitsW& qs, const std::vector<CplxD>& mat)
     dfree(tmp, st);
     total = t32;
   }
+  if (total > uint64_t(INT32_MAX)) throw Error(NCSIM_ERR_UNSUPPORTED, "sparse state of more than 2^31 entries");
   WKey<W>* okey = dalloc<WKey<W>>(total, st);
   double2* oamp = dalloc<double2>(total, st);
   if (total) {
-    k_w_expand<W><<<sp_grid(m), SP_THREADS, 0, st>>>(keys_of<W>(s), s->amp, m, qs, dcs, dcr, dcv, off, okey, oamp);
+    k_w_expand<W><<<sp_grid(m), SP_THREADS, 0, st>>>(keys_of<W>(s), s->amp, m, qs, dcs, dcr, dcv, off, per,
+                                                     okey, oamp);
     NCSIM_LAUNCHED("sparse expand (wide)");
   }
   dfree(dcs, st);

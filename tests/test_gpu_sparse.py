@@ -167,3 +167,38 @@ def test_errors(nb):
         s.scale(0.0)
         s.sample(nb.StdRng(0), 3)
     assert e.value.kind == "ZeroState"
+
+
+def poly_run_text(n, rng):
+    """|+>^n, then phase polynomials over the whole register (20..44 terms of
+    1..3 parities, half of them single bits, half multi-bit masks; 3- and 5-bit
+    phases) interleaved with Toffoli and CNOT gates: one run of one-to-one ops."""
+    lines = [f"QUBITS {n}"] + [f"H {q}" for q in range(n)]
+    for _ in range(6):
+        terms = []
+        for _ in range(int(rng.integers(20, 45))):
+            masks = [int(rng.integers(1, 1 << n)) if rng.random() < 0.5 else 1 << int(rng.integers(n))
+                     for _ in range(int(rng.integers(1, 4)))]
+            terms.append(f"{int(rng.integers(1, 32))}:" + ",".join(map(str, masks)))
+        bits = int(rng.choice([3, 5]))
+        lines.append(f"DIAG({bits};{int(rng.integers(1 << bits))};" + ";".join(terms) + ") "
+                     + " ".join(map(str, range(n))))
+        a, b, c = (int(v) for v in rng.choice(n, 3, replace=False))
+        lines.append(f"CCX {a} {b} {c}")
+        lines.append(f"CX {b} {c}")
+    return "\n".join(lines) + "\n"
+
+
+def test_phase_polynomials_in_a_run_match_the_dense_vector(nb, oracle):
+    """Phase polynomials inside a run (the warp-shared term loads): single-bit and
+    multi-bit parities, more than 32 terms, against the dense FP64 oracle."""
+    rng = np.random.default_rng(21)
+    for trial in range(4):
+        n = 10 + trial
+        text = poly_run_text(n, rng)
+        s = nb.GpuSparseVector(n)
+        s.run(nb.Circuit.parse(text), nb.StdRng(0))
+        v = oracle.StateVector(n)
+        v.run(oracle.Circuit(text), oracle.StdRng(0))
+        assert s.num_entries() == 1 << n
+        assert np.abs(s.to_vector() - v.to_vector()).max() < TOL, trial
